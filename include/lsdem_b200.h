@@ -1,0 +1,178 @@
+/*
+ * lsdem_b200 — C ABI of the B200-native level-set DEM step.
+ *
+ * Plain pointers and sizes only. Vectors are 3 doubles (x, y, z), quaternions
+ * 4 doubles (q0 scalar first, local -> world), symmetric tensors 6 doubles
+ * (xx, yy, zz, xy, xz, yz), integer triples 3 ints. Every call returns an
+ * LSDEM_* status; lsdem_last_error() gives the message of the last failure.
+ *
+ * Each entry point replaces a part of the reference solver's host API or of
+ * its internal extern "C" launcher layer; the reference interface is cited
+ * (paths relative to the reference project root).
+ */
+#ifndef LSDEM_B200_H
+#define LSDEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSDEM_OK 0
+#define LSDEM_ERR_ARG 1      /* invalid argument (reference: cerr + return) */
+#define LSDEM_ERR_CUDA 2     /* CUDA runtime error (reference: CUDA_CHECK throws) */
+#define LSDEM_ERR_NOMEM 3    /* device allocation failed */
+#define LSDEM_ERR_STATE 4    /* call out of order (e.g. step before initialize) */
+#define LSDEM_ERR_NODEVICE 5 /* no usable CUDA device (reference: exit(1)) */
+
+/* Compatibility switches (lsdem_set_flags). Both quirks of the reference are
+ * kept by default; setting a bit replaces the quirk by the exact form. */
+#define LSDEM_FIX_GRADIENT 1 /* x weight of the SDF gradient (LSParticleContactDetectionKernel.cuh:34-52) */
+#define LSDEM_FIX_SQRTF 2    /* FP64 sqrt in the damping terms (contactKernel.cuh:51,53,58) */
+
+/* Contact list kinds for lsdem_get_contacts / lsdem_count_contacts. */
+#define LSDEM_CONTACT_PARTICLE 0 /* particle-particle (LSSolver.h:706-763) */
+#define LSDEM_CONTACT_WALL 1     /* particle-wall (LSSolver.h:765-822) */
+#define LSDEM_CONTACT_GHOST 2    /* particle-periodic image (PeriodicBoundary.h:75-141) */
+
+typedef struct lsdem_solver lsdem_solver;
+
+/* External force hook, called once per step after the contact and bond
+ * forces and before the second half kick, with the simulation time of the
+ * step. Replaces the virtual LSSolver::addExternalForceTorque (LSSolver.h:508).
+ * Kernels it launches on the solver's stream (or the legacy default stream
+ * when the solver uses it) see the step's forces. When a step batch is
+ * re-run after a capacity overflow, the hook is called again for those steps. */
+typedef void (*lsdem_hook)(void* user, double time);
+
+/* Solver lifetime. Replaces LSSolver(dir, stream, maxGPUThread, device) (LSSolver.h:14).
+ * `stream` is a cudaStream_t (NULL: legacy default stream, as the reference).
+ * No device work happens before lsdem_initialize. */
+int lsdem_create(int device, void* stream, lsdem_solver** out);
+void lsdem_destroy(lsdem_solver* s);
+const char* lsdem_last_error(const lsdem_solver* s);
+int lsdem_set_flags(lsdem_solver* s, int flags);
+
+/* Mass, centroid, inertia and inverse inertia of a level-set body by smoothed
+ * Heaviside integration of its SDF grid (LSSolver.h:66-135). out[16] = mass,
+ * centroid(3), inertia(6), inverse inertia(6). Host only; needs no device. */
+int lsdem_mass_properties(const double* sdf, const int* size3, const double* origin3, double spacing,
+                          double density, double* out16);
+
+/* Registers a shape template (surface nodes in the body frame + SDF grid with
+ * index ix + nx*(iy + ny*iz), phi < 0 inside). Identical templates are shared.
+ * Replaces the per-particle copies appended by LSParticle::add (LSParticle.h:115-212). */
+int lsdem_add_shape(lsdem_solver* s, const double* nodes, int n_nodes, const double* sdf, const int* size3,
+                    const double* origin3, double spacing, int* shape_id);
+
+/* Appends n particles of registered shapes with explicit inverse mass and
+ * body-frame inverse inertia (LSSolver.h:190-223 + LSParticle::add). `scale`
+ * (nullable) uniformly scales the template (nodes, grid, SDF values).
+ * Quaternions are normalised, kn/ks/mu clamped at 0, restitution outside
+ * (0, 1] set to 1 (LSParticle.h:193-202). `first_index` (nullable) receives
+ * the index of the first new particle. */
+int lsdem_add_particles(lsdem_solver* s, int n, const int* shape, const double* scale, const double* pos,
+                        const double* vel, const double* angvel, const double* quat, const double* inv_mass,
+                        const double* inv_inertia6, const double* kn, const double* ks, const double* mu,
+                        const double* e, int* first_index);
+
+/* One particle with mass and inertia from the SDF and density, frame moved to
+ * the centroid: LSSolver::addLSParticle (LSSolver.h:51-163). */
+int lsdem_add_ls_particle(lsdem_solver* s, const double* nodes, int n_nodes, const double* sdf, const int* size3,
+                          const double* origin3, double spacing, const double* pos, const double* vel,
+                          const double* angvel, const double* quat, double kn, double ks, double mu, double e,
+                          double density, int* index);
+
+/* A fixed level-set wall (LSSolver::addWall, LSSolver.h:245-272). */
+int lsdem_add_wall(lsdem_solver* s, const double* verts, int n_verts, const double* sdf, const int* size3,
+                   const double* origin3, double spacing, const double* pos, const double* quat, double mu, double e,
+                   int* index);
+/* LSSolver::moveLSParticle / moveWall / setFixedVelocityToWall / setFixedAngularVelocityToWall (LSSolver.h:280-320). */
+int lsdem_move_particle(lsdem_solver* s, int index, const double* offset3);
+int lsdem_move_wall(lsdem_solver* s, int index, const double* offset3);
+int lsdem_set_wall_velocity(lsdem_solver* s, int index, const double* v3);
+int lsdem_set_wall_angular_velocity(lsdem_solver* s, int index, const double* w3);
+
+/* V-bond between two particles (LSSolver::addBondedInteraction, LSSolver.h:344-379;
+ * VBondedInteraction::add, VBondedInteraction.h:74-195). */
+int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3, const double* normal3,
+                   double radius, double initial_length, double youngs, double poisson, double tensile,
+                   double cohesion, double mu);
+/* Bonds from the current particle-particle contacts (LSSolver::createBondsFromContacts, LSSolver.h:385-418). */
+int lsdem_create_bonds_from_contacts(lsdem_solver* s, double radius, double initial_length, double youngs,
+                                     double poisson, double tensile, double cohesion, double mu);
+
+/* Periodic axes bit mask (bit 0 x, 1 y, 2 z). x and y follow
+ * addPeriodicBoundaryXD/YD (LSSolver.h:426-447); z applies the same rule. 0 removes
+ * periodicity (removePeriodicBoundary, LSSolver.h:459-464). */
+int lsdem_set_periodic(lsdem_solver* s, int axes);
+
+/* Uploads the model and builds the grids for the domain [min, max)
+ * (LSSolver::upload + checkSolverInput, LSSolver.h:566-623). */
+int lsdem_initialize(lsdem_solver* s, const double* min3, const double* max3, const double* gravity3);
+
+/* Advances nsteps time steps of size dt (loop body of LSSolver::compute*, LSSolver.h:1000-1128):
+ * half kick, drift, hash, narrowphase + contact forces, periodic images, bonds,
+ * hook, half kick. No host synchronisation inside a batch of steps. */
+int lsdem_step(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user);
+
+/* When on, the last step of every lsdem_step call also records contact point,
+ * normal, overlap and elastic energies (needed for output and bond creation). */
+int lsdem_set_record_contacts(lsdem_solver* s, int on);
+/* Capacities: per-particle candidate slots (particles, walls, ghosts), contact
+ * list, steps per batch. Values <= 0 keep the current setting. */
+int lsdem_set_capacity(lsdem_solver* s, int pp_slots, int wall_slots, int ghost_slots, long long contacts,
+                       int batch_steps);
+
+/* Sizes: 0 particles, 1 walls, 2 bonds, 3 surface nodes, 4 shapes, 5 grid cells,
+ * 6 steps taken, 7 overflow re-runs so far. */
+long long lsdem_num(const lsdem_solver* s, int what);
+double lsdem_time(const lsdem_solver* s);
+
+/* Particle state in particle order (nullable outputs are skipped). Synchronous. */
+int lsdem_get_state(lsdem_solver* s, double* pos, double* vel, double* angvel, double* quat, double* force,
+                    double* torque);
+int lsdem_get_wall_state(lsdem_solver* s, double* pos, double* vel, double* angvel, double* quat);
+/* Overwrites particle state on the device (history is kept). */
+int lsdem_set_state(lsdem_solver* s, const double* pos, const double* vel, const double* angvel, const double* quat);
+/* Per-particle constants: inverse mass, body-frame inverse inertia (6), radius,
+ * kn, ks, mu, e, shape id, scale, grid origin (3), inverse grid spacing, first node id. */
+int lsdem_get_particle_params(const lsdem_solver* s, double* inv_mass, double* inv_inertia6, double* radius,
+                              double* kn, double* ks, double* mu, double* e, int* shape, double* scale,
+                              double* origin3, double* invh, long long* node_base);
+int lsdem_get_wall_params(const lsdem_solver* s, double* radius, double* mu, double* e, int* shape, double* origin3,
+                          double* invh);
+/* Shape template in the caller's node order. */
+int lsdem_get_shape(const lsdem_solver* s, int shape, double* nodes, double* sdf, int* size3, double* origin3,
+                    double* spacing, int* n_nodes);
+
+/* Broadphase of the last step: particle cell keys (-1 outside), stable sorted
+ * particle index and key, per-cell [start, end) or -1 (launchUpdateSpatialGridHashStartEnd,
+ * mySpatialGrid.h:33-49 / buildHashStartEnd.h). Grid: min, max, inverse cell size, cell counts. */
+int lsdem_get_grid(const lsdem_solver* s, double* min3, double* max3, double* inv3, int* size3);
+int lsdem_get_wall_grid(const lsdem_solver* s, double* min3, double* max3, double* inv3, int* size3);
+int lsdem_get_hash(lsdem_solver* s, int* key, int* sorted_idx, int* sorted_key, int* cell_start, int* cell_end);
+
+/* Contacts of the last step of one kind: global surface-node id, partner index
+ * (particle, wall, or the particle whose image was hit), image set (ghosts),
+ * tangential spring; geometry when recorded (nullable outputs skipped).
+ * Order: by owner particle, candidate slot, node. */
+int lsdem_count_contacts(lsdem_solver* s, int kind, long long* n);
+int lsdem_get_contacts(lsdem_solver* s, int kind, long long cap, long long* node, int* partner, int* image,
+                       double* spring, double* point, double* normal, double* overlap, double* en_n, double* en_s);
+
+/* Bond state: master/slave ids, bonded flag, Un, Us, Ub, Ut, max normal and
+ * shear stress, bond point (addBondedForceTorqueKernel outputs). */
+int lsdem_get_bonds(lsdem_solver* s, int* ids2, int* bonded, double* state9);
+
+/* Device pointers (double3 arrays in particle order, AoS) for external-force
+ * kernels: what LSParticle::force()/torque()/velocity()/angularVelocity()
+ * return to the reference's apps (LSParticle.h:665-669). Valid after initialize. */
+int lsdem_device_pointers(lsdem_solver* s, void** force, void** torque, void** vel, void** angvel, void** pos,
+                          void** quat);
+/* The solver's CUDA stream (cudaStream_t). */
+void* lsdem_stream(const lsdem_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

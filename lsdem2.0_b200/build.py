@@ -1,0 +1,76 @@
+"""Builds the CUDA library liblsdem_b200.so (sm_100a) in-tree.
+
+Each .cu under csrc/ is compiled separately (in parallel) and linked into one
+shared library next to this file; the library exports the C ABI declared in
+include/lsdem_b200.h.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
+CSRC = HERE / "csrc"
+OBJ = HERE / "_build"
+LIB = HERE / "liblsdem_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+           "-I", str(ROOT / "include")]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def _stale(src: Path, obj: Path) -> bool:
+    if not obj.exists():
+        return True
+    deps = [src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "lsdem_b200.h"]
+    return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps if d.exists())
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
+    nvcc = _nvcc()
+    OBJ.mkdir(exist_ok=True)
+    srcs = sorted(CSRC.glob("*.cu"))
+    jobs = []
+    for s in srcs:
+        o = OBJ / (s.stem + ".o")
+        if _stale(s, o) or ptxas_info:
+            cmd = [nvcc, *ARCH, *NVFLAGS, "-c", str(s), "-o", str(o)]
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            jobs.append(cmd)
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return cmd, r
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        for cmd, r in ex.map(run, jobs):
+            if verbose or ptxas_info:
+                sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed: {' '.join(cmd)}")
+    objs = [str(OBJ / (s.stem + ".o")) for s in srcs]
+    if jobs or not LIB.exists():
+        cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("link failed")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))

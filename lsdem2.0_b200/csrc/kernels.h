@@ -1,0 +1,153 @@
+// Internal interface between the host runtime and the CUDA kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "common.cuh"
+
+namespace lsdem {
+
+// Compatibility switches for two arithmetic quirks of the reference
+// (both on by default, so results follow the reference):
+//   LSDEM_FIX_GRADIENT: use the true x weight in the SDF gradient instead of the
+//     int-truncated one (LSParticleContactDetectionKernel.cuh:34-52);
+//   LSDEM_FIX_SQRTF: double-precision square roots in the damping terms instead
+//     of sqrtf (contactKernel.cuh:51,53,58).
+enum { FIX_GRADIENT = 1, FIX_SQRTF = 2 };
+
+// Overflow bits of the device status word.
+enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8 };
+
+struct Status {
+  int flags;
+  int need_pp;       // largest per-particle particle-candidate count seen
+  int need_wall;     // largest per-particle wall-candidate count
+  int need_ghost;    // largest per-particle ghost-candidate count
+  int need_contact;  // largest contact total requested
+  int pad[3];
+};
+
+// Shape templates: SDF grid + surface nodes in cluster order.
+struct ShapeView {
+  const int3* gsize;          // per shape
+  const long long* sdf_off;   // per shape, into sdf
+  const double* sdf;          // FP64 SDF store
+  const int* node_off;        // per shape, into node_pos
+  const int* node_cnt;        // per shape
+  const int* cl_off;          // per shape, into cl_sphere
+  const int* cl_cnt;          // per shape
+  const double3* node_pos;    // node store, cluster order, unscaled
+  const int* node_orig;       // original node index within the shape
+  const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
+};
+
+// A set of rigid bodies (particles or walls).
+struct BodyView {
+  int n;
+  double3* pos;
+  double3* vel;
+  double3* angvel;
+  double3* force;
+  double3* torque;
+  Quat* quat;
+  const double* invmass;
+  const Sym6* invI;
+  const double* radius;
+  const double* kn;
+  const double* ks;
+  const double* mu;
+  const double* res;
+  const int* shape;
+  const double* scale;       // uniform template scale
+  const double3* origin;     // grid node (0,0,0) in body frame (scaled)
+  const double* invh;        // inverse grid spacing (scaled)
+  const long long* node_base;  // global id of the first surface node (particles)
+  int* key;                  // cell key of this step, -1 outside the domain
+};
+
+// Per-particle candidate slots of one partner kind, with the contact segment
+// each slot produced.
+struct SlotView {
+  int cap;
+  int* cnt;        // per particle
+  int* id;         // n * cap partner ids
+  int* seg_start;  // n * cap
+  int* seg_cnt;    // n * cap
+};
+
+struct ContactView {
+  int cap;
+  int* count;          // device counter
+  int* node;           // node index within the owner's shape (cluster order)
+  double3* spring;     // tangential spring (FP64 history)
+  double3* point;      // optional geometry (nullptr when not recorded)
+  double3* normal;
+  double* overlap;
+  double* en_n;
+  double* en_s;
+};
+
+// Ghost images of the periodic boundary: up to 7 image sets.
+struct GhostView {
+  int nsets;
+  int mask[7];         // axes of each set (bit 0 x, 1 y, 2 z)
+  double3* gpos;       // nsets * n
+  int* gkey;           // nsets * n, clamped cell or -1
+};
+
+struct BucketScratch {
+  int* counts;
+  int* fill;
+  int* offs;
+  int* scan_tmp;
+  int* big_list;
+  int* big_count;
+  int* tmp;
+};
+
+size_t scan_temp_elems(long long n);
+void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s);
+void scan_i64(const long long* in, long long* out, long long n, long long* tmp, bool inclusive, cudaStream_t s);
+void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorted_idx, int* sorted_key, int* start,
+                 int* end, cudaStream_t s);
+
+struct StepArgs {
+  BodyView P;       // particles
+  BodyView W;       // walls
+  ShapeView S;
+  GridP pg;         // particle grid
+  GridP wg;         // wall grid
+  const int* cell_idx;    // particle grid: sorted particle index
+  const int* cell_start;
+  const int* cell_end;
+  SlotView pp, pw, pgh;          // this step
+  SlotView pp_old, pw_old, pgh_old;  // previous step
+  ContactView C, C_old;
+  GhostView G;
+  Status* status;
+  double dt;
+  double3 gravity;
+  int flags;        // FIX_* bits
+};
+
+void launch_integrate_first(const StepArgs& a, cudaStream_t s);
+void launch_candidates(const StepArgs& a, cudaStream_t s);
+void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s);
+void launch_kick(const StepArgs& a, cudaStream_t s);
+void launch_periodic(const StepArgs& a, int axes, cudaStream_t s);
+void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,
+                             const int* g2_key, cudaStream_t s);
+void launch_clamped_keys(const StepArgs& a, int* key2, cudaStream_t s);
+
+// V-bonds.
+struct BondView {
+  int n;
+  const int* ids;        // 2 per bond: master, slave
+  const double* B;       // 4 per bond
+  const double* geo;     // 5 per bond: radius, L0, tensile, cohesion, mu
+  const double3* frames; // 8 per bond: master n1,n2,n3,pos, slave n1,n2,n3,pos
+  int* bonded;
+  double* state;         // 9 per bond: Un, Us, Ub, Ut, sigma_max, tau_max, point xyz
+};
+void launch_bonds(const StepArgs& a, const BondView& b, cudaStream_t s);
+
+}  // namespace lsdem

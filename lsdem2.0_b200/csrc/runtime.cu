@@ -1,0 +1,1389 @@
+// Host runtime and C ABI of the B200 level-set DEM step.
+//
+// Owns the model (shape templates, particles, walls, bonds), the device
+// buffers and the step loop. The step loop runs in batches: the state at the
+// start of a batch is copied aside, the batch is launched without any host
+// synchronisation, and one status word is read back at the end. If a
+// capacity (candidate slots, contact list) overflowed anywhere in the batch,
+// buffers grow to the recorded need and the batch is re-run from the copy.
+// This replaces the reference's per-list device-to-host count read and
+// stream synchronisation every step (FunDEM/kernel/SolidInteraction.h:104-121).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
+#include "../../include/lsdem_b200.h"
+#include "kernels.h"
+
+using namespace lsdem;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Device array owner.
+template <class T>
+struct DArr {
+  T* p = nullptr;
+  size_t n = 0;
+  DArr() = default;
+  DArr(const DArr&) = delete;
+  DArr& operator=(const DArr&) = delete;
+  ~DArr() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t m) {
+    release();
+    if (m == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)&p, m * sizeof(T));
+    if (e == cudaSuccess) n = m;
+    else p = nullptr;
+    return e;
+  }
+  cudaError_t upload(const T* h, size_t m, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (m != n || !p) e = alloc(m);
+    if (e != cudaSuccess || m == 0) return e;
+    return cudaMemcpyAsync(p, h, m * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+  cudaError_t zero(cudaStream_t s) { return n ? cudaMemsetAsync(p, 0, n * sizeof(T), s) : cudaSuccess; }
+};
+
+struct Fail {
+  int code;
+  std::string msg;
+};
+#define CK(x)                                                                                    \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess)                                                                       \
+      throw Fail{e_ == cudaErrorMemoryAllocation ? LSDEM_ERR_NOMEM : LSDEM_ERR_CUDA,             \
+                 std::string(#x) + ": " + cudaGetErrorString(e_)};                               \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Host-side helpers (same arithmetic as the reference host code).
+struct V3 { double x, y, z; };
+inline V3 v3(const double* p) { return V3{p[0], p[1], p[2]}; }
+inline double hlen(V3 v) { return std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); }
+inline void qnormalize(const double* q, double* out) {
+  double l2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  if (std::fabs(l2) <= 1.0e-20) { for (int a = 0; a < 4; ++a) out[a] = q[a]; return; }
+  double inv = 1.0 / std::sqrt(l2);
+  for (int a = 0; a < 4; ++a) out[a] = q[a] * inv;
+}
+inline V3 hrotate(const double* q, V3 v) {  // rotateVectorByQuaternion
+  V3 qv{q[1], q[2], q[3]};
+  auto cr = [](V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; };
+  V3 t = cr(qv, v);
+  t = V3{t.x * 2.0, t.y * 2.0, t.z * 2.0};
+  V3 u = cr(qv, t);
+  V3 a{v.x + t.x * q[0], v.y + t.y * q[0], v.z + t.z * q[0]};
+  return V3{a.x + u.x, a.y + u.y, a.z + u.z};
+}
+inline V3 hrotate_inv(V3 v, const double* q) {  // reverseRotateVectorByQuaternion
+  double c[4] = {q[0], -q[1], -q[2], -q[3]};
+  return hrotate(c, v);
+}
+inline V3 hnormalize(V3 v) {
+  double l2 = v.x * v.x + v.y * v.y + v.z * v.z;
+  if (std::fabs(l2) <= 1.0e-20) return V3{0, 0, 0};
+  double inv = 1.0 / std::sqrt(l2);
+  return V3{v.x * inv, v.y * inv, v.z * inv};
+}
+inline V3 hcross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+inline int lin3h(int x, int y, int z, int nx, int ny) { return z * ny * nx + y * nx + x; }
+
+// Mass properties by smoothed Heaviside integration (LSSolver.h:66-135).
+void mass_props(const double* sdf, const int* sz, const double* o, double h, double density, double* out) {
+  auto H = [](double phi, double eps) -> double {
+    if (eps <= 0.0) return (phi > 0.0) ? 0.0 : 1.0;
+    if (phi < -eps) return 1.0;
+    if (phi > eps) return 0.0;
+    const double x = -phi / eps;
+    return 0.5 * (1.0 + x + std::sin(M_PI * x) / M_PI);
+  };
+  const int nx = sz[0], ny = sz[1], nz = sz[2];
+  double mass = 0.;
+  const double mg = density * h * h * h;
+  for (int x = 0; x < nx; x++)
+    for (int y = 0; y < ny; y++)
+      for (int z = 0; z < nz; z++) mass += H(sdf[lin3h(x, y, z, nx, ny)] / h, 1.5);
+  mass *= mg;
+  double c[3] = {0, 0, 0};
+  double I[6] = {0, 0, 0, 0, 0, 0};
+  if (mass > 0.) {
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        for (int z = 0; z < nz; z++) {
+          const double Hv = H(sdf[lin3h(x, y, z, nx, ny)] / h, 1.5);
+          c[0] += Hv * (o[0] + double(x) * h);
+          c[1] += Hv * (o[1] + double(y) * h);
+          c[2] += Hv * (o[2] + double(z) * h);
+        }
+    const double f = mg / mass;
+    c[0] *= f; c[1] *= f; c[2] *= f;
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        for (int z = 0; z < nz; z++) {
+          const double Hv = H(sdf[lin3h(x, y, z, nx, ny)] / h, 1.5);
+          const double rx = o[0] + h * double(x) - c[0];
+          const double ry = o[1] + h * double(y) - c[1];
+          const double rz = o[2] + h * double(z) - c[2];
+          I[0] += Hv * (ry * ry + rz * rz) * mg;
+          I[1] += Hv * (rx * rx + rz * rz) * mg;
+          I[2] += Hv * (ry * ry + rx * rx) * mg;
+          I[3] -= Hv * rx * ry * mg;
+          I[4] -= Hv * rx * rz * mg;
+          I[5] -= Hv * ry * rz * mg;
+        }
+  }
+  // inverse (myMat.h:163-195)
+  double inv[6] = {0, 0, 0, 0, 0, 0};
+  if (mass > 0.) {
+    const double xx = I[0], yy = I[1], zz = I[2], xy = I[3], xz = I[4], yz = I[5];
+    const double det = xx * (yy * zz - yz * yz) + xy * (yz * xz - xy * zz) + xz * (xy * yz - yy * xz);
+    if (!(std::fabs(det) < 1e-30)) {
+      const double di = 1.0 / det;
+      inv[0] = (yy * zz - yz * yz) * di;
+      inv[1] = (xx * zz - xz * xz) * di;
+      inv[2] = (xx * yy - xy * xy) * di;
+      inv[3] = -(xy * zz - xz * yz) * di;
+      inv[4] = (xy * yz - xz * yy) * di;
+      inv[5] = -(xx * yz - xz * xy) * di;
+    }
+  }
+  out[0] = mass;
+  for (int a = 0; a < 3; ++a) out[1 + a] = c[a];
+  for (int a = 0; a < 6; ++a) out[4 + a] = I[a];
+  for (int a = 0; a < 6; ++a) out[10 + a] = inv[a];
+}
+
+void sym_inverse(const double* A, double* inv) {
+  const double xx = A[0], yy = A[1], zz = A[2], xy = A[3], xz = A[4], yz = A[5];
+  const double det = xx * (yy * zz - yz * yz) + xy * (yz * xz - xy * zz) + xz * (xy * yz - yy * xz);
+  for (int a = 0; a < 6; ++a) inv[a] = 0.;
+  if (std::fabs(det) < 1e-30) return;
+  const double di = 1.0 / det;
+  inv[0] = (yy * zz - yz * yz) * di;
+  inv[1] = (xx * zz - xz * xz) * di;
+  inv[2] = (xx * yy - xy * xy) * di;
+  inv[3] = -(xy * zz - xz * yz) * di;
+  inv[4] = (xy * yz - xz * yy) * di;
+  inv[5] = -(xx * yz - xz * xy) * di;
+}
+
+uint64_t fnv(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* p = (const unsigned char*)data;
+  for (size_t i = 0; i < bytes; ++i) { h ^= p[i]; h *= 1099511628211ull; }
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+struct ShapeHost {
+  std::vector<double> nodes;  // caller order, 3 per node
+  std::vector<double> sdf;
+  int size[3];
+  double origin[3];
+  double h;
+  std::vector<int> perm;      // cluster position -> caller index
+  std::vector<double> cl;     // 4 per cluster
+  uint64_t hash;
+};
+
+// Orders nodes along a Morton curve so that runs of 32 consecutive nodes are
+// spatially compact, and bounds each run by a sphere.
+void build_clusters(ShapeHost& s) {
+  const int M = (int)(s.nodes.size() / 3);
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < M; ++i)
+    for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], s.nodes[3 * i + a]); hi[a] = std::max(hi[a], s.nodes[3 * i + a]); }
+  auto spread = [](uint32_t v) {
+    uint64_t x = v & 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+  };
+  std::vector<std::pair<uint64_t, int>> key(M);
+  for (int i = 0; i < M; ++i) {
+    uint64_t code = 0;
+    for (int a = 0; a < 3; ++a) {
+      double ext = hi[a] - lo[a];
+      double t = ext > 0 ? (s.nodes[3 * i + a] - lo[a]) / ext : 0.0;
+      uint32_t q = (uint32_t)std::min(1023.0, std::max(0.0, t * 1023.0));
+      code |= spread(q) << a;
+    }
+    key[i] = {code, i};
+  }
+  std::stable_sort(key.begin(), key.end());
+  s.perm.resize(M);
+  for (int i = 0; i < M; ++i) s.perm[i] = key[i].second;
+  const int ncl = (M + 31) / 32;
+  s.cl.assign(4 * (size_t)ncl, 0.0);
+  for (int c = 0; c < ncl; ++c) {
+    const int b = c * 32, e = std::min(M, b + 32);
+    double m[3] = {0, 0, 0};
+    for (int k = b; k < e; ++k)
+      for (int a = 0; a < 3; ++a) m[a] += s.nodes[3 * s.perm[k] + a];
+    for (int a = 0; a < 3; ++a) m[a] /= (e - b);
+    double r = 0;
+    for (int k = b; k < e; ++k) {
+      const double* p = &s.nodes[3 * s.perm[k]];
+      r = std::max(r, std::sqrt((p[0] - m[0]) * (p[0] - m[0]) + (p[1] - m[1]) * (p[1] - m[1]) +
+                                (p[2] - m[2]) * (p[2] - m[2])));
+    }
+    s.cl[4 * c] = m[0]; s.cl[4 * c + 1] = m[1]; s.cl[4 * c + 2] = m[2];
+    s.cl[4 * c + 3] = r * (1.0 + 1e-12) + 1e-300;
+  }
+}
+
+struct BodyHost {
+  std::vector<double> pos, vel, angvel, quat, invm, invI, radius, kn, ks, mu, res, scale, origin, invh;
+  std::vector<int> shape;
+  std::vector<long long> node_base;
+  int n() const { return (int)shape.size(); }
+};
+
+struct BodyDev {
+  DArr<double3> pos, vel, angvel, force, torque, origin;
+  DArr<Quat> quat;
+  DArr<double> invm, radius, kn, ks, mu, res, scale, invh;
+  DArr<Sym6> invI;
+  DArr<int> shape, key;
+  DArr<long long> node_base;
+};
+
+struct SlotsDev {
+  int cap = 0;
+  DArr<int> cnt, id, seg_start, seg_cnt;
+};
+
+struct ContactsDev {
+  long long cap = 0;
+  DArr<int> count, node;
+  DArr<double3> spring, point, normal;
+  DArr<double> overlap, en_n, en_s;
+  bool geom = false;
+};
+
+struct BondHost {
+  std::vector<int> ids, bonded;
+  std::vector<double> B, geo, frames, state;
+};
+
+}  // namespace
+
+struct lsdem_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int flags = 0;
+  std::string err;
+  // model
+  std::vector<ShapeHost> shapes;
+  std::unordered_map<uint64_t, std::vector<int>> shape_by_hash;
+  std::map<std::pair<int, uint64_t>, double> radius_cache;  // (shape, scale bits) -> radius
+  BodyHost P, W;
+  BondHost bonds;
+  int periodic = 0;
+  double dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0}, grav[3] = {0, 0, 0};
+  // device
+  bool ready = false;
+  BodyDev dP, dW;
+  DArr<int3> s_gsize;
+  DArr<long long> s_sdf_off;
+  DArr<double> s_sdf;
+  DArr<int> s_node_off, s_node_cnt, s_cl_off, s_cl_cnt, s_node_orig;
+  DArr<double3> s_node_pos;
+  DArr<double4> s_cl;
+  std::vector<int> h_node_off, h_cl_off;
+  GridP pg{}, wg{};
+  DArr<int> cell_idx, cell_start, cell_end, sorted_key;
+  DArr<int> bk_counts, bk_fill, bk_offs, bk_scan, bk_big, bk_bigc, bk_tmp;
+  SlotsDev slots[2][3];      // [history parity][kind]
+  ContactsDev con[2];
+  int hp = 0;                // parity of the last completed step's history
+  int cap_pp = 32, cap_w = 4, cap_g = 16;
+  long long cap_c = 0;
+  int batch = 16;
+  bool record = false;
+  // periodic
+  int nsets = 0;
+  int set_mask[7] = {0};
+  DArr<double3> gpos;
+  DArr<int> gkey, key2, g2_idx, g2_start, g2_end;
+  // bonds
+  DArr<int> b_ids, b_bonded;
+  DArr<double> b_B, b_geo, b_state;
+  DArr<double3> b_frames;
+  // status + backup
+  DArr<Status> status;
+  Status* h_status = nullptr;
+  int* h_count = nullptr;
+  DArr<double3> bk_pos, bk_vel, bk_angvel, bk_force, bk_torque, bk_wpos;
+  DArr<Quat> bk_quat, bk_wquat;
+  DArr<int> bk_bonded, bk_slot[3][4], bk_cnode;
+  DArr<double3> bk_cspring;
+  int bk_cap[3] = {0, 0, 0};
+  long long hist_count = 0;  // contacts in the history buffer hp
+  long long steps = 0, reruns = 0;
+  double time = 0.0;
+
+  ~lsdem_solver() {
+    if (h_status) cudaFreeHost(h_status);
+    if (h_count) cudaFreeHost(h_count);
+  }
+};
+
+namespace {
+
+int fail(lsdem_solver* s, int code, const std::string& m) {
+  if (s) s->err = m;
+  return code;
+}
+
+template <class F>
+int guard(lsdem_solver* s, F&& f) {
+  try {
+    return f();
+  } catch (const Fail& e) {
+    return fail(s, e.code, e.msg);
+  } catch (const std::exception& e) {
+    return fail(s, LSDEM_ERR_ARG, e.what());
+  }
+}
+
+int add_shape_impl(lsdem_solver* s, const double* nodes, int nn, const double* sdf, const int* sz, const double* o,
+                   double h) {
+  if (sz[0] < 2 || sz[1] < 2 || sz[2] < 2) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid size (must be >= 2 per axis)"};
+  if (!(h > 0.0)) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid spacing (must be > 0)"};
+  if (nn < 0 || nn > 256 * 32) throw Fail{LSDEM_ERR_ARG, "Invalid surface node count (0..8192)"};
+  const size_t ng = (size_t)sz[0] * sz[1] * sz[2];
+  uint64_t hsh = fnv(nodes, sizeof(double) * 3 * (size_t)nn);
+  hsh = fnv(sdf, sizeof(double) * ng, hsh);
+  hsh = fnv(sz, sizeof(int) * 3, hsh);
+  hsh = fnv(o, sizeof(double) * 3, hsh);
+  hsh = fnv(&h, sizeof(double), hsh);
+  auto it = s->shape_by_hash.find(hsh);
+  if (it != s->shape_by_hash.end()) {
+    for (int id : it->second) {
+      const ShapeHost& e = s->shapes[id];
+      if (e.nodes.size() == 3 * (size_t)nn && e.sdf.size() == ng && e.size[0] == sz[0] && e.size[1] == sz[1] &&
+          e.size[2] == sz[2] && e.origin[0] == o[0] && e.origin[1] == o[1] && e.origin[2] == o[2] && e.h == h &&
+          std::memcmp(e.nodes.data(), nodes, sizeof(double) * 3 * (size_t)nn) == 0 &&
+          std::memcmp(e.sdf.data(), sdf, sizeof(double) * ng) == 0)
+        return id;
+    }
+  }
+  ShapeHost sh;
+  sh.nodes.assign(nodes, nodes + 3 * (size_t)nn);
+  sh.sdf.assign(sdf, sdf + ng);
+  for (int a = 0; a < 3; ++a) { sh.size[a] = sz[a]; sh.origin[a] = o[a]; }
+  sh.h = h;
+  sh.hash = hsh;
+  build_clusters(sh);
+  s->shapes.push_back(std::move(sh));
+  const int id = (int)s->shapes.size() - 1;
+  s->shape_by_hash[hsh].push_back(id);
+  s->ready = false;
+  return id;
+}
+
+// radius = max |scale * node| over the body's nodes (LSParticle.h:175-181).
+double shape_radius(lsdem_solver* s, int shape, double scale) {
+  uint64_t bits;
+  std::memcpy(&bits, &scale, 8);
+  auto key = std::make_pair(shape, bits);
+  auto it = s->radius_cache.find(key);
+  if (it != s->radius_cache.end()) return it->second;
+  const ShapeHost& sh = s->shapes[shape];
+  double r = 0.;
+  for (size_t i = 0; i < sh.nodes.size() / 3; ++i) {
+    V3 p{scale * sh.nodes[3 * i], scale * sh.nodes[3 * i + 1], scale * sh.nodes[3 * i + 2]};
+    r = std::max(hlen(p), r);
+  }
+  s->radius_cache[key] = r;
+  return r;
+}
+
+void push_body(lsdem_solver* s, BodyHost& B, int shape, double scale, const double* pos, const double* vel,
+               const double* angvel, const double* quat, double invm, const double* invI, double kn, double ks,
+               double mu, double e, double radius) {
+  const ShapeHost& sh = s->shapes[shape];
+  for (int a = 0; a < 3; ++a) {
+    B.pos.push_back(pos[a]);
+    B.vel.push_back(vel ? vel[a] : 0.);
+    B.angvel.push_back(angvel ? angvel[a] : 0.);
+    B.origin.push_back(scale == 1.0 ? sh.origin[a] : scale * sh.origin[a]);
+  }
+  double q[4];
+  qnormalize(quat, q);
+  for (int a = 0; a < 4; ++a) B.quat.push_back(q[a]);
+  B.invm.push_back(invm);
+  for (int a = 0; a < 6; ++a) B.invI.push_back(invI ? invI[a] : 0.);
+  B.radius.push_back(radius);
+  B.kn.push_back(kn > 0. ? kn : 0.);
+  B.ks.push_back(ks > 0. ? ks : 0.);
+  B.mu.push_back(mu > 0. ? mu : 0.);
+  double ee = e;
+  if (ee <= 0.0 || ee > 1.0) ee = 1.0;
+  B.res.push_back(ee);
+  B.scale.push_back(scale);
+  B.invh.push_back(1. / (scale == 1.0 ? sh.h : scale * sh.h));
+  B.shape.push_back(shape);
+}
+
+// ---------------------------------------------------------------------------
+// Device set-up.
+void alloc_slots(lsdem_solver* s) {
+  const int n = s->P.n();
+  const int caps[3] = {s->cap_pp, s->P.n() ? s->cap_w : 0, s->cap_g};
+  for (int h = 0; h < 2; ++h)
+    for (int k = 0; k < 3; ++k) {
+      SlotsDev& sl = s->slots[h][k];
+      const int cap = (k == 1 && s->W.n() == 0) ? 0 : caps[k];
+      if (k == 2 && s->nsets == 0) {
+        sl.cap = 0;
+        sl.cnt.release(); sl.id.release(); sl.seg_start.release(); sl.seg_cnt.release();
+        continue;
+      }
+      sl.cap = cap;
+      CK(sl.cnt.alloc((size_t)std::max(n, 1)));
+      CK(sl.cnt.zero(s->stream));
+      const size_t m = (size_t)std::max(n, 1) * std::max(cap, 1);
+      CK(sl.id.alloc(m));
+      CK(sl.seg_start.alloc(m));
+      CK(sl.seg_cnt.alloc(m));
+      CK(sl.seg_cnt.zero(s->stream));
+    }
+}
+
+void alloc_contacts(lsdem_solver* s, ContactsDev& c, long long cap) {
+  c.cap = cap;
+  CK(c.count.alloc(1));
+  CK(c.count.zero(s->stream));
+  CK(c.node.alloc((size_t)std::max(cap, 1LL)));
+  CK(c.spring.alloc((size_t)std::max(cap, 1LL)));
+  c.point.release(); c.normal.release(); c.overlap.release(); c.en_n.release(); c.en_s.release();
+  c.geom = false;
+}
+
+void ensure_geom(lsdem_solver* s, ContactsDev& c) {
+  if (c.geom) return;
+  const size_t m = (size_t)std::max(c.cap, 1LL);
+  CK(c.point.alloc(m));
+  CK(c.normal.alloc(m));
+  CK(c.overlap.alloc(m));
+  CK(c.en_n.alloc(m));
+  CK(c.en_s.alloc(m));
+  c.geom = true;
+}
+
+void upload_bodies(lsdem_solver* s, BodyHost& H, BodyDev& D) {
+  const size_t n = (size_t)H.n();
+  cudaStream_t st = s->stream;
+  CK(D.pos.upload((const double3*)H.pos.data(), n, st));
+  CK(D.vel.upload((const double3*)H.vel.data(), n, st));
+  CK(D.angvel.upload((const double3*)H.angvel.data(), n, st));
+  CK(D.force.alloc(n)); CK(D.force.zero(st));
+  CK(D.torque.alloc(n)); CK(D.torque.zero(st));
+  CK(D.origin.upload((const double3*)H.origin.data(), n, st));
+  CK(D.quat.upload((const Quat*)H.quat.data(), n, st));
+  CK(D.invm.upload(H.invm.data(), n, st));
+  CK(D.invI.upload((const Sym6*)H.invI.data(), n, st));
+  CK(D.radius.upload(H.radius.data(), n, st));
+  CK(D.kn.upload(H.kn.data(), n, st));
+  CK(D.ks.upload(H.ks.data(), n, st));
+  CK(D.mu.upload(H.mu.data(), n, st));
+  CK(D.res.upload(H.res.data(), n, st));
+  CK(D.scale.upload(H.scale.data(), n, st));
+  CK(D.invh.upload(H.invh.data(), n, st));
+  CK(D.shape.upload(H.shape.data(), n, st));
+  CK(D.key.alloc(std::max<size_t>(n, 1)));
+  if (!H.node_base.empty()) CK(D.node_base.upload(H.node_base.data(), n, st));
+}
+
+void set_grid(GridP& g, const double* mn, const double* mx_in, double cell) {  // spatialGrid::set
+  double mx[3] = {mx_in[0], mx_in[1], mx_in[2]};
+  for (int a = 0; a < 3; ++a)
+    if (mx[a] <= mn[a]) mx[a] = mn[a] + cell;
+  int size[3] = {2, 2, 2};
+  double inv[3] = {0, 0, 0};
+  if (!(std::fabs(cell) <= 1.0e-20)) {
+    for (int a = 0; a < 3; ++a) {
+      const double d = mx[a] - mn[a];
+      size[a] = d > 2. * cell ? int(d / cell) : 2;
+      inv[a] = (d > 0.0) ? (double(size[a]) / d) : 0.0;
+    }
+  }
+  g.mn = make_double3(mn[0], mn[1], mn[2]);
+  g.mx = make_double3(mx[0], mx[1], mx[2]);
+  g.inv = make_double3(inv[0], inv[1], inv[2]);
+  g.size = make_int3(size[0], size[1], size[2]);
+  g.ncells = size[0] * size[1] * size[2];
+}
+
+void alloc_bucket(lsdem_solver* s, int n, int ncells) {
+  const int nb = ncells + 2;
+  CK(s->bk_counts.alloc(nb + 1));
+  CK(s->bk_fill.alloc(nb + 1));
+  CK(s->bk_offs.alloc(nb + 1));
+  CK(s->bk_scan.alloc(scan_temp_elems(nb + 1)));
+  CK(s->bk_big.alloc((size_t)n / 65 + 1));
+  CK(s->bk_bigc.alloc(1));
+  CK(s->bk_tmp.alloc((size_t)std::max(n, 1)));
+}
+
+void initialize(lsdem_solver* s) {
+  CK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  // shapes
+  std::vector<int3> gs;
+  std::vector<long long> sdf_off;
+  std::vector<double> sdf;
+  std::vector<int> node_off, node_cnt, cl_off, cl_cnt, node_orig;
+  std::vector<double3> node_pos;
+  std::vector<double4> cl;
+  for (const ShapeHost& sh : s->shapes) {
+    gs.push_back(make_int3(sh.size[0], sh.size[1], sh.size[2]));
+    sdf_off.push_back((long long)sdf.size());
+    sdf.insert(sdf.end(), sh.sdf.begin(), sh.sdf.end());
+    node_off.push_back((int)node_pos.size());
+    const int M = (int)sh.perm.size();
+    node_cnt.push_back(M);
+    for (int k = 0; k < M; ++k) {
+      const double* p = &sh.nodes[3 * sh.perm[k]];
+      node_pos.push_back(make_double3(p[0], p[1], p[2]));
+      node_orig.push_back(sh.perm[k]);
+    }
+    cl_off.push_back((int)cl.size());
+    cl_cnt.push_back((int)(sh.cl.size() / 4));
+    for (size_t c = 0; c < sh.cl.size() / 4; ++c)
+      cl.push_back(make_double4(sh.cl[4 * c], sh.cl[4 * c + 1], sh.cl[4 * c + 2], sh.cl[4 * c + 3]));
+  }
+  s->h_node_off = node_off;
+  s->h_cl_off = cl_off;
+  CK(s->s_gsize.upload(gs.data(), gs.size(), st));
+  CK(s->s_sdf_off.upload(sdf_off.data(), sdf_off.size(), st));
+  CK(s->s_sdf.upload(sdf.data(), sdf.size(), st));
+  CK(s->s_node_off.upload(node_off.data(), node_off.size(), st));
+  CK(s->s_node_cnt.upload(node_cnt.data(), node_cnt.size(), st));
+  CK(s->s_cl_off.upload(cl_off.data(), cl_off.size(), st));
+  CK(s->s_cl_cnt.upload(cl_cnt.data(), cl_cnt.size(), st));
+  CK(s->s_node_pos.upload(node_pos.data(), node_pos.size(), st));
+  CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
+  CK(s->s_cl.upload(cl.data(), cl.size(), st));
+  // node ids (LSBoundaryNode order: particle by particle, caller node order)
+  s->P.node_base.resize(s->P.n());
+  long long nb = 0;
+  for (int i = 0; i < s->P.n(); ++i) {
+    s->P.node_base[i] = nb;
+    nb += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3);
+  }
+  upload_bodies(s, s->P, s->dP);
+  upload_bodies(s, s->W, s->dW);
+  // grids: cell = 2 x max bounding radius (LSParticle.h:241-256)
+  double rp = 0., rw = 0.;
+  for (double r : s->P.radius) rp = std::max(rp, r);
+  for (double r : s->W.radius) rw = std::max(rw, r);
+  set_grid(s->pg, s->dmin, s->dmax, s->P.n() ? 2.0 * rp : 0.0);
+  set_grid(s->wg, s->dmin, s->dmax, s->W.n() ? 2.0 * rw : 0.0);
+  const int n = s->P.n();
+  CK(s->cell_idx.alloc(std::max(n, 1)));
+  CK(s->sorted_key.alloc(std::max(n, 1)));
+  CK(s->cell_start.alloc(s->pg.ncells));
+  CK(s->cell_end.alloc(s->pg.ncells));
+  alloc_bucket(s, n, s->pg.ncells);
+  // periodic image sets: single axes in x, y, z order, then pairs, then xyz
+  s->nsets = 0;
+  const int ax = s->periodic;
+  const int order[7] = {1, 2, 4, 3, 5, 6, 7};
+  for (int k = 0; k < 7; ++k)
+    if ((order[k] & ax) == order[k]) s->set_mask[s->nsets++] = order[k];
+  if (s->nsets > 0) {
+    CK(s->gpos.alloc((size_t)s->nsets * std::max(n, 1)));
+    CK(s->gkey.alloc((size_t)s->nsets * std::max(n, 1)));
+    CK(s->key2.alloc(std::max(n, 1)));
+    CK(s->g2_idx.alloc(std::max(n, 1)));
+    CK(s->g2_start.alloc(s->pg.ncells));
+    CK(s->g2_end.alloc(s->pg.ncells));
+  }
+  // history buffers
+  if (s->cap_c <= 0) s->cap_c = std::max<long long>(1 << 16, (long long)n * 64);
+  alloc_slots(s);
+  alloc_contacts(s, s->con[0], s->cap_c);
+  alloc_contacts(s, s->con[1], s->cap_c);
+  s->hp = 0;
+  s->hist_count = 0;
+  // bonds
+  const size_t nbnd = s->bonds.bonded.size();
+  if (nbnd) {
+    CK(s->b_ids.upload(s->bonds.ids.data(), s->bonds.ids.size(), st));
+    CK(s->b_bonded.upload(s->bonds.bonded.data(), nbnd, st));
+    CK(s->b_B.upload(s->bonds.B.data(), s->bonds.B.size(), st));
+    CK(s->b_geo.upload(s->bonds.geo.data(), s->bonds.geo.size(), st));
+    CK(s->b_frames.upload((const double3*)s->bonds.frames.data(), s->bonds.frames.size() / 3, st));
+    CK(s->b_state.upload(s->bonds.state.data(), s->bonds.state.size(), st));
+  }
+  CK(s->status.alloc(1));
+  CK(s->status.zero(st));
+  if (!s->h_status) CK(cudaMallocHost((void**)&s->h_status, sizeof(Status)));
+  if (!s->h_count) CK(cudaMallocHost((void**)&s->h_count, sizeof(int)));
+  CK(cudaStreamSynchronize(st));
+  s->ready = true;
+}
+
+StepArgs make_args(lsdem_solver* s, double dt) {
+  StepArgs a{};
+  auto bv = [&](BodyDev& D, int n) {
+    BodyView v;
+    v.n = n;
+    v.pos = D.pos.p; v.vel = D.vel.p; v.angvel = D.angvel.p; v.force = D.force.p; v.torque = D.torque.p;
+    v.quat = D.quat.p; v.invmass = D.invm.p; v.invI = D.invI.p; v.radius = D.radius.p; v.kn = D.kn.p;
+    v.ks = D.ks.p; v.mu = D.mu.p; v.res = D.res.p; v.shape = D.shape.p; v.scale = D.scale.p;
+    v.origin = D.origin.p; v.invh = D.invh.p; v.node_base = D.node_base.p; v.key = D.key.p;
+    return v;
+  };
+  a.P = bv(s->dP, s->P.n());
+  a.W = bv(s->dW, s->W.n());
+  a.S.gsize = s->s_gsize.p; a.S.sdf_off = s->s_sdf_off.p; a.S.sdf = s->s_sdf.p;
+  a.S.node_off = s->s_node_off.p; a.S.node_cnt = s->s_node_cnt.p; a.S.cl_off = s->s_cl_off.p;
+  a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
+  a.S.cl_sphere = s->s_cl.p;
+  a.pg = s->pg;
+  a.wg = s->wg;
+  a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
+  auto sv = [](SlotsDev& d) {
+    SlotView v;
+    v.cap = d.cap; v.cnt = d.cnt.p; v.id = d.id.p; v.seg_start = d.seg_start.p; v.seg_cnt = d.seg_cnt.p;
+    return v;
+  };
+  const int cur = 1 - s->hp, old = s->hp;
+  a.pp = sv(s->slots[cur][0]); a.pw = sv(s->slots[cur][1]); a.pgh = sv(s->slots[cur][2]);
+  a.pp_old = sv(s->slots[old][0]); a.pw_old = sv(s->slots[old][1]); a.pgh_old = sv(s->slots[old][2]);
+  auto cv = [](ContactsDev& c, bool geom) {
+    ContactView v;
+    v.cap = (int)std::min<long long>(c.cap, 0x7fffffff);
+    v.count = c.count.p; v.node = c.node.p; v.spring = c.spring.p;
+    v.point = geom ? c.point.p : nullptr; v.normal = geom ? c.normal.p : nullptr;
+    v.overlap = geom ? c.overlap.p : nullptr; v.en_n = geom ? c.en_n.p : nullptr; v.en_s = geom ? c.en_s.p : nullptr;
+    return v;
+  };
+  a.C = cv(s->con[cur], false);
+  a.C_old = cv(s->con[old], false);
+  a.G.nsets = s->nsets;
+  for (int k = 0; k < 7; ++k) a.G.mask[k] = s->set_mask[k];
+  a.G.gpos = s->gpos.p;
+  a.G.gkey = s->gkey.p;
+  a.status = s->status.p;
+  a.dt = dt;
+  a.gravity = make_double3(s->grav[0], s->grav[1], s->grav[2]);
+  a.flags = s->flags;
+  return a;
+}
+
+// One time step in the reference order (LSSolver.h:1000-1011, 1104-1128).
+void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* user, double t) {
+  cudaStream_t st = s->stream;
+  StepArgs a = make_args(s, dt);
+  if (record) {
+    ContactsDev& c = s->con[1 - s->hp];
+    ensure_geom(s, c);
+    a.C.point = c.point.p; a.C.normal = c.normal.p; a.C.overlap = c.overlap.p; a.C.en_n = c.en_n.p;
+    a.C.en_s = c.en_s.p;
+  }
+  launch_integrate_first(a, st);
+  BucketScratch w{s->bk_counts.p, s->bk_fill.p, s->bk_offs.p, s->bk_scan.p, s->bk_big.p, s->bk_bigc.p, s->bk_tmp.p};
+  bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st);
+  launch_candidates(a, st);
+  launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st);
+  if (s->nsets > 0) {
+    launch_periodic(a, s->periodic, st);
+    launch_clamped_keys(a, s->key2.p, st);
+    bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
+    launch_ghost_candidates(a, s->g2_idx.p, s->g2_start.p, s->g2_end.p, s->key2.p, st);
+    launch_narrowphase(a, 4, st);
+  }
+  if (!s->bonds.bonded.empty()) {
+    BondView b{(int)s->bonds.bonded.size(), s->b_ids.p, s->b_B.p, s->b_geo.p, s->b_frames.p, s->b_bonded.p,
+               s->b_state.p};
+    launch_bonds(a, b, st);
+  }
+  if (hook) hook(user, t);
+  launch_kick(a, st);
+  CK(cudaGetLastError());
+  s->hp = 1 - s->hp;
+}
+
+// Snapshot of everything a batch may change, taken at the batch start.
+void backup(lsdem_solver* s) {
+  cudaStream_t st = s->stream;
+  const size_t n = (size_t)s->P.n(), nw = (size_t)s->W.n();
+  auto cp = [&](auto& dst, auto& src, size_t m) {
+    if (dst.n < m) CK(dst.alloc(m));
+    if (m) CK(cudaMemcpyAsync(dst.p, src.p, m * sizeof(*src.p), cudaMemcpyDeviceToDevice, st));
+  };
+  cp(s->bk_pos, s->dP.pos, n); cp(s->bk_vel, s->dP.vel, n); cp(s->bk_angvel, s->dP.angvel, n);
+  cp(s->bk_quat, s->dP.quat, n); cp(s->bk_force, s->dP.force, n); cp(s->bk_torque, s->dP.torque, n);
+  cp(s->bk_wpos, s->dW.pos, nw); cp(s->bk_wquat, s->dW.quat, nw);
+  cp(s->bk_bonded, s->b_bonded, s->bonds.bonded.size());
+  for (int k = 0; k < 3; ++k) {
+    SlotsDev& sl = s->slots[s->hp][k];
+    s->bk_cap[k] = sl.cap;
+    if (!sl.cnt.p) continue;
+    cp(s->bk_slot[k][0], sl.cnt, n);
+    cp(s->bk_slot[k][1], sl.id, n * sl.cap);
+    cp(s->bk_slot[k][2], sl.seg_start, n * sl.cap);
+    cp(s->bk_slot[k][3], sl.seg_cnt, n * sl.cap);
+  }
+  const size_t nc = (size_t)s->hist_count;
+  cp(s->bk_cnode, s->con[s->hp].node, nc);
+  cp(s->bk_cspring, s->con[s->hp].spring, nc);
+}
+
+void restore(lsdem_solver* s, int hp0) {
+  cudaStream_t st = s->stream;
+  s->hp = hp0;
+  const size_t n = (size_t)s->P.n(), nw = (size_t)s->W.n();
+  auto cp = [&](auto& dst, auto& src, size_t m) {
+    if (m) CK(cudaMemcpyAsync(dst.p, src.p, m * sizeof(*src.p), cudaMemcpyDeviceToDevice, st));
+  };
+  cp(s->dP.pos, s->bk_pos, n); cp(s->dP.vel, s->bk_vel, n); cp(s->dP.angvel, s->bk_angvel, n);
+  cp(s->dP.quat, s->bk_quat, n); cp(s->dP.force, s->bk_force, n); cp(s->dP.torque, s->bk_torque, n);
+  cp(s->dW.pos, s->bk_wpos, nw); cp(s->dW.quat, s->bk_wquat, nw);
+  cp(s->b_bonded, s->bk_bonded, s->bonds.bonded.size());
+  for (int k = 0; k < 3; ++k) {
+    SlotsDev& sl = s->slots[hp0][k];
+    if (!sl.cnt.p) continue;
+    const int oc = s->bk_cap[k];
+    cp(sl.cnt, s->bk_slot[k][0], n);
+    if (oc > 0 && n > 0) {
+      for (int a = 1; a < 4; ++a) {
+        DArr<int>& dst = a == 1 ? sl.id : (a == 2 ? sl.seg_start : sl.seg_cnt);
+        CK(cudaMemcpy2DAsync(dst.p, sizeof(int) * sl.cap, s->bk_slot[k][a].p, sizeof(int) * oc,
+                             sizeof(int) * std::min(oc, sl.cap), n, cudaMemcpyDeviceToDevice, st));
+      }
+    }
+  }
+  const size_t nc = (size_t)s->hist_count;
+  cp(s->con[hp0].node, s->bk_cnode, nc);
+  cp(s->con[hp0].spring, s->bk_cspring, nc);
+}
+
+// Grows capacities after an overflow. Slot arrays of both parities and both
+// contact lists are reallocated (their contents come back from the backup).
+void grow(lsdem_solver* s, const Status& st) {
+  if (st.flags & OVF_PP) s->cap_pp = std::max(s->cap_pp * 2, st.need_pp + st.need_pp / 4 + 1);
+  if (st.flags & OVF_WALL) s->cap_w = std::max(s->cap_w * 2, st.need_wall + 1);
+  if (st.flags & OVF_GHOST) s->cap_g = std::max(s->cap_g * 2, st.need_ghost + st.need_ghost / 4 + 1);
+  if (st.flags & OVF_CONTACT)
+    s->cap_c = std::max<long long>(s->cap_c * 2, (long long)st.need_contact + st.need_contact / 4 + 1);
+  // history slots must keep the old contents until restore: they are restored from backup
+  alloc_slots(s);
+  if (st.flags & OVF_CONTACT) {
+    const bool g0 = s->con[0].geom, g1 = s->con[1].geom;
+    alloc_contacts(s, s->con[0], s->cap_c);
+    alloc_contacts(s, s->con[1], s->cap_c);
+    if (g0) ensure_geom(s, s->con[0]);
+    if (g1) ensure_geom(s, s->con[1]);
+  }
+}
+
+int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
+  if (!s->ready) throw Fail{LSDEM_ERR_STATE, "lsdem_step before lsdem_initialize"};
+  if (!(dt > 0.)) throw Fail{LSDEM_ERR_ARG, "Invalid timeStep"};
+  cudaStream_t st = s->stream;
+  long long done = 0;
+  while (done < nsteps) {
+    const long long B = std::min<long long>(s->batch, nsteps - done);
+    const int hp0 = s->hp;
+    backup(s);
+    for (int attempt = 0;; ++attempt) {
+      CK(cudaMemsetAsync(s->status.p, 0, sizeof(Status), st));
+      double t = s->time;
+      for (long long k = 0; k < B; ++k) {
+        const bool rec = s->record && (done + k == nsteps - 1);
+        step_once(s, dt, rec, hook, user, t);
+        t += dt;
+      }
+      CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(Status), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(s->h_count, s->con[s->hp].count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      const Status stat = *s->h_status;
+      if (stat.flags == 0) {
+        s->hist_count = *s->h_count;
+        break;
+      }
+      if (attempt > 8) throw Fail{LSDEM_ERR_NOMEM, "capacity growth did not converge"};
+      grow(s, stat);
+      restore(s, hp0);
+      s->reruns++;
+    }
+    done += B;
+    s->steps += B;
+    s->time += dt * (double)B;
+  }
+  return LSDEM_OK;
+}
+
+template <class T>
+std::vector<T> dl(const DArr<T>& d, size_t n, cudaStream_t st) {
+  std::vector<T> h(n);
+  if (n) CK(cudaMemcpyAsync(h.data(), d.p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+  return h;
+}
+
+}  // namespace
+
+namespace {
+// Walks the history buffer of the last step: owner A, slot j, segment.
+template <class F>
+void walk_contacts(lsdem_solver* s, int kind, F&& f) {
+  cudaStream_t st = s->stream;
+  const int n = s->P.n();
+  SlotsDev& sl = s->slots[s->hp][kind];
+  if (!sl.cnt.p || sl.cap == 0) return;
+  auto cnt = dl(sl.cnt, (size_t)n, st);
+  auto id = dl(sl.id, (size_t)n * sl.cap, st);
+  auto ss = dl(sl.seg_start, (size_t)n * sl.cap, st);
+  auto sc = dl(sl.seg_cnt, (size_t)n * sl.cap, st);
+  CK(cudaStreamSynchronize(st));
+  for (int A = 0; A < n; ++A) {
+    const int m = std::min(cnt[A], sl.cap);
+    for (int j = 0; j < m; ++j) {
+      const size_t k = (size_t)A * sl.cap + j;
+      f(A, id[k], ss[k], sc[k]);
+    }
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int lsdem_create(int device, void* stream, lsdem_solver** out) {
+  if (!out) return LSDEM_ERR_ARG;
+  lsdem_solver* s = new lsdem_solver();
+  s->device = device;
+  s->stream = (cudaStream_t)stream;
+  *out = s;
+  return LSDEM_OK;
+}
+
+void lsdem_destroy(lsdem_solver* s) {
+  if (!s) return;
+  if (s->ready) cudaStreamSynchronize(s->stream);
+  delete s;
+}
+
+const char* lsdem_last_error(const lsdem_solver* s) { return s ? s->err.c_str() : "null solver"; }
+
+int lsdem_set_flags(lsdem_solver* s, int flags) {
+  if (!s) return LSDEM_ERR_ARG;
+  s->flags = flags & (FIX_GRADIENT | FIX_SQRTF);
+  return LSDEM_OK;
+}
+
+int lsdem_mass_properties(const double* sdf, const int* size3, const double* origin3, double spacing, double density,
+                          double* out16) {
+  if (!sdf || !size3 || !origin3 || !out16) return LSDEM_ERR_ARG;
+  if (size3[0] < 2 || size3[1] < 2 || size3[2] < 2 || !(spacing > 0.)) return LSDEM_ERR_ARG;
+  mass_props(sdf, size3, origin3, spacing, density, out16);
+  return LSDEM_OK;
+}
+
+int lsdem_add_shape(lsdem_solver* s, const double* nodes, int n_nodes, const double* sdf, const int* size3,
+                    const double* origin3, double spacing, int* shape_id) {
+  if (!s || !sdf || !size3 || !origin3 || (n_nodes > 0 && !nodes)) return fail(s, LSDEM_ERR_ARG, "null argument");
+  return guard(s, [&] {
+    int id = add_shape_impl(s, nodes, n_nodes, sdf, size3, origin3, spacing);
+    if (shape_id) *shape_id = id;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_add_particles(lsdem_solver* s, int n, const int* shape, const double* scale, const double* pos,
+                        const double* vel, const double* angvel, const double* quat, const double* inv_mass,
+                        const double* inv_inertia6, const double* kn, const double* ks, const double* mu,
+                        const double* e, int* first_index) {
+  if (!s || n < 0 || !shape || !pos || !quat || !inv_mass || !kn || !ks || !mu || !e)
+    return fail(s, LSDEM_ERR_ARG, "null argument");
+  return guard(s, [&] {
+    for (int i = 0; i < n; ++i)
+      if (shape[i] < 0 || shape[i] >= (int)s->shapes.size()) throw Fail{LSDEM_ERR_ARG, "unknown shape id"};
+    if (first_index) *first_index = s->P.n();
+    for (int i = 0; i < n; ++i) {
+      const double sc = scale ? scale[i] : 1.0;
+      if (!(sc > 0.)) throw Fail{LSDEM_ERR_ARG, "scale must be > 0"};
+      push_body(s, s->P, shape[i], sc, pos + 3 * i, vel ? vel + 3 * i : nullptr, angvel ? angvel + 3 * i : nullptr,
+                quat + 4 * i, inv_mass[i], inv_inertia6 ? inv_inertia6 + 6 * i : nullptr, kn[i], ks[i], mu[i], e[i],
+                shape_radius(s, shape[i], sc));
+    }
+    s->ready = false;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_add_ls_particle(lsdem_solver* s, const double* nodes, int n_nodes, const double* sdf, const int* size3,
+                          const double* origin3, double spacing, const double* pos, const double* vel,
+                          const double* angvel, const double* quat, double kn, double ks, double mu, double e,
+                          double density, int* index) {
+  if (!s || !sdf || !size3 || !origin3 || !pos || !quat) return fail(s, LSDEM_ERR_ARG, "null argument");
+  return guard(s, [&] {
+    if (size3[0] < 2 || size3[1] < 2 || size3[2] < 2) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid size"};
+    if (!(spacing > 0.)) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid spacing"};
+    double mp[16];
+    mass_props(sdf, size3, origin3, spacing, density, mp);
+    const double mass = mp[0];
+    const double c[3] = {mp[1], mp[2], mp[3]};
+    double qn[4];
+    qnormalize(quat, qn);
+    V3 off = hrotate(qn, V3{c[0], c[1], c[2]});
+    const double pnew[3] = {pos[0] + off.x, pos[1] + off.y, pos[2] + off.z};
+    std::vector<double> nn(3 * (size_t)n_nodes);
+    for (int i = 0; i < n_nodes; ++i)
+      for (int a = 0; a < 3; ++a) nn[3 * i + a] = nodes[3 * i + a] - c[a];
+    const double onew[3] = {origin3[0] - c[0], origin3[1] - c[1], origin3[2] - c[2]};
+    const int sh = add_shape_impl(s, nn.data(), n_nodes, sdf, size3, onew, spacing);
+    if (index) *index = s->P.n();
+    const double invm = mass > 0. ? 1. / mass : 0.;
+    push_body(s, s->P, sh, 1.0, pnew, vel, angvel, qn, invm, mp + 10, kn, ks, mu, e, shape_radius(s, sh, 1.0));
+    s->ready = false;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_add_wall(lsdem_solver* s, const double* verts, int n_verts, const double* sdf, const int* size3,
+                   const double* origin3, double spacing, const double* pos, const double* quat, double mu, double e,
+                   int* index) {
+  if (!s || !sdf || !size3 || !origin3 || !pos || !quat || (n_verts > 0 && !verts))
+    return fail(s, LSDEM_ERR_ARG, "null argument");
+  return guard(s, [&] {
+    // walls keep their vertices as nodes (LSSolver.h:255-271); only the radius uses them
+    const int sh = add_shape_impl(s, verts, 0, sdf, size3, origin3, spacing);
+    double r = 0.;
+    for (int i = 0; i < n_verts; ++i) r = std::max(r, hlen(v3(verts + 3 * i)));
+    if (index) *index = s->W.n();
+    push_body(s, s->W, sh, 1.0, pos, nullptr, nullptr, quat, 0., nullptr, 0., 0., mu, e, r);
+    s->ready = false;
+    return LSDEM_OK;
+  });
+}
+
+static int set_vec(lsdem_solver* s, std::vector<double>& v, int n, int index, const double* x, bool add) {
+  if (!s || !x) return LSDEM_ERR_ARG;
+  if (index < 0 || index >= n) return LSDEM_OK;  // reference: silently ignored
+  for (int a = 0; a < 3; ++a) v[3 * (size_t)index + a] = add ? v[3 * (size_t)index + a] + x[a] : x[a];
+  s->ready = false;
+  return LSDEM_OK;
+}
+int lsdem_move_particle(lsdem_solver* s, int index, const double* o) { return s ? set_vec(s, s->P.pos, s->P.n(), index, o, true) : LSDEM_ERR_ARG; }
+int lsdem_move_wall(lsdem_solver* s, int index, const double* o) { return s ? set_vec(s, s->W.pos, s->W.n(), index, o, true) : LSDEM_ERR_ARG; }
+int lsdem_set_wall_velocity(lsdem_solver* s, int index, const double* v) { return s ? set_vec(s, s->W.vel, s->W.n(), index, v, false) : LSDEM_ERR_ARG; }
+int lsdem_set_wall_angular_velocity(lsdem_solver* s, int index, const double* w) { return s ? set_vec(s, s->W.angvel, s->W.n(), index, w, false) : LSDEM_ERR_ARG; }
+
+// VBondedInteraction::add (VBondedInteraction.h:74-195) with the initial frame
+// vectors of getInitialOrthogonalUnitVectorsN2/N3 (:10-22).
+static int add_bond_impl(lsdem_solver* s, int i, int j, const double* pi, const double* qi, const double* pj,
+                         const double* qj, const double* point, const double* normal, double Rb, double Lb, double Eb,
+                         double nu, double ten, double coh, double fmu) {
+  V3 gn = v3(normal);
+  if (std::fabs(gn.x * gn.x + gn.y * gn.y + gn.z * gn.z) <= 1.0e-20) return fail(s, LSDEM_ERR_ARG, "Invalid bond normal");
+  if (Rb <= 0.) return fail(s, LSDEM_ERR_ARG, "Invalid bond radius");
+  if (Lb <= 0.) return fail(s, LSDEM_ERR_ARG, "Invalid bond length");
+  if (Eb <= 0.) return fail(s, LSDEM_ERR_ARG, "Invalid Young's modulus");
+  if (nu <= -1.0 || nu >= 0.5) return fail(s, LSDEM_ERR_ARG, "Invalid Poisson ratio");
+  const double Gb = Eb / (2. * (1. + nu));
+  const double Ab = M_PI * Rb * Rb;
+  const double Ib = Ab * Rb * Rb / 4.;
+  const double Jb = 2. * Ib;
+  const double Kn = Eb * Ab / Lb, Kt = Gb * Jb / Lb, Ks = 12. * Eb * Ib / (Lb * Lb * Lb), Kb = Eb * Ib / Lb;
+  const double B1 = Kn, B2 = Lb * Lb * Ks, B4 = Kt, B3 = Kb - B2 / 4. - B4 / 2.;
+  const double inv_len = 1.0 / hlen(gn);
+  const V3 n{gn.x * inv_len, gn.y * inv_len, gn.z * inv_len};
+  const V3 c = v3(point);
+  const V3 gpi{c.x + 0.5 * Lb * n.x, c.y + 0.5 * Lb * n.y, c.z + 0.5 * Lb * n.z};
+  const V3 gpj{c.x - 0.5 * Lb * n.x, c.y - 0.5 * Lb * n.y, c.z - 0.5 * Lb * n.z};
+  const V3 lpi = hrotate_inv(V3{gpi.x - pi[0], gpi.y - pi[1], gpi.z - pi[2]}, qi);
+  const V3 lpj = hrotate_inv(V3{gpj.x - pj[0], gpj.y - pj[1], gpj.z - pj[2]}, qj);
+  const V3 n1i{-n.x, -n.y, -n.z};
+  const V3 ref = (std::fabs(n1i.x) < 0.9) ? V3{1., 0., 0.} : V3{0., 1., 0.};
+  const V3 n2i = hnormalize(hcross(ref, n1i));
+  const V3 n3i = hnormalize(hcross(n1i, n2i));
+  const V3 n1j{-n1i.x, -n1i.y, -n1i.z};
+  const V3 loc[8] = {hnormalize(hrotate_inv(n1i, qi)), hnormalize(hrotate_inv(n2i, qi)), hnormalize(hrotate_inv(n3i, qi)), lpi,
+                     hnormalize(hrotate_inv(n1j, qj)), hnormalize(hrotate_inv(n2i, qj)), hnormalize(hrotate_inv(n3i, qj)), lpj};
+  BondHost& b = s->bonds;
+  b.ids.push_back(i); b.ids.push_back(j);
+  b.bonded.push_back(1);
+  b.B.insert(b.B.end(), {B1, B2, B3, B4});
+  b.geo.insert(b.geo.end(), {Rb, Lb, ten, coh, fmu});
+  for (const V3& v : loc) b.frames.insert(b.frames.end(), {v.x, v.y, v.z});
+  b.state.insert(b.state.end(), {0., 0., 0., 0., 0., 0., c.x, c.y, c.z});
+  s->ready = false;
+  return LSDEM_OK;
+}
+
+int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3, const double* normal3, double radius,
+                   double initial_length, double youngs, double poisson, double tensile, double cohesion, double mu) {
+  if (!s || !point3 || !normal3) return LSDEM_ERR_ARG;
+  if (master >= s->P.n() || slave >= s->P.n() || master < 0 || slave < 0) return LSDEM_OK;  // reference: ignored
+  return add_bond_impl(s, master, slave, &s->P.pos[3 * (size_t)master], &s->P.quat[4 * (size_t)master],
+                       &s->P.pos[3 * (size_t)slave], &s->P.quat[4 * (size_t)slave], point3, normal3, radius,
+                       initial_length, youngs, poisson, tensile, cohesion, mu);
+}
+
+int lsdem_set_periodic(lsdem_solver* s, int axes) {
+  if (!s) return LSDEM_ERR_ARG;
+  s->periodic = axes & 7;
+  s->ready = false;
+  return LSDEM_OK;
+}
+
+int lsdem_set_record_contacts(lsdem_solver* s, int on) {
+  if (!s) return LSDEM_ERR_ARG;
+  s->record = on != 0;
+  return LSDEM_OK;
+}
+
+int lsdem_set_capacity(lsdem_solver* s, int pp, int w, int g, long long c, int batch) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (pp > 0) s->cap_pp = pp;
+  if (w > 0) s->cap_w = w;
+  if (g > 0) s->cap_g = g;
+  if (c > 0) s->cap_c = c;
+  if (batch > 0) s->batch = batch;
+  s->ready = false;
+  return LSDEM_OK;
+}
+
+int lsdem_initialize(lsdem_solver* s, const double* min3, const double* max3, const double* gravity3) {
+  if (!s || !min3 || !max3) return fail(s, LSDEM_ERR_ARG, "null argument");
+  for (int a = 0; a < 3; ++a)
+    if (!(max3[a] - min3[a] > 0.0)) return fail(s, LSDEM_ERR_ARG, "Invalid simulation domain size");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= s->device)
+    return fail(s, LSDEM_ERR_NODEVICE, "no usable CUDA device");
+  for (int a = 0; a < 3; ++a) {
+    s->dmin[a] = min3[a];
+    s->dmax[a] = max3[a];
+    s->grav[a] = gravity3 ? gravity3[a] : 0.;
+  }
+  return guard(s, [&] {
+    initialize(s);
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_step(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (nsteps <= 0) return LSDEM_OK;
+  return guard(s, [&] { return run_steps(s, dt, nsteps, hook, user); });
+}
+
+long long lsdem_num(const lsdem_solver* s, int what) {
+  if (!s) return -1;
+  switch (what) {
+    case 0: return s->P.n();
+    case 1: return s->W.n();
+    case 2: return (long long)s->bonds.bonded.size();
+    case 3: {
+      long long nb = 0;
+      for (int i = 0; i < s->P.n(); ++i) nb += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3);
+      return nb;
+    }
+    case 4: return (long long)s->shapes.size();
+    case 5: return s->ready ? s->pg.ncells : 0;
+    case 6: return s->steps;
+    case 7: return s->reruns;
+    default: return -1;
+  }
+}
+
+double lsdem_time(const lsdem_solver* s) { return s ? s->time : 0.0; }
+
+int lsdem_get_state(lsdem_solver* s, double* pos, double* vel, double* angvel, double* quat, double* force,
+                    double* torque) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (!s->ready) {
+    const size_t n = (size_t)s->P.n();
+    if (pos) std::memcpy(pos, s->P.pos.data(), 24 * n);
+    if (vel) std::memcpy(vel, s->P.vel.data(), 24 * n);
+    if (angvel) std::memcpy(angvel, s->P.angvel.data(), 24 * n);
+    if (quat) std::memcpy(quat, s->P.quat.data(), 32 * n);
+    if (force) std::memset(force, 0, 24 * n);
+    if (torque) std::memset(torque, 0, 24 * n);
+    return LSDEM_OK;
+  }
+  return guard(s, [&] {
+    const size_t n = (size_t)s->P.n();
+    cudaStream_t st = s->stream;
+    if (pos && n) CK(cudaMemcpyAsync(pos, s->dP.pos.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (vel && n) CK(cudaMemcpyAsync(vel, s->dP.vel.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (angvel && n) CK(cudaMemcpyAsync(angvel, s->dP.angvel.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (quat && n) CK(cudaMemcpyAsync(quat, s->dP.quat.p, 32 * n, cudaMemcpyDeviceToHost, st));
+    if (force && n) CK(cudaMemcpyAsync(force, s->dP.force.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (torque && n) CK(cudaMemcpyAsync(torque, s->dP.torque.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_wall_state(lsdem_solver* s, double* pos, double* vel, double* angvel, double* quat) {
+  if (!s) return LSDEM_ERR_ARG;
+  const size_t n = (size_t)s->W.n();
+  if (!s->ready) {
+    if (pos) std::memcpy(pos, s->W.pos.data(), 24 * n);
+    if (vel) std::memcpy(vel, s->W.vel.data(), 24 * n);
+    if (angvel) std::memcpy(angvel, s->W.angvel.data(), 24 * n);
+    if (quat) std::memcpy(quat, s->W.quat.data(), 32 * n);
+    return LSDEM_OK;
+  }
+  return guard(s, [&] {
+    cudaStream_t st = s->stream;
+    if (pos && n) CK(cudaMemcpyAsync(pos, s->dW.pos.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (vel && n) CK(cudaMemcpyAsync(vel, s->dW.vel.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (angvel && n) CK(cudaMemcpyAsync(angvel, s->dW.angvel.p, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (quat && n) CK(cudaMemcpyAsync(quat, s->dW.quat.p, 32 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_set_state(lsdem_solver* s, const double* pos, const double* vel, const double* angvel, const double* quat) {
+  if (!s) return LSDEM_ERR_ARG;
+  const size_t n = (size_t)s->P.n();
+  if (!s->ready) {
+    if (pos) std::memcpy(s->P.pos.data(), pos, 24 * n);
+    if (vel) std::memcpy(s->P.vel.data(), vel, 24 * n);
+    if (angvel) std::memcpy(s->P.angvel.data(), angvel, 24 * n);
+    if (quat) std::memcpy(s->P.quat.data(), quat, 32 * n);
+    return LSDEM_OK;
+  }
+  return guard(s, [&] {
+    cudaStream_t st = s->stream;
+    if (pos && n) CK(cudaMemcpyAsync(s->dP.pos.p, pos, 24 * n, cudaMemcpyHostToDevice, st));
+    if (vel && n) CK(cudaMemcpyAsync(s->dP.vel.p, vel, 24 * n, cudaMemcpyHostToDevice, st));
+    if (angvel && n) CK(cudaMemcpyAsync(s->dP.angvel.p, angvel, 24 * n, cudaMemcpyHostToDevice, st));
+    if (quat && n) CK(cudaMemcpyAsync(s->dP.quat.p, quat, 32 * n, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_particle_params(const lsdem_solver* s, double* inv_mass, double* inv_inertia6, double* radius,
+                              double* kn, double* ks, double* mu, double* e, int* shape, double* scale,
+                              double* origin3, double* invh, long long* node_base) {
+  if (!s) return LSDEM_ERR_ARG;
+  const BodyHost& P = s->P;
+  const size_t n = (size_t)P.n();
+  if (inv_mass) std::memcpy(inv_mass, P.invm.data(), 8 * n);
+  if (inv_inertia6) std::memcpy(inv_inertia6, P.invI.data(), 48 * n);
+  if (radius) std::memcpy(radius, P.radius.data(), 8 * n);
+  if (kn) std::memcpy(kn, P.kn.data(), 8 * n);
+  if (ks) std::memcpy(ks, P.ks.data(), 8 * n);
+  if (mu) std::memcpy(mu, P.mu.data(), 8 * n);
+  if (e) std::memcpy(e, P.res.data(), 8 * n);
+  if (shape) std::memcpy(shape, P.shape.data(), 4 * n);
+  if (scale) std::memcpy(scale, P.scale.data(), 8 * n);
+  if (origin3) std::memcpy(origin3, P.origin.data(), 24 * n);
+  if (invh) std::memcpy(invh, P.invh.data(), 8 * n);
+  if (node_base) {
+    long long nb = 0;
+    for (size_t i = 0; i < n; ++i) {
+      node_base[i] = nb;
+      nb += (long long)(s->shapes[P.shape[i]].nodes.size() / 3);
+    }
+  }
+  return LSDEM_OK;
+}
+
+int lsdem_get_wall_params(const lsdem_solver* s, double* radius, double* mu, double* e, int* shape, double* origin3,
+                          double* invh) {
+  if (!s) return LSDEM_ERR_ARG;
+  const BodyHost& W = s->W;
+  const size_t n = (size_t)W.n();
+  if (radius) std::memcpy(radius, W.radius.data(), 8 * n);
+  if (mu) std::memcpy(mu, W.mu.data(), 8 * n);
+  if (e) std::memcpy(e, W.res.data(), 8 * n);
+  if (shape) std::memcpy(shape, W.shape.data(), 4 * n);
+  if (origin3) std::memcpy(origin3, W.origin.data(), 24 * n);
+  if (invh) std::memcpy(invh, W.invh.data(), 8 * n);
+  return LSDEM_OK;
+}
+
+int lsdem_get_shape(const lsdem_solver* s, int shape, double* nodes, double* sdf, int* size3, double* origin3,
+                    double* spacing, int* n_nodes) {
+  if (!s || shape < 0 || shape >= (int)s->shapes.size()) return LSDEM_ERR_ARG;
+  const ShapeHost& sh = s->shapes[shape];
+  if (nodes) std::memcpy(nodes, sh.nodes.data(), 8 * sh.nodes.size());
+  if (sdf) std::memcpy(sdf, sh.sdf.data(), 8 * sh.sdf.size());
+  if (size3) for (int a = 0; a < 3; ++a) size3[a] = sh.size[a];
+  if (origin3) for (int a = 0; a < 3; ++a) origin3[a] = sh.origin[a];
+  if (spacing) *spacing = sh.h;
+  if (n_nodes) *n_nodes = (int)(sh.nodes.size() / 3);
+  return LSDEM_OK;
+}
+
+static void grid_out(const GridP& g, double* mn, double* mx, double* inv, int* size) {
+  if (mn) { mn[0] = g.mn.x; mn[1] = g.mn.y; mn[2] = g.mn.z; }
+  if (mx) { mx[0] = g.mx.x; mx[1] = g.mx.y; mx[2] = g.mx.z; }
+  if (inv) { inv[0] = g.inv.x; inv[1] = g.inv.y; inv[2] = g.inv.z; }
+  if (size) { size[0] = g.size.x; size[1] = g.size.y; size[2] = g.size.z; }
+}
+int lsdem_get_grid(const lsdem_solver* s, double* mn, double* mx, double* inv, int* size) {
+  if (!s || !s->ready) return LSDEM_ERR_STATE;
+  grid_out(s->pg, mn, mx, inv, size);
+  return LSDEM_OK;
+}
+int lsdem_get_wall_grid(const lsdem_solver* s, double* mn, double* mx, double* inv, int* size) {
+  if (!s || !s->ready) return LSDEM_ERR_STATE;
+  grid_out(s->wg, mn, mx, inv, size);
+  return LSDEM_OK;
+}
+
+int lsdem_get_hash(lsdem_solver* s, int* key, int* sorted_idx, int* sorted_key, int* cell_start, int* cell_end) {
+  if (!s || !s->ready) return LSDEM_ERR_STATE;
+  return guard(s, [&] {
+    const size_t n = (size_t)s->P.n(), nc = (size_t)s->pg.ncells;
+    cudaStream_t st = s->stream;
+    if (key && n) CK(cudaMemcpyAsync(key, s->dP.key.p, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (sorted_idx && n) CK(cudaMemcpyAsync(sorted_idx, s->cell_idx.p, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (sorted_key && n) CK(cudaMemcpyAsync(sorted_key, s->sorted_key.p, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (cell_start) CK(cudaMemcpyAsync(cell_start, s->cell_start.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    if (cell_end) CK(cudaMemcpyAsync(cell_end, s->cell_end.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_count_contacts(lsdem_solver* s, int kind, long long* n) {
+  if (!s || !n || kind < 0 || kind > 2) return LSDEM_ERR_ARG;
+  if (!s->ready) { *n = 0; return LSDEM_OK; }
+  return guard(s, [&] {
+    long long t = 0;
+    walk_contacts(s, kind, [&](int, int, int, int c) { t += c; });
+    *n = t;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_contacts(lsdem_solver* s, int kind, long long cap, long long* node, int* partner, int* image,
+                       double* spring, double* point, double* normal, double* overlap, double* en_n, double* en_s) {
+  if (!s || kind < 0 || kind > 2) return LSDEM_ERR_ARG;
+  if (!s->ready) return LSDEM_OK;
+  return guard(s, [&] {
+    cudaStream_t st = s->stream;
+    ContactsDev& c = s->con[s->hp];
+    const size_t nc = (size_t)s->hist_count;
+    auto cn = dl(c.node, nc, st);
+    auto cs = dl(c.spring, nc, st);
+    const bool g = c.geom && (point || normal || overlap || en_n || en_s);
+    std::vector<double3> cp, cnm;
+    std::vector<double> co, ce, cf;
+    if (g) { cp = dl(c.point, nc, st); cnm = dl(c.normal, nc, st); co = dl(c.overlap, nc, st); ce = dl(c.en_n, nc, st); cf = dl(c.en_s, nc, st); }
+    CK(cudaStreamSynchronize(st));
+    std::vector<long long> nbase(s->P.n());
+    long long nb = 0;
+    for (int i = 0; i < s->P.n(); ++i) { nbase[i] = nb; nb += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3); }
+    long long out = 0;
+    walk_contacts(s, kind, [&](int A, int pid, int start, int cntk) {
+      const ShapeHost& sh = s->shapes[s->P.shape[A]];
+      for (int t = 0; t < cntk; ++t) {
+        if (out >= cap) return;
+        const size_t k = (size_t)start + t;
+        if (node) node[out] = nbase[A] + sh.perm[cn[k]];
+        if (partner) partner[out] = kind == 2 ? (pid >> 3) : pid;
+        if (image) image[out] = kind == 2 ? s->set_mask[pid & 7] : 0;
+        if (spring) { spring[3 * out] = cs[k].x; spring[3 * out + 1] = cs[k].y; spring[3 * out + 2] = cs[k].z; }
+        if (g) {
+          if (point) { point[3 * out] = cp[k].x; point[3 * out + 1] = cp[k].y; point[3 * out + 2] = cp[k].z; }
+          if (normal) { normal[3 * out] = cnm[k].x; normal[3 * out + 1] = cnm[k].y; normal[3 * out + 2] = cnm[k].z; }
+          if (overlap) overlap[out] = co[k];
+          if (en_n) en_n[out] = ce[k];
+          if (en_s) en_s[out] = cf[k];
+        }
+        ++out;
+      }
+    });
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_create_bonds_from_contacts(lsdem_solver* s, double radius, double L0, double E, double nu, double ten,
+                                     double coh, double mu) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (!s->ready) return LSDEM_OK;  // no contact list yet
+  return guard(s, [&] {
+    long long n = 0;
+    lsdem_count_contacts(s, LSDEM_CONTACT_PARTICLE, &n);
+    if (n == 0) return LSDEM_OK;
+    if (!s->con[s->hp].geom) throw Fail{LSDEM_ERR_STATE, "contact geometry not recorded (lsdem_set_record_contacts)"};
+    std::vector<long long> node(n);
+    std::vector<int> partner(n);
+    std::vector<double> point(3 * n), normal(3 * n);
+    int rc = lsdem_get_contacts(s, LSDEM_CONTACT_PARTICLE, n, node.data(), partner.data(), nullptr, nullptr,
+                                point.data(), normal.data(), nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    // host copy of particle state, as the reference reads its host mirrors
+    std::vector<double> pos(3 * (size_t)s->P.n()), quat(4 * (size_t)s->P.n());
+    rc = lsdem_get_state(s, pos.data(), nullptr, nullptr, quat.data(), nullptr, nullptr);
+    if (rc) return rc;
+    std::vector<long long> nbase(s->P.n() + 1);
+    long long nb = 0;
+    for (int i = 0; i < s->P.n(); ++i) { nbase[i] = nb; nb += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3); }
+    nbase[s->P.n()] = nb;
+    for (long long k = 0; k < n; ++k) {
+      const int i = (int)(std::upper_bound(nbase.begin(), nbase.end(), node[k]) - nbase.begin()) - 1;
+      const int j = partner[k];
+      add_bond_impl(s, i, j, &pos[3 * (size_t)i], &quat[4 * (size_t)i], &pos[3 * (size_t)j], &quat[4 * (size_t)j],
+                    &point[3 * k], &normal[3 * k], radius, L0, E, nu, ten, coh, mu);
+    }
+    s->ready = false;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_bonds(lsdem_solver* s, int* ids2, int* bonded, double* state9) {
+  if (!s) return LSDEM_ERR_ARG;
+  const size_t nb = s->bonds.bonded.size();
+  if (ids2) std::memcpy(ids2, s->bonds.ids.data(), 8 * nb);
+  if (!s->ready || nb == 0) {
+    if (bonded) std::memcpy(bonded, s->bonds.bonded.data(), 4 * nb);
+    if (state9) std::memcpy(state9, s->bonds.state.data(), 72 * nb);
+    return LSDEM_OK;
+  }
+  return guard(s, [&] {
+    cudaStream_t st = s->stream;
+    if (bonded) CK(cudaMemcpyAsync(bonded, s->b_bonded.p, 4 * nb, cudaMemcpyDeviceToHost, st));
+    if (state9) CK(cudaMemcpyAsync(state9, s->b_state.p, 72 * nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_device_pointers(lsdem_solver* s, void** force, void** torque, void** vel, void** angvel, void** pos,
+                          void** quat) {
+  if (!s || !s->ready) return LSDEM_ERR_STATE;
+  if (force) *force = s->dP.force.p;
+  if (torque) *torque = s->dP.torque.p;
+  if (vel) *vel = s->dP.vel.p;
+  if (angvel) *angvel = s->dP.angvel.p;
+  if (pos) *pos = s->dP.pos.p;
+  if (quat) *quat = s->dP.quat.p;
+  return LSDEM_OK;
+}
+
+void* lsdem_stream(const lsdem_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// Device-wide prefix sums and the stable cell bucket sort of the broadphase.
+//
+// Replaces the reference's thrust::inclusive_scan / thrust::sort_by_key +
+// findStartAndEnd (FunDEM/kernel/CUDAKernelFunction/myUtility/buildHashStartEnd.cu:18-66,
+// :69-137, :139-178). Cell keys are small integers, so instead of a radix sort
+// the particles are bucketed by key (histogram -> exclusive scan -> scatter)
+// and each bucket is put back into ascending particle order, which yields
+// exactly the order of a stable sort by key. Memory traffic per particle:
+// key read three times, index written twice, plus 8 B per cell.
+#include "kernels.h"
+
+namespace lsdem {
+
+static constexpr int SCAN_THREADS = 1024;
+static constexpr int SCAN_ITEMS = 4;
+static constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <typename T>
+__device__ T block_exclusive_scan(T v, T* smem_warp, T* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    T w = (lane < (int)(blockDim.x >> 5)) ? smem_warp[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    smem_warp[lane] = w;
+  }
+  __syncthreads();
+  T warp_off = warp > 0 ? smem_warp[warp - 1] : T(0);
+  if (total) *total = smem_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_off + x - v;
+}
+
+template <typename T>
+__global__ void k_scan_tile_sums(const T* __restrict__ in, long long n, T* __restrict__ sums) {
+  __shared__ T sw[32];
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k)
+    if (base + k < n) s += in[base + k];
+  T tot;
+  block_exclusive_scan<T>(s, sw, &tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// Exclusive scan of `n` tile sums in place by a single block, chunk by chunk.
+template <typename T>
+__global__ void k_scan_sums(T* sums, long long n) {
+  __shared__ T sw[32];
+  T carry = 0;
+  for (long long c = 0; c < n; c += SCAN_TILE) {
+    long long base = c + (long long)threadIdx.x * SCAN_ITEMS;
+    T v[SCAN_ITEMS];
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      v[k] = (base + k < n) ? sums[base + k] : T(0);
+      s += v[k];
+    }
+    T tot;
+    T ex = block_exclusive_scan<T>(s, sw, &tot);
+    T run = carry + ex;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      if (base + k < n) sums[base + k] = run;
+      run += v[k];
+    }
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void k_scan_apply(const T* __restrict__ in, T* __restrict__ out, long long n, const T* __restrict__ sums,
+                             int inclusive) {
+  __shared__ T sw[32];
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  T v[SCAN_ITEMS];
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : T(0);
+    s += v[k];
+  }
+  T ex = block_exclusive_scan<T>(s, sw, nullptr);
+  T run = sums[blockIdx.x] + ex;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    if (base + k < n) {
+      if (inclusive) { run += v[k]; out[base + k] = run; }
+      else { out[base + k] = run; run += v[k]; }
+    }
+  }
+}
+
+size_t scan_temp_elems(long long n) { return (size_t)((n + SCAN_TILE - 1) / SCAN_TILE) + 1; }
+
+template <typename T>
+void scan_impl(const T* in, T* out, long long n, T* tmp, bool inclusive, cudaStream_t s) {
+  if (n <= 0) return;
+  long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_tile_sums<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, tmp);
+  k_scan_sums<T><<<1, SCAN_THREADS, 0, s>>>(tmp, tiles);
+  k_scan_apply<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, out, n, tmp, inclusive ? 1 : 0);
+}
+
+void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s) {
+  scan_impl<int>(in, out, n, tmp, inclusive, s);
+}
+void scan_i64(const long long* in, long long* out, long long n, long long* tmp, bool inclusive, cudaStream_t s) {
+  scan_impl<long long>(in, out, n, tmp, inclusive, s);
+}
+
+// ---------------------------------------------------------------------------
+// Bucket sort by cell key.
+// Bucket of a key: 0 for -1 (outside the domain), 1 + key for a cell, and a
+// last bucket for keys >= ncells (a centre rounding onto the upper domain face),
+// which, as in the reference, sort after every cell and belong to none.
+__device__ __forceinline__ int bucket_of(int k, int ncells) { return k < 0 ? 0 : (k >= ncells ? ncells + 1 : k + 1); }
+
+__global__ void k_bucket_hist(const int* __restrict__ key, int n, int ncells, int* __restrict__ counts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  atomicAdd(&counts[bucket_of(key[i], ncells)], 1);
+}
+
+__global__ void k_bucket_scatter(const int* __restrict__ key, int n, int ncells, const int* __restrict__ offs,
+                                 int* __restrict__ fill, int* __restrict__ sorted_idx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int b = bucket_of(key[i], ncells);
+  int p = offs[b] + atomicAdd(&fill[b], 1);
+  sorted_idx[p] = i;
+}
+
+// One thread per bucket: restore ascending particle order inside the bucket
+// (insertion sort for small buckets, deferred to k_bucket_big otherwise) and
+// write the cell range [start, end) of cell b - 1, -1 when empty
+// (findStartAndEnd, buildHashStartEnd.cu:47-67).
+__global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int ncells, int* __restrict__ sorted_idx,
+                             int* __restrict__ start, int* __restrict__ end, int* __restrict__ big_list,
+                             int* __restrict__ big_count) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbuckets) return;
+  const int s = offs[b], e = offs[b + 1], L = e - s;
+  if (b > 0 && b <= ncells) {
+    start[b - 1] = L > 0 ? s : -1;
+    end[b - 1] = L > 0 ? e : -1;
+  }
+  if (L <= 1) return;
+  if (L > 64) {
+    int slot = atomicAdd(big_count, 1);
+    big_list[slot] = b;
+    return;
+  }
+  for (int p = s + 1; p < e; ++p) {
+    int v = sorted_idx[p];
+    int q = p - 1;
+    while (q >= s && sorted_idx[q] > v) { sorted_idx[q + 1] = sorted_idx[q]; --q; }
+    sorted_idx[q + 1] = v;
+  }
+}
+
+// One block per large bucket: rank each member by the number of smaller
+// particle indices in the bucket (indices are unique, so ranks are a permutation).
+__global__ void k_bucket_big(const int* __restrict__ offs, const int* __restrict__ big_list,
+                             const int* __restrict__ big_count, int* __restrict__ sorted_idx, int* __restrict__ tmp) {
+  if ((int)blockIdx.x >= *big_count) return;
+  const int b = big_list[blockIdx.x];
+  const int s = offs[b], e = offs[b + 1], L = e - s;
+  for (int k = threadIdx.x; k < L; k += blockDim.x) tmp[s + k] = sorted_idx[s + k];
+  __syncthreads();
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const int v = tmp[s + k];
+    int r = 0;
+    for (int m = 0; m < L; ++m) r += tmp[s + m] < v;
+    sorted_idx[s + r] = v;
+  }
+}
+
+__global__ void k_sorted_keys(const int* __restrict__ key, const int* __restrict__ sorted_idx, int n,
+                              int* __restrict__ sorted_key) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) sorted_key[p] = key[sorted_idx[p]];
+}
+
+void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorted_idx, int* sorted_key, int* start,
+                 int* end, cudaStream_t s) {
+  const int nb = ncells + 2;  // bucket 0: key -1, 1..ncells: cells, ncells+1: keys past the last cell
+  cudaMemsetAsync(w.counts, 0, sizeof(int) * (size_t)(nb + 1), s);
+  cudaMemsetAsync(w.fill, 0, sizeof(int) * (size_t)(nb + 1), s);
+  cudaMemsetAsync(w.big_count, 0, sizeof(int), s);
+  if (n > 0) k_bucket_hist<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.counts);
+  // exclusive scan over nb + 1 entries: offs[nb] = n
+  scan_i32(w.counts, w.offs, nb + 1, w.scan_tmp, false, s);
+  if (n > 0) k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx);
+  k_bucket_fix<<<(nb + 255) / 256, 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list, w.big_count);
+  // at most n / 65 buckets can exceed 64 members
+  int max_big = n / 65 + 1;
+  k_bucket_big<<<max_big, 256, 0, s>>>(w.offs, w.big_list, w.big_count, sorted_idx, w.tmp);
+  if (sorted_key && n > 0) k_sorted_keys<<<(n + 255) / 256, 256, 0, s>>>(key, sorted_idx, n, sorted_key);
+}
+
+}  // namespace lsdem

@@ -1,0 +1,758 @@
+// Level-set DEM step kernels for sm_100a (FP64 "plain" form).
+//
+// Kernel map against the reference hot path (paths relative to the reference root):
+//   k_integrate_first  half kick + drift + cell key (+ wall drift/key); replaces
+//                      particleVelocityAngularVelocityIntegrationKernel + particlePositionOrientationIntegrationKernel
+//                      (FunDEM/kernel/CUDAKernelFunction/particleIntegrationKernel.cu:3-40) and
+//                      calculateHashKernel (myUtility/mySpatialGrid.cu:4-26)
+//   k_candidates       particle-level candidate partners from the cell grid (new: replaces the
+//                      per-node 27-cell scan of LSParticleContactDetectionKernel.cu:44-61)
+//   k_narrowphase      node-vs-SDF tests (LSParticleContactDetectionKernel.cu:4-590), history
+//                      carry-over (…cu:280-289) and the linear contact force
+//                      (contactKernel.cuh:4-77, contactKernel.cu:46-271) fused in one pass
+//   k_kick             second half kick (particleIntegrationKernel.cu:3-24)
+//   k_periodic         wrap + ghost images + ghost keys (mySpatialGrid.cu:28-56, 87-152, 214-240)
+//   k_bonds            V-bond forces (contactKernel.cuh:138-199, contactKernel.cu:273-351)
+#include "kernels.h"
+
+namespace lsdem {
+
+static constexpr unsigned FULL = 0xffffffffu;
+static constexpr int NP_WARPS = 4;     // warps per narrowphase block
+static constexpr int MAXCL = 256;      // clusters of 32 nodes per shape (8192 nodes)
+
+LD unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+LD T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+LD double3 warp_sum3(double3 v) { return d3(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)); }
+LD void atomic_add3(double3* arr, int i, double3 v) {
+  atomicAdd(&arr[i].x, v.x);
+  atomicAdd(&arr[i].y, v.y);
+  atomicAdd(&arr[i].z, v.z);
+}
+
+// Absolute slack for conservative culling: covers FP64 rounding of coordinates.
+LD double coord_slack(double3 a, double3 b) {
+  return 1e-14 * (fabs(a.x) + fabs(a.y) + fabs(a.z) + fabs(b.x) + fabs(b.y) + fabs(b.z)) + 1e-300;
+}
+
+// ---------------------------------------------------------------------------
+// Integration, first half of the step (reference step order, LSSolver.h:1000-1011).
+__global__ void k_integrate_first(StepArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *a.C.count = 0;
+  if (i < a.P.n) {
+    const BodyView& P = a.P;
+    const double h = 0.5 * a.dt;
+    double3 v = P.vel[i], w = P.angvel[i];
+    Quat q = P.quat[i];
+    const double im = P.invmass[i];
+    if (!is_zero(im)) {
+      v += (P.force[i] * im + a.gravity) * h;
+      w += (mul(rotate_inv_inertia(q, P.invI[i]), P.torque[i])) * h;
+      P.vel[i] = v;
+      P.angvel[i] = w;
+    }
+    double3 x = P.pos[i];
+    x += a.dt * v;
+    q = quat_integrate(q, w, a.dt);
+    P.pos[i] = x;
+    P.quat[i] = q;
+    P.force[i] = d3(0., 0., 0.);
+    P.torque[i] = d3(0., 0., 0.);
+    P.key[i] = hash_key(x, a.pg);
+    if (a.pgh.cnt) a.pgh.cnt[i] = 0;
+  } else if (i < a.P.n + a.W.n) {
+    const int k = i - a.P.n;
+    const BodyView& W = a.W;
+    double3 x = W.pos[k];
+    x += a.dt * W.vel[k];
+    W.pos[k] = x;
+    W.quat[k] = quat_integrate(W.quat[k], W.angvel[k], a.dt);
+    W.key[k] = hash_key(x, a.wg);
+  }
+}
+
+void launch_integrate_first(const StepArgs& a, cudaStream_t s) {
+  int n = a.P.n + a.W.n;
+  if (n < 1) n = 1;
+  k_integrate_first<<<(n + 255) / 256, 256, 0, s>>>(a);
+}
+
+__global__ void k_kick(StepArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.P.n) return;
+  const BodyView& P = a.P;
+  const double im = P.invmass[i];
+  if (is_zero(im)) return;
+  const double h = 0.5 * a.dt;
+  double3 v = P.vel[i];
+  v += (P.force[i] * im + a.gravity) * h;
+  P.vel[i] = v;
+  double3 w = P.angvel[i];
+  w += (mul(rotate_inv_inertia(P.quat[i], P.invI[i]), P.torque[i])) * h;
+  P.angvel[i] = w;
+}
+
+void launch_kick(const StepArgs& a, cudaStream_t s) {
+  if (a.P.n > 0) k_kick<<<(a.P.n + 255) / 256, 256, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Box distance helpers for conservative culling (body frame).
+LD double box_dist(double3 l, double3 lo, double3 hi) {
+  double dx = fmax(fmax(lo.x - l.x, l.x - hi.x), 0.0);
+  double dy = fmax(fmax(lo.y - l.y, l.y - hi.y), 0.0);
+  double dz = fmax(fmax(lo.z - l.z, l.z - hi.z), 0.0);
+  return sqrt(dx * dx + dy * dy + dz * dz);
+}
+LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi) {
+  lo = o;
+  hi = d3(o.x + (gs.x - 1) / invh, o.y + (gs.y - 1) / invh, o.z + (gs.z - 1) / invh);
+}
+
+// Candidate partners of each particle A (one thread per particle).
+// Particle partners: B > A, visible (in a cell), bounding spheres within
+// reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
+// reference's |node - xB| <= rB test, which in turn implies B lies in the
+// node's 27-cell window since cells are at least 2 max radius wide).
+// Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
+__global__ void k_candidates(StepArgs a) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= a.P.n) return;
+  const double3 xA = a.P.pos[A];
+  const double rA = a.P.radius[A];
+  const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
+  int n = 0;
+  const int cap = a.pp.cap;
+  int* out = a.pp.id + (size_t)A * cap;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = c.z + dz;
+    if (z < 0 || z >= a.pg.size.z) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = c.y + dy;
+      if (y < 0 || y >= a.pg.size.y) continue;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = c.x + dx;
+        if (x < 0 || x >= a.pg.size.x) continue;
+        const int h = lin3(make_int3(x, y, z), a.pg.size);
+        const int st = a.cell_start[h];
+        if (st < 0) continue;
+        const int en = a.cell_end[h];
+        for (int k = st; k < en; ++k) {
+          const int B = a.cell_idx[k];
+          if (B <= A) continue;
+          const double3 xB = a.P.pos[B];
+          const double R = (rA + a.P.radius[B]) * (1.0 + 1e-9) + coord_slack(xA, xB);
+          if (len2(xA - xB) > R * R) continue;
+          if (n < cap) out[n] = B;
+          ++n;
+        }
+      }
+    }
+  }
+  a.pp.cnt[A] = n < cap ? n : cap;
+  if (n > cap) {
+    atomicOr(&a.status->flags, OVF_PP);
+    atomicMax(&a.status->need_pp, n);
+  }
+  // walls
+  int nw = 0;
+  const int capw = a.pw.cap;
+  for (int w = 0; w < a.W.n; ++w) {
+    if (a.W.key[w] < 0) continue;
+    const double3 l = rotate_inv(xA - a.W.pos[w], a.W.quat[w]);
+    double3 lo, hi;
+    grid_box(a.W.origin[w], a.W.invh[w], a.S.gsize[a.W.shape[w]], lo, hi);
+    const double reach = rA * (1.0 + 1e-9) + coord_slack(xA, a.W.pos[w]) + 1e-12 * len(hi - lo);
+    if (box_dist(l, lo, hi) > reach) continue;
+    if (nw < capw) a.pw.id[(size_t)A * capw + nw] = w;
+    ++nw;
+  }
+  if (capw > 0) a.pw.cnt[A] = nw < capw ? nw : capw;
+  if (nw > capw) {
+    atomicOr(&a.status->flags, OVF_WALL);
+    atomicMax(&a.status->need_wall, nw);
+  }
+}
+
+void launch_candidates(const StepArgs& a, cudaStream_t s) {
+  if (a.P.n > 0) k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Narrowphase.
+enum { KIND_PP = 0, KIND_WALL = 1, KIND_GHOST = 2 };
+
+// The owner particle A of the warp.
+struct SelfCtx {
+  double3 x, v, w;
+  Quat q;
+  Mat3 R;
+  double sc, invm, kn, ks, mu, res;
+  int n0, nn, cl0, ncl;
+};
+
+// The SDF side of a test.
+struct Partner {
+  double3 x;        // centre
+  Quat q;
+  double r;         // bounding radius (particle partners)
+  double3 o;        // grid origin (body frame)
+  double invh;
+  int3 gs;
+  const double* sdf;
+  double sc;        // SDF value scale
+  int key;          // cell key (walls: wall grid, ghosts: particle grid)
+  int real;         // particle index receiving the reaction (-1: none)
+  double3 v, w;     // velocity, angular velocity
+  double invm, kn, ks, mu, res;
+};
+
+template <int KIND>
+LD Partner load_partner(const StepArgs& a, int pid) {
+  Partner P;
+  if (KIND == KIND_WALL) {
+    const BodyView& W = a.W;
+    P.x = W.pos[pid]; P.q = W.quat[pid]; P.r = W.radius[pid];
+    P.o = W.origin[pid]; P.invh = W.invh[pid];
+    const int sh = W.shape[pid];
+    P.gs = a.S.gsize[sh]; P.sdf = a.S.sdf + a.S.sdf_off[sh]; P.sc = W.scale[pid];
+    P.key = W.key[pid]; P.real = -1;
+    P.v = W.vel[pid]; P.w = W.angvel[pid];
+    P.invm = 0.; P.kn = 0.; P.ks = 0.; P.mu = W.mu[pid]; P.res = W.res[pid];
+  } else {
+    const BodyView& B = a.P;
+    int i = pid, set = 0;
+    if (KIND == KIND_GHOST) { i = pid >> 3; set = pid & 7; }
+    if (KIND == KIND_GHOST) {
+      P.x = a.G.gpos[(size_t)set * B.n + i];
+      P.key = a.G.gkey[(size_t)set * B.n + i];
+    } else {
+      P.x = B.pos[i];
+      P.key = B.key[i];
+    }
+    P.q = B.quat[i]; P.r = B.radius[i];
+    P.o = B.origin[i]; P.invh = B.invh[i];
+    const int sh = B.shape[i];
+    P.gs = a.S.gsize[sh]; P.sdf = a.S.sdf + a.S.sdf_off[sh]; P.sc = B.scale[i];
+    P.real = i;
+    P.v = B.vel[i]; P.w = B.angvel[i];
+    P.invm = B.invmass[i]; P.kn = B.kn[i]; P.ks = B.ks[i]; P.mu = B.mu[i]; P.res = B.res[i];
+  }
+  return P;
+}
+
+LD double3 node_world(const StepArgs& a, const SelfCtx& S, int ni) {
+  const double3 nl = a.S.node_pos[S.n0 + ni] * S.sc;
+  return rotate(S.q, nl) + S.x;
+}
+
+// Trilinear SDF evaluation at world point w (LSParticleContactDetectionKernel.cu:63-115,
+// interpolateLevelSetFunctionValue .cuh:4-32). True when inside the grid with overlap >= 0.
+LD bool sdf_eval(double3 w, const Partner& P, double& ov, double& fx, double& fy, double& fz, double* c) {
+  const double3 l = rotate_inv(w - P.x, P.q);
+  const double gx = (l.x - P.o.x) * P.invh;
+  const double gy = (l.y - P.o.y) * P.invh;
+  const double gz = (l.z - P.o.z) * P.invh;
+  const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
+  if (i0 < 0 || j0 < 0 || k0 < 0) return false;
+  if (i0 >= P.gs.x - 1 || j0 >= P.gs.y - 1 || k0 >= P.gs.z - 1) return false;
+  fx = gx - (double)i0;
+  fy = gy - (double)j0;
+  fz = gz - (double)k0;
+  const int sx = 1, sy = P.gs.x, sz = P.gs.x * P.gs.y;
+  const double* b = P.sdf + (k0 * sz + j0 * sy + i0);
+  c[0] = P.sc * __ldg(b);
+  c[1] = P.sc * __ldg(b + sx);
+  c[2] = P.sc * __ldg(b + sy);
+  c[3] = P.sc * __ldg(b + sy + sx);
+  c[4] = P.sc * __ldg(b + sz);
+  c[5] = P.sc * __ldg(b + sz + sx);
+  c[6] = P.sc * __ldg(b + sz + sy);
+  c[7] = P.sc * __ldg(b + sz + sy + sx);
+  const double wx0 = 1.0 - fx, wx1 = fx, wy0 = 1.0 - fy, wy1 = fy, wz0 = 1.0 - fz, wz1 = fz;
+  const double phi = c[0] * wx0 * wy0 * wz0 + c[1] * wx1 * wy0 * wz0 + c[2] * wx0 * wy1 * wz0 +
+                     c[3] * wx1 * wy1 * wz0 + c[4] * wx0 * wy0 * wz1 + c[5] * wx1 * wy0 * wz1 +
+                     c[6] * wx0 * wy1 * wz1 + c[7] * wx1 * wy1 * wz1;
+  ov = -phi;
+  return ov >= 0.;
+}
+
+// Gradient in grid units (interpolateLevelSetFunctionGradient, .cuh:34-77).
+LD double3 sdf_grad(double fx, double fy, double fz, const double* c, int flags) {
+  const double x = (flags & FIX_GRADIENT) ? fx : (double)(int)fx;
+  const double wx0 = 1.0 - x, wx1 = x, wy0 = 1.0 - fy, wy1 = fy, wz0 = 1.0 - fz, wz1 = fz;
+  const double gx = (c[1] - c[0]) * wy0 * wz0 + (c[3] - c[2]) * wy1 * wz0 + (c[5] - c[4]) * wy0 * wz1 +
+                    (c[7] - c[6]) * wy1 * wz1;
+  const double gy = (c[2] - c[0]) * wx0 * wz0 + (c[3] - c[1]) * wx1 * wz0 + (c[6] - c[4]) * wx0 * wz1 +
+                    (c[7] - c[5]) * wx1 * wz1;
+  const double gz = (c[4] - c[0]) * wx0 * wy0 + (c[5] - c[1]) * wx1 * wy0 + (c[6] - c[2]) * wx0 * wy1 +
+                    (c[7] - c[3]) * wx1 * wy1;
+  return d3(gx, gy, gz);
+}
+
+// Exact per-node admission test of the reference for each partner kind.
+template <int KIND>
+LD bool node_admitted(const StepArgs& a, double3 w, const Partner& P) {
+  if (KIND == KIND_PP) {
+    const double3 r = w - P.x;
+    return !(len2(r) > P.r * P.r);
+  } else {
+    int3 c, lo, hi;
+    node_window(w, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
+    return in_window(P.key, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
+  }
+}
+
+// Conservative cluster cull: false only when no node of the cluster can pass.
+template <int KIND>
+LD bool cluster_may_hit(double3 wc, double rad, const Partner& P) {
+  const double slack = coord_slack(wc, P.x);
+  if (KIND == KIND_PP) {
+    const double R = (P.r + rad) * (1.0 + 1e-9) + slack;
+    return len2(wc - P.x) <= R * R;
+  } else {
+    const double3 l = rotate_inv(wc - P.x, P.q);
+    double3 lo, hi;
+    grid_box(P.o, P.invh, P.gs, lo, hi);
+    return box_dist(l, lo, hi) <= rad * (1.0 + 1e-9) + slack + 1e-12 * len(hi - lo);
+  }
+}
+
+LD double sqrt_damp(double v, int flags) { return (flags & FIX_SQRTF) ? sqrt(v) : (double)sqrtf((float)v); }
+
+// integrateSlidingSpring + LinearContact (contactKernel.cuh:4-77).
+LD void linear_contact(double3& F, double3& spring, double3 vc, double3 n, double delta, double dt, double kn,
+                       double ks, double mu, double e, double effM, int flags) {
+  if (delta > 0.) {
+    const double logRes = log(e);
+    const double diss = -logRes / sqrt_damp(logRes * logRes + M_PI * M_PI, flags);
+    const double cn = 2. * diss * sqrt_damp(effM * kn, flags);
+    const double3 vn = dot(vc, n) * n;
+    const double3 fn = kn * delta * n - cn * vn;
+    const double cs = 2. * diss * sqrt_damp(effM * ks, flags);
+    const double3 vs = vc - vn;
+    double3 s = d3(0., 0., 0.);
+    if (mu > 0. && ks > 0.) {
+      double3 p1 = spring - dot(spring, n) * n;
+      const double a1 = len(p1);
+      if (!is_zero(a1)) p1 *= len(spring) / a1;
+      s = p1 + vs * dt;
+      double3 fs = -ks * s - cs * vs;
+      const double afs = len(fs), afn = len(fn);
+      if (!is_zero(afs) && afs > mu * afn) {
+        const double ratio = mu * afn / afs;
+        fs *= ratio;
+        s = -(fs + cs * vs) / ks;
+      }
+    }
+    spring = s;
+    const double3 fsl = -ks * spring - cs * vs;
+    F = fn + fsl;
+  } else {
+    spring = d3(0., 0., 0.);
+    F = d3(0., 0., 0.);
+  }
+}
+
+template <int KIND>
+LD const SlotView& slots_of(const StepArgs& a, bool old) {
+  if (KIND == KIND_PP) return old ? a.pp_old : a.pp;
+  if (KIND == KIND_WALL) return old ? a.pw_old : a.pw;
+  return old ? a.pgh_old : a.pgh;
+}
+
+// Processes one (A, partner) pair with the whole warp. Contacts are found in
+// two sweeps over the surviving node clusters: the first counts them (ballot),
+// one atomic reserves a contiguous segment ordered by node, the second
+// recomputes the contact geometry, carries the tangential spring over from the
+// previous step's segment of the same pair, evaluates the linear contact force
+// and writes the contact. The partner's reaction is reduced over the warp and
+// added with one atomic per component.
+template <int KIND>
+LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, int* s_cl, unsigned* s_mask,
+                double3& FA, double3& TA) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();  // the previous pair's second sweep may still read s_cl / s_mask
+  const Partner P = load_partner<KIND>(a, pid);
+  const SlotView& cur = slots_of<KIND>(a, false);
+  // cluster culling
+  int nsurv = 0;
+  for (int c0 = 0; c0 < S.ncl; c0 += 32) {
+    const int c = c0 + lane;
+    bool keep = false;
+    if (c < S.ncl) {
+      const double4 sp = a.S.cl_sphere[S.cl0 + c];
+      const double3 wc = mat_mul(S.R, d3(sp.x, sp.y, sp.z) * S.sc) + S.x;
+      keep = cluster_may_hit<KIND>(wc, sp.w * S.sc, P);
+    }
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
+    nsurv += __popc(m);
+  }
+  __syncwarp();
+  // sweep 1: admission + SDF test
+  int total = 0;
+  for (int k = 0; k < nsurv; ++k) {
+    const int ni = s_cl[k] * 32 + lane;
+    bool hit = false;
+    if (ni < S.nn) {
+      const double3 w = node_world(a, S, ni);
+      if (node_admitted<KIND>(a, w, P)) {
+        double ov, fx, fy, fz, cr[8];
+        hit = sdf_eval(w, P, ov, fx, fy, fz, cr);
+      }
+    }
+    const unsigned m = __ballot_sync(FULL, hit);
+    if (lane == 0) s_mask[k] = m;
+    total += __popc(m);
+  }
+  __syncwarp();
+  const size_t sidx = (size_t)A * cur.cap + slot;
+  int base = 0;
+  if (lane == 0 && total > 0) {
+    base = atomicAdd(a.C.count, total);
+    atomicMax(&a.status->need_contact, base + total);
+  }
+  base = __shfl_sync(FULL, base, 0);
+  const bool can_write = (base + total <= a.C.cap);
+  if (lane == 0) {
+    cur.seg_start[sidx] = base;
+    cur.seg_cnt[sidx] = can_write ? total : 0;
+    if (!can_write) atomicOr(&a.status->flags, OVF_CONTACT);
+  }
+  if (total == 0) return;
+  // previous segment of the same pair
+  const SlotView& old = slots_of<KIND>(a, true);
+  int ostart = 0, ocnt = 0;
+  if (old.cnt != nullptr) {
+    const int on = old.cnt[A] < old.cap ? old.cnt[A] : old.cap;
+    for (int j0 = 0; j0 < on; j0 += 32) {
+      const int j = j0 + lane;
+      const bool match = j < on && old.id[(size_t)A * old.cap + j] == pid;
+      const unsigned m = __ballot_sync(FULL, match);
+      if (m) {
+        const int src = j0 + __ffs(m) - 1;
+        ostart = old.seg_start[(size_t)A * old.cap + src];
+        ocnt = old.seg_cnt[(size_t)A * old.cap + src];
+        break;
+      }
+    }
+  }
+  // sweep 2
+  double3 FB = d3(0., 0., 0.), TB = d3(0., 0., 0.);
+  int off = 0;
+  for (int k = 0; k < nsurv; ++k) {
+    const unsigned m = s_mask[k];
+    if (m == 0) continue;
+    if ((m >> lane) & 1u) {
+      const int ni = s_cl[k] * 32 + lane;
+      const double3 w = node_world(a, S, ni);
+      double ov, fx, fy, fz, cr[8];
+      sdf_eval(w, P, ov, fx, fy, fz, cr);
+      double3 n = sdf_grad(fx, fy, fz, cr, a.flags);
+      n = rotate(P.q, n);
+      n = normalize_dev(n);
+      const double3 pc = w + 0.5 * ov * n;
+      // carried-over spring: binary search of node ni in the old segment (sorted by node)
+      double3 spring = d3(0., 0., 0.);
+      int lo = 0, hi = ocnt - 1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int v = a.C_old.node[ostart + mid];
+        if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
+        if (v < ni) lo = mid + 1; else hi = mid - 1;
+      }
+      // contact force (contactKernel.cu:75-117 / :155-190 / :225-270)
+      const double3 vc = S.v + cross(S.w, pc - S.x) - (P.v + cross(P.w, pc - P.x));
+      double kn = 0., ks = 0., effM = 0., mu, res;
+      if (KIND == KIND_WALL) {
+        kn = S.kn; ks = S.ks;
+        if (S.invm > 0.) effM = 1. / S.invm;
+        mu = fmin(S.mu, P.mu);
+        res = fmin(S.res, P.res);
+      } else {
+        if (S.kn > 0. && P.kn > 0.) kn = S.kn * P.kn / (S.kn + P.kn);
+        if (S.ks > 0. && P.ks > 0.) ks = S.ks * P.ks / (S.ks + P.ks);
+        if (S.invm > 0. || P.invm > 0.) effM = 1. / (S.invm + P.invm);
+        res = fmin(S.res, P.res);
+        mu = fmin(S.mu, P.mu);
+      }
+      double3 F;
+      linear_contact(F, spring, vc, n, ov, a.dt, kn, ks, mu, res, effM, a.flags);
+      const int pos = base + off + __popc(m & lanemask_lt());
+      if (can_write) {
+        a.C.node[pos] = ni;
+        a.C.spring[pos] = spring;
+        if (a.C.point) {
+          a.C.point[pos] = pc;
+          a.C.normal[pos] = n;
+          a.C.overlap[pos] = ov;
+          a.C.en_n[pos] = 0.5 * ov * ov * kn;
+          a.C.en_s[pos] = 0.5 * len2(spring) * ks;
+        }
+      }
+      FA += F;
+      TA += cross(pc - S.x, F);
+      FB -= F;
+      TB += cross(pc - P.x, -F);
+    }
+    off += __popc(m);
+  }
+  if (KIND != KIND_WALL && !(KIND == KIND_GHOST && P.real == A)) {
+    FB = warp_sum3(FB);
+    TB = warp_sum3(TB);
+    if (lane == 0) {
+      atomic_add3(a.P.force, P.real, FB);
+      atomic_add3(a.P.torque, P.real, TB);
+    }
+  }
+}
+
+template <int KINDS>
+__global__ void __launch_bounds__(NP_WARPS * 32) k_narrowphase(StepArgs a) {
+  __shared__ int s_cl[NP_WARPS][MAXCL];
+  __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
+    const int npp = (KINDS & 1) ? a.pp.cnt[A] : 0;
+    const int nw = (KINDS & 2) ? (a.pw.cap > 0 ? a.pw.cnt[A] : 0) : 0;
+    const int ng = (KINDS & 4) ? a.pgh.cnt[A] : 0;
+    const int ngc = ng < a.pgh.cap ? ng : a.pgh.cap;
+    if (npp + nw + ngc == 0) continue;
+    SelfCtx S;
+    S.x = a.P.pos[A]; S.v = a.P.vel[A]; S.w = a.P.angvel[A]; S.q = a.P.quat[A];
+    S.R = quat_to_mat(S.q);
+    S.sc = a.P.scale[A]; S.invm = a.P.invmass[A]; S.kn = a.P.kn[A]; S.ks = a.P.ks[A];
+    S.mu = a.P.mu[A]; S.res = a.P.res[A];
+    const int sh = a.P.shape[A];
+    S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
+    S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
+    double3 FA = d3(0., 0., 0.), TA = d3(0., 0., 0.);
+    for (int j = 0; j < npp; ++j)
+      do_pair<KIND_PP>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+    for (int j = 0; j < nw; ++j)
+      do_pair<KIND_WALL>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+    for (int j = 0; j < ngc; ++j)
+      do_pair<KIND_GHOST>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+    FA = warp_sum3(FA);
+    TA = warp_sum3(TA);
+    if (lane == 0) {
+      atomic_add3(a.P.force, A, FA);
+      atomic_add3(a.P.torque, A, TA);
+    }
+  }
+}
+
+static int g_num_sms = 0;
+static int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
+  if (a.P.n <= 0) return;
+  int want = (a.P.n + NP_WARPS - 1) / NP_WARPS;
+  int cap = num_sms() * 16;
+  int blocks = want < cap ? want : cap;
+  if (kinds == 3) k_narrowphase<3><<<blocks, NP_WARPS * 32, 0, s>>>(a);
+  else if (kinds == 1) k_narrowphase<1><<<blocks, NP_WARPS * 32, 0, s>>>(a);
+  else if (kinds == 4) k_narrowphase<4><<<blocks, NP_WARPS * 32, 0, s>>>(a);
+  else k_narrowphase<7><<<blocks, NP_WARPS * 32, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Periodic boundary: wrap along each periodic axis in x, y, z order, each
+// single-axis image set taken right after its own axis is wrapped, the
+// multi-axis sets after all wraps (mySpatialGrid.cu:28-56, 87-152 and the order
+// of PeriodicBoundaryXY2D::updateGhostSpatialGrid, PeriodicBoundary.h:215-288).
+// Ghost keys follow calculateGhostHashKernel (mySpatialGrid.cu:214-240),
+// including its z-upper test against the y bound.
+LD void ghost_image(double3 p, const GridP& g, int mask, double3& out) {
+  const int3 c = cell_of(p, g);
+  bool hit = true;
+  if (mask & 1) hit = hit && c.x == 0;
+  if (mask & 2) hit = hit && c.y == 0;
+  if (mask & 4) hit = hit && c.z == 0;
+  out = p;
+  if (hit) {
+    double3 off = d3(0., 0., 0.);
+    if (mask & 1) off = off + d3(g.mx.x - g.mn.x, 0., 0.);
+    if (mask & 2) off = off + d3(0., g.mx.y - g.mn.y, 0.);
+    if (mask & 4) off = off + d3(0., 0., g.mx.z - g.mn.z);
+    out += off;
+  }
+}
+LD int ghost_key(double3 p, const GridP& g) {
+  int3 c = cell_of(p, g);
+  bool out = false;
+  if (p.x < g.mn.x) { c.x = 0; out = true; } else if (p.x >= g.mx.x) { c.x = g.size.x - 1; out = true; }
+  if (p.y < g.mn.y) { c.y = 0; out = true; } else if (p.y >= g.mx.y) { c.y = g.size.y - 1; out = true; }
+  if (p.z < g.mn.z) { c.z = 0; out = true; } else if (p.z >= g.mx.y) { c.z = g.size.z - 1; out = true; }
+  return out ? lin3(c, g.size) : -1;
+}
+
+__global__ void k_periodic(StepArgs a, int axes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.P.n) return;
+  const GridP& g = a.pg;
+  double3 p = a.P.pos[i];
+  const int n = a.P.n;
+  for (int ax = 0; ax < 3; ++ax) {
+    if (!((axes >> ax) & 1)) continue;
+    if (ax == 0) { const double L = g.mx.x - g.mn.x; if (p.x < g.mn.x) p.x += L; else if (p.x >= g.mx.x) p.x -= L; }
+    if (ax == 1) { const double L = g.mx.y - g.mn.y; if (p.y < g.mn.y) p.y += L; else if (p.y >= g.mx.y) p.y -= L; }
+    if (ax == 2) { const double L = g.mx.z - g.mn.z; if (p.z < g.mn.z) p.z += L; else if (p.z >= g.mx.z) p.z -= L; }
+    for (int s = 0; s < a.G.nsets; ++s)
+      if (a.G.mask[s] == (1 << ax)) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
+  }
+  for (int s = 0; s < a.G.nsets; ++s)
+    if (__popc(a.G.mask[s]) >= 2) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
+  for (int s = 0; s < a.G.nsets; ++s) a.G.gkey[(size_t)s * n + i] = ghost_key(a.G.gpos[(size_t)s * n + i], g);
+  a.P.pos[i] = p;
+}
+
+void launch_periodic(const StepArgs& a, int axes, cudaStream_t s) {
+  if (a.P.n > 0) k_periodic<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, axes);
+}
+
+// Clamped cell of every particle after the wrap (search grid for ghost partners).
+__global__ void k_clamped_keys(StepArgs a, int* key2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.P.n) return;
+  key2[i] = lin3(clamp_cell(cell_of(a.P.pos[i], a.pg), a.pg.size), a.pg.size);
+}
+void launch_clamped_keys(const StepArgs& a, int* key2, cudaStream_t s) {
+  if (a.P.n > 0) k_clamped_keys<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, key2);
+}
+
+// Ghost partners, searched from each visible ghost image G: a node of A can
+// only reach G's cell window when A's clamped cell is within 2 cells of G's
+// cell, and only when A's bounding sphere reaches G's SDF grid box.
+__global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, const int* __restrict__ g2_start,
+                                   const int* __restrict__ g2_end) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.P.n;
+  if (t >= (long long)a.G.nsets * n) return;
+  const int s = (int)(t / n), i = (int)(t % n);
+  const int gk = a.G.gkey[t];
+  if (gk < 0) return;
+  const double3 xg = a.G.gpos[t];
+  const GridP& g = a.pg;
+  const int cx = gk % g.size.x, cy = (gk / g.size.x) % g.size.y, cz = gk / (g.size.x * g.size.y);
+  // circumradius of the ghost's SDF grid box about its centre
+  double3 lo, hi;
+  grid_box(a.P.origin[i], a.P.invh[i], a.S.gsize[a.P.shape[i]], lo, hi);
+  const double3 far = d3(fmax(fabs(lo.x), fabs(hi.x)), fmax(fabs(lo.y), fabs(hi.y)), fmax(fabs(lo.z), fabs(hi.z)));
+  const double Rg = len(far);
+  const int pid = (i << 3) | s;
+  for (int z = cz - 2; z <= cz + 2; ++z) {
+    if (z < 0 || z >= g.size.z) continue;
+    for (int y = cy - 2; y <= cy + 2; ++y) {
+      if (y < 0 || y >= g.size.y) continue;
+      for (int x = cx - 2; x <= cx + 2; ++x) {
+        if (x < 0 || x >= g.size.x) continue;
+        const int h = lin3(make_int3(x, y, z), g.size);
+        const int st = g2_start[h];
+        if (st < 0) continue;
+        const int en = g2_end[h];
+        for (int k = st; k < en; ++k) {
+          const int A = g2_idx[k];
+          const double3 xA = a.P.pos[A];
+          const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
+          if (len2(xA - xg) > R * R) continue;
+          const int slot = atomicAdd(&a.pgh.cnt[A], 1);
+          if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
+          else {
+            atomicOr(&a.status->flags, OVF_GHOST);
+            atomicMax(&a.status->need_ghost, slot + 1);
+          }
+        }
+      }
+    }
+  }
+}
+
+void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,
+                             const int* /*g2_key*/, cudaStream_t s) {
+  long long n = (long long)a.G.nsets * a.P.n;
+  if (n > 0) k_ghost_candidates<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, g2_idx, g2_start, g2_end);
+}
+
+// ---------------------------------------------------------------------------
+// V-bond forces, one thread per bond.
+__global__ void k_bonds(StepArgs a, BondView b) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b.n) return;
+  double* st = b.state + 9 * (size_t)k;
+  if (b.bonded[k] == 0) {
+    for (int q = 0; q < 6; ++q) st[q] = 0.;
+    return;
+  }
+  const int i = b.ids[2 * k], j = b.ids[2 * k + 1];
+  const Quat qi = a.P.quat[i], qj = a.P.quat[j];
+  const double3* fr = b.frames + 8 * (size_t)k;
+  const double3 n1i = rotate(qi, fr[0]), n2i = rotate(qi, fr[1]), n3i = rotate(qi, fr[2]);
+  const double3 n1j = rotate(qj, fr[4]), n2j = rotate(qj, fr[5]), n3j = rotate(qj, fr[6]);
+  const double3 ri = a.P.pos[i], rj = a.P.pos[j];
+  const double3 rbi = rotate(qi, fr[3]) + ri;
+  const double3 rbj = rotate(qj, fr[7]) + rj;
+  const double3 bp = 0.5 * (rbi + rbj);
+  st[6] = bp.x; st[7] = bp.y; st[8] = bp.z;
+  const double B1 = b.B[4 * k], B2 = b.B[4 * k + 1], B3 = b.B[4 * k + 2], B4 = b.B[4 * k + 3];
+  const double Rb = b.geo[5 * k], D0 = b.geo[5 * k + 1], ten = b.geo[5 * k + 2], coh = b.geo[5 * k + 3],
+               fmu = b.geo[5 * k + 4];
+  double3 F = d3(0., 0., 0.), Mij = d3(0., 0., 0.), Mji = d3(0., 0., 0.);
+  int ok = 1;
+  const double3 rbij = rbi - rbj;
+  const double D = len(rbij);
+  if (!is_zero(D)) {
+    const double3 nij = normalize_dev(rbij);
+    const double3 e = -nij;
+    st[0] = 0.5 * B1 * (D - D0) * (D - D0);
+    st[1] = B2 * (0.5 * dot((n1j - n1i), e) - 0.25 * dot(n1i, n1j) + 0.75);
+    st[2] = (0.25 * B2 + B3 + 0.5 * B4) * (dot(n1i, n1j) + 1.);
+    st[3] = -0.5 * B4 * (dot(n1i, n1j) + dot(n2i, n2j) + dot(n3i, n3j) - 1);
+    F = B1 * (D - D0) * e + B2 / (2 * D) * ((n1j - n1i) - dot((n1j - n1i), e) * e);
+    const double3 MTB = B3 * cross(n1j, n1i) - 0.5 * B4 * (cross(n2j, n2i) + cross(n3j, n3i));
+    Mij = -0.5 * B2 * cross(e, n1i) + MTB;
+    Mji = 0.5 * B2 * cross(e, n1j) - MTB;
+    const double fnb = dot(F, nij);
+    const double3 fsb = F - fnb * nij;
+    const double tt = dot(MTB, nij);
+    const double3 tb = MTB - tt * nij;
+    const double Ab = Rb * Rb * M_PI;
+    const double Ib = Ab * Rb * Rb / 4.;
+    const double Jb = 2 * Ib;
+    st[4] = -fnb / Ab + len(tb) / Ib * Rb;
+    st[5] = len(fsb) / Ab + fabs(tt) / Jb * Rb;
+    if (ten > 0. && st[4] > ten) ok = 0;
+    else if (coh > 0. && st[5] > coh - fmu * st[4]) ok = 0;
+  }
+  b.bonded[k] = ok;
+  atomic_add3(a.P.force, i, F);
+  atomic_add3(a.P.torque, i, Mij + cross(rbi - ri, F));
+  atomic_add3(a.P.force, j, -F);
+  atomic_add3(a.P.torque, j, Mji + cross(rbj - rj, -F));
+}
+
+void launch_bonds(const StepArgs& a, const BondView& b, cudaStream_t s) {
+  if (b.n > 0) k_bonds<<<(b.n + 127) / 128, 128, 0, s>>>(a, b);
+}
+
+}  // namespace lsdem

@@ -1,0 +1,30 @@
+#!/usr/bin/env bash
+# Builds the reference solver's own CUDA kernels, compiled from its sources
+# where they lie in the reference tree, together with oracle/ref_wrapper.cu
+# into oracle/_ref/libfundem_ref.so (sm_100a). Test infrastructure only:
+# the library produces golden vectors on a B200 and is never part of the
+# product path. The reference tree is read, never written.
+set -euo pipefail
+REF=${REF:-/root/reference}
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+K="$REF/FunDEM/kernel"
+if [ ! -d "$K" ]; then
+  echo "reference tree not found at $REF; skipping" >&2
+  exit 0
+fi
+mkdir -p "$OUT"
+SRCS=(
+  "$K/CUDAKernelFunction/myUtility/mySpatialGrid.cu"
+  "$K/CUDAKernelFunction/myUtility/buildHashStartEnd.cu"
+  "$K/CUDAKernelFunction/LSParticleContactDetectionKernel.cu"
+  "$K/CUDAKernelFunction/contactKernel.cu"
+  "$K/CUDAKernelFunction/particleIntegrationKernel.cu"
+  "$HERE/ref_wrapper.cu"
+)
+# Release flags as the reference's CMake Release build (-O3 -DNDEBUG), sm_100a.
+nvcc -std=c++17 -O3 -DNDEBUG -Xcompiler -fPIC -shared \
+  -gencode arch=compute_100a,code=sm_100a \
+  -I"$K" -I"$K/CUDAKernelFunction" \
+  "${SRCS[@]}" -o "$OUT/libfundem_ref.so"
+echo "built $OUT/libfundem_ref.so"
