@@ -286,3 +286,31 @@ def load_into(solver, scene, walls=True):
         cx, cy = 0.5 * (scene["min"][0] + scene["max"][0]), 0.5 * (scene["min"][1] + scene["max"][1])
         solver.add_wall(f["verts"], f["sdf"], f["size"], f["origin"], f["spacing"], [cx, cy, scene["min"][2]],
                         [1.0, 0.0, 0.0, 0.0], scene["mu"], scene["e"])
+
+
+# ---------------------------------------------------------------------------
+# Polydisperse multi-template scenes (precision-form workload)
+
+
+def unit_templates(n_grid=48, n_nodes=2000):
+    """The four templates of the precision-form workload, each scaled to a bounding
+    diameter of 1 (so a particle of bounding diameter d uses scale d):
+    ellipsoid 1:0.8:0.6, superquadric |x|^4+|y|^4+|z|^4 = 1, cube with edge radius
+    0.1 of the side, capsule of aspect ratio 2 (length = 2 x diameter)."""
+    out = []
+    # ellipsoid, exact distance
+    ax = np.array([0.5, 0.4, 0.3])
+    out.append(make_ellipsoid(ax, n_grid, n_nodes))
+    # superquadric exponent 4: max radius at the diagonal, 3^(1/4) * half-size
+    hs = 0.5 / 3 ** 0.25
+    out.append(make_from_sdf(superquadric_fn((hs, hs, hs), 4.0), np.array([hs, hs, hs]), n_grid, n_nodes,
+                             exact=False))
+    # rounded cube: side s, edge radius 0.1 s, bounding radius sqrt(3)(s/2 - r) + r = 0.5
+    s = 1.0 / (np.sqrt(3.0) * 0.8 + 0.2)
+    out.append(make_from_sdf(rounded_box_sdf([s / 2] * 3, 0.1 * s), np.array([s / 2] * 3), n_grid, n_nodes))
+    # capsule: radius r, half length of the axis segment r (total length 4r = 2 x diameter), bounding radius 2r = 0.5
+    r = 0.25
+    out.append(make_from_sdf(capsule_sdf(r, r), np.array([r, r, 2 * r]), n_grid, n_nodes))
+    for t in out:
+        t["bound"] = float(np.max(np.linalg.norm(t["nodes"], axis=1)))
+    return out
