@@ -124,7 +124,7 @@ int lsdem_set_capacity(lsdem_solver* s, int pp_slots, int wall_slots, int ghost_
                        int batch_steps);
 
 /* Sizes: 0 particles, 1 walls, 2 bonds, 3 surface nodes, 4 shapes, 5 grid cells,
- * 6 steps taken, 7 overflow re-runs so far. */
+ * 6 steps taken, 7 overflow re-runs so far, 8 kernels launched by steps so far. */
 long long lsdem_num(const lsdem_solver* s, int what);
 double lsdem_time(const lsdem_solver* s);
 
@@ -171,6 +171,22 @@ int lsdem_device_pointers(lsdem_solver* s, void** force, void** torque, void** v
                           void** quat);
 /* The solver's CUDA stream (cudaStream_t). */
 void* lsdem_stream(const lsdem_solver* s);
+
+/* Device timing of the step phases with CUDA events on the solver stream
+ * (no counterpart in the reference, which has no timers). Phases: 0 kick+drift+keys,
+ * 1 cell sort, 2 candidates, 3 particle/wall narrowphase + forces, 4 periodic wrap +
+ * ghost images + ghost candidates, 5 ghost narrowphase + forces, 6 bonds,
+ * 7 second half kick. Enabling resets the totals. */
+int lsdem_set_profiling(lsdem_solver* s, int on);
+int lsdem_get_profile(const lsdem_solver* s, double* ms8, long long* calls8);
+/* Work counts of the last step: candidate pairs (particle, wall, ghost) and contacts. */
+int lsdem_step_stats(lsdem_solver* s, long long* out4);
+
+/* Scene set-up helper: random sequential addition of spheres (in the given
+ * order) in [lo, hi), periodic or not (the reference's sphere-packing helper,
+ * FunDEM/kernel/helper/SpherePackingGenerator.h:75-217, does the same job on the host). */
+int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic,
+                   unsigned long long seed, int max_tries, double* pos_out);
 
 #ifdef __cplusplus
 }

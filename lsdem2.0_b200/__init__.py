@@ -89,6 +89,10 @@ _SIGS = {
     "lsdem_device_pointers": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                         C.POINTER(P)]),
     "lsdem_stream": (P, [P]),
+    "lsdem_set_profiling": (C.c_int, [P, C.c_int]),
+    "lsdem_get_profile": (C.c_int, [P, DP, LP]),
+    "lsdem_step_stats": (C.c_int, [P, LP]),
+    "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, DP]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -118,6 +122,16 @@ def _dp(a):  # pointer into a writable float64 array
 
 def _ip(a):
     return None if a is None else a.ctypes.data_as(IP)
+
+
+def pack_rsa(radius, lo, hi, periodic=False, seed=12345, max_tries=1000):
+    """Random sequential addition of spheres with the given radii (placed in order)."""
+    r = np.ascontiguousarray(radius, np.float64)
+    out = np.zeros((len(r), 3))
+    rc = lib.lsdem_pack_rsa(len(r), _d(r), _d(lo), _d(hi), 1 if periodic else 0, int(seed), int(max_tries), _dp(out))
+    if rc:
+        raise LSDEMError(rc, "pack_rsa: could not place every sphere")
+    return out
 
 
 def mass_properties(sdf, size, origin, spacing, density):
@@ -347,6 +361,23 @@ class Solver:
         state = np.zeros((nb, 9))
         self._chk(lib.lsdem_get_bonds(self.h, _ip(ids), _ip(bonded), _dp(state)), "get_bonds")
         return {"ids": ids, "bonded": bonded, "state": state}
+
+    PHASES = ("kick_drift_keys", "cell_sort", "candidates", "narrowphase", "periodic", "ghost_narrowphase", "bonds",
+              "kick")
+
+    def set_profiling(self, on=True):
+        self._chk(lib.lsdem_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def profile(self):
+        ms = np.zeros(8)
+        calls = np.zeros(8, np.int64)
+        self._chk(lib.lsdem_get_profile(self.h, _dp(ms), calls.ctypes.data_as(LP)), "get_profile")
+        return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(self.PHASES)}
+
+    def step_stats(self):
+        o = np.zeros(4, np.int64)
+        self._chk(lib.lsdem_step_stats(self.h, o.ctypes.data_as(LP)), "step_stats")
+        return {"pairs_particle": int(o[0]), "pairs_wall": int(o[1]), "pairs_ghost": int(o[2]), "contacts": int(o[3])}
 
     def device_pointers(self):
         ptrs = [P() for _ in range(6)]

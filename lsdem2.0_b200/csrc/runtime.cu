@@ -335,12 +335,20 @@ struct lsdem_solver {
   DArr<double3> bk_cspring;
   int bk_cap[3] = {0, 0, 0};
   long long hist_count = 0;  // contacts in the history buffer hp
-  long long steps = 0, reruns = 0;
+  long long steps = 0, reruns = 0, launches = 0;
   double time = 0.0;
+  // optional per-phase device timing (CUDA events on the solver stream)
+  bool profiling = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+  std::vector<cudaEvent_t> event_pool;
+  double prof_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long prof_calls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   ~lsdem_solver() {
     if (h_status) cudaFreeHost(h_status);
     if (h_count) cudaFreeHost(h_count);
+    for (auto& p : prof_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
   }
 };
 
@@ -691,6 +699,48 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   return a;
 }
 
+// Phase timing: events recorded on the solver stream around each phase;
+// resolved after the batch synchronisation.
+cudaEvent_t pool_event(lsdem_solver* s) {
+  if (!s->event_pool.empty()) {
+    cudaEvent_t e = s->event_pool.back();
+    s->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+struct PhaseTimer {
+  lsdem_solver* s;
+  int id;
+  cudaEvent_t a = nullptr, b = nullptr;
+  PhaseTimer(lsdem_solver* s_, int id_) : s(s_), id(id_) {
+    if (!s->profiling) return;
+    a = pool_event(s);
+    b = pool_event(s);
+    CK(cudaEventRecord(a, s->stream));
+  }
+  ~PhaseTimer() {
+    if (!a) return;
+    cudaEventRecord(b, s->stream);
+    s->prof_pending.push_back({id, {a, b}});
+  }
+};
+void resolve_profile(lsdem_solver* s, bool keep) {
+  for (auto& p : s->prof_pending) {
+    if (keep) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+      s->prof_ms[p.first] += ms;
+      s->prof_calls[p.first] += 1;
+    }
+    s->event_pool.push_back(p.second.first);
+    s->event_pool.push_back(p.second.second);
+  }
+  s->prof_pending.clear();
+}
+
 // One time step in the reference order (LSSolver.h:1000-1011, 1104-1128).
 void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* user, double t) {
   cudaStream_t st = s->stream;
@@ -701,25 +751,36 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
     a.C.point = c.point.p; a.C.normal = c.normal.p; a.C.overlap = c.overlap.p; a.C.en_n = c.en_n.p;
     a.C.en_s = c.en_s.p;
   }
-  launch_integrate_first(a, st);
+  { PhaseTimer pt(s, 0); launch_integrate_first(a, st); }
   BucketScratch w{s->bk_counts.p, s->bk_fill.p, s->bk_offs.p, s->bk_scan.p, s->bk_big.p, s->bk_bigc.p, s->bk_tmp.p};
-  bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st);
-  launch_candidates(a, st);
-  launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st);
+  {
+    PhaseTimer pt(s, 1);
+    bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st);
+  }
+  { PhaseTimer pt(s, 2); launch_candidates(a, st); }
+  { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
   if (s->nsets > 0) {
-    launch_periodic(a, s->periodic, st);
-    launch_clamped_keys(a, s->key2.p, st);
-    bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
-    launch_ghost_candidates(a, s->g2_idx.p, s->g2_start.p, s->g2_end.p, s->key2.p, st);
-    launch_narrowphase(a, 4, st);
+    {
+      PhaseTimer pt(s, 4);
+      launch_periodic(a, s->periodic, st);
+      launch_clamped_keys(a, s->key2.p, st);
+      bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
+      launch_ghost_candidates(a, s->g2_idx.p, s->g2_start.p, s->g2_end.p, s->key2.p, st);
+    }
+    { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
   }
   if (!s->bonds.bonded.empty()) {
+    PhaseTimer pt(s, 6);
     BondView b{(int)s->bonds.bonded.size(), s->b_ids.p, s->b_B.p, s->b_geo.p, s->b_frames.p, s->b_bonded.p,
                s->b_state.p};
     launch_bonds(a, b, st);
   }
   if (hook) hook(user, t);
-  launch_kick(a, st);
+  { PhaseTimer pt(s, 7); launch_kick(a, st); }
+  // kernels launched by this step: kick/drift/keys, cell sort (8), candidates,
+  // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (7),
+  // ghost candidates, ghost narrowphase; bonds
+  if (a.P.n > 0) s->launches += 12 + (s->nsets > 0 ? 11 : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
 }
@@ -819,6 +880,7 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
       CK(cudaMemcpyAsync(s->h_count, s->con[s->hp].count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       const Status stat = *s->h_status;
+      resolve_profile(s, stat.flags == 0);
       if (stat.flags == 0) {
         s->hist_count = *s->h_count;
         break;
@@ -1106,6 +1168,7 @@ long long lsdem_num(const lsdem_solver* s, int what) {
     case 5: return s->ready ? s->pg.ncells : 0;
     case 6: return s->steps;
     case 7: return s->reruns;
+    case 8: return s->launches;
     default: return -1;
   }
 }
@@ -1385,5 +1448,109 @@ int lsdem_device_pointers(lsdem_solver* s, void** force, void** torque, void** v
 }
 
 void* lsdem_stream(const lsdem_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+
+int lsdem_set_profiling(lsdem_solver* s, int on) {
+  if (!s) return LSDEM_ERR_ARG;
+  s->profiling = on != 0;
+  for (int k = 0; k < 8; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
+  return LSDEM_OK;
+}
+
+int lsdem_get_profile(const lsdem_solver* s, double* ms8, long long* calls8) {
+  if (!s) return LSDEM_ERR_ARG;
+  for (int k = 0; k < 8; ++k) {
+    if (ms8) ms8[k] = s->prof_ms[k];
+    if (calls8) calls8[k] = s->prof_calls[k];
+  }
+  return LSDEM_OK;
+}
+
+int lsdem_step_stats(lsdem_solver* s, long long* out4) {
+  if (!s || !out4) return LSDEM_ERR_ARG;
+  if (!s->ready) { for (int k = 0; k < 4; ++k) out4[k] = 0; return LSDEM_OK; }
+  return guard(s, [&] {
+    long long pairs[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+      SlotsDev& sl = s->slots[s->hp][k];
+      if (!sl.cnt.p || sl.cap == 0) continue;
+      auto c = dl(sl.cnt, (size_t)s->P.n(), s->stream);
+      CK(cudaStreamSynchronize(s->stream));
+      for (int v : c) pairs[k] += std::min(v, sl.cap);
+    }
+    out4[0] = pairs[0]; out4[1] = pairs[1]; out4[2] = pairs[2]; out4[3] = s->hist_count;
+    return LSDEM_OK;
+  });
+}
+
+// Random sequential addition of spheres (largest first, in the given order)
+// in the box [lo, hi), optionally periodic, using a uniform cell list.
+// Returns LSDEM_ERR_ARG when a sphere cannot be placed in max_tries.
+int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic, unsigned long long seed,
+                   int max_tries, double* pos_out) {
+  if (n < 0 || !radius || !lo || !hi || !pos_out) return LSDEM_ERR_ARG;
+  if (n == 0) return LSDEM_OK;
+  double rmax = 0.;
+  for (int i = 0; i < n; ++i) rmax = std::max(rmax, radius[i]);
+  double L[3];
+  int dims[3];
+  for (int a = 0; a < 3; ++a) {
+    L[a] = hi[a] - lo[a];
+    dims[a] = std::max(1, (int)(L[a] / (2.0 * rmax)));
+  }
+  const size_t ncell = (size_t)dims[0] * dims[1] * dims[2];
+  std::vector<std::vector<int>> cells(ncell);
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto rnd = [&]() {  // splitmix64 -> [0, 1)
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  for (int i = 0; i < n; ++i) {
+    const double r = radius[i];
+    bool placed = false;
+    for (int t = 0; t < max_tries && !placed; ++t) {
+      double p[3];
+      int c[3];
+      for (int a = 0; a < 3; ++a) {
+        p[a] = periodic ? lo[a] + rnd() * L[a] : lo[a] + r + rnd() * (L[a] - 2 * r);
+        c[a] = std::min(dims[a] - 1, std::max(0, (int)((p[a] - lo[a]) / L[a] * dims[a])));
+      }
+      bool ok = true;
+      for (int dz = -1; dz <= 1 && ok; ++dz)
+        for (int dy = -1; dy <= 1 && ok; ++dy)
+          for (int dx = -1; dx <= 1 && ok; ++dx) {
+            int cc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
+            bool skip = false;
+            for (int a = 0; a < 3; ++a) {
+              if (cc[a] < 0 || cc[a] >= dims[a]) {
+                if (!periodic) skip = true;
+                cc[a] = (cc[a] + dims[a]) % dims[a];
+              }
+            }
+            if (skip) continue;
+            for (int j : cells[((size_t)cc[2] * dims[1] + cc[1]) * dims[0] + cc[0]]) {
+              double d2 = 0.;
+              for (int a = 0; a < 3; ++a) {
+                double dd = pos_out[3 * (size_t)j + a] - p[a];
+                if (periodic) dd -= L[a] * std::round(dd / L[a]);
+                d2 += dd * dd;
+              }
+              const double R = r + radius[j];
+              if (d2 < R * R) { ok = false; break; }
+            }
+          }
+      if (ok) {
+        for (int a = 0; a < 3; ++a) pos_out[3 * (size_t)i + a] = p[a];
+        cells[((size_t)c[2] * dims[1] + c[1]) * dims[0] + c[0]].push_back(i);
+        placed = true;
+      }
+    }
+    if (!placed) return LSDEM_ERR_ARG;
+  }
+  return LSDEM_OK;
+}
 
 }  // extern "C"

@@ -314,3 +314,51 @@ def unit_templates(n_grid=48, n_nodes=2000):
     for t in out:
         t["bound"] = float(np.max(np.linalg.norm(t["nodes"], axis=1)))
     return out
+
+
+def polydisperse_periodic(lsdem, n=100_000, box=0.1, median=2e-3, sigma=0.25, n_grid=48, n_nodes=2000, seed=None,
+                          vel_sigma=0.1, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=5e-7, exclusion=0.8,
+                          templates=None):
+    """Precision-form workload: n particles from the four unit templates, log-normal bounding
+    diameters (median 2 mm, sigma 0.25), in a triply periodic cube of side `box`, velocities
+    N(0, 0.1 m/s) per component, linear contact as the small workload, dt = 5e-7 s.
+
+    Positions come from random sequential addition of spheres of `exclusion` x the bounding
+    radius (largest first): at this count the bounding spheres alone fill more than half of
+    the box, beyond any sequential packing, so bounding spheres may overlap by up to 20 %
+    while the non-spherical bodies themselves mostly stay apart.
+
+    Returns a dict with the per-template data and per-particle arrays ready for
+    Solver.add_shape / Solver.add_particles (frame moved to each template's centroid,
+    mass and inertia scaled from the unit-density template integrals)."""
+    rng = np.random.default_rng(seed_for(1) if seed is None else seed)
+    T = templates or unit_templates(n_grid, n_nodes)
+    d = median * np.exp(sigma * rng.standard_normal(n))
+    order = np.argsort(-d)
+    d = d[order]
+    shape = rng.integers(0, len(T), size=n).astype(np.int32)
+    pos = lsdem.pack_rsa(0.5 * exclusion * d, np.zeros(3), np.full(3, box), periodic=True,
+                         seed=int(rng.integers(1 << 62)))
+    quat = random_quaternions(rng, n)
+    vel = rng.normal(0.0, vel_sigma, size=(n, 3))
+    tm = []
+    for t in T:
+        mp = lsdem.mass_properties(t["sdf"], t["size"], t["origin"], t["spacing"], 1.0)
+        c = mp["centroid"]
+        tm.append({"nodes": t["nodes"] - c, "sdf": t["sdf"], "size": t["size"], "origin": t["origin"] - c,
+                   "spacing": t["spacing"], "mass": mp["mass"], "inv_inertia": mp["inv_inertia"]})
+    m1 = np.array([t["mass"] for t in tm])[shape]
+    iI = np.array([t["inv_inertia"] for t in tm])[shape]
+    inv_mass = 1.0 / (density * m1 * d ** 3)
+    inv_inertia = iI / (density * d[:, None] ** 5)
+    return {"templates": tm, "shape": shape, "scale": d, "pos": pos, "quat": quat, "vel": vel,
+            "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn, "mu": mu, "e": e,
+            "dt": dt, "min": np.zeros(3), "max": np.full(3, box), "gravity": np.zeros(3), "periodic": 7}
+
+
+def load_polydisperse(solver, sc):
+    ids = [solver.add_shape(t["nodes"], t["sdf"], t["size"], t["origin"], t["spacing"]) for t in sc["templates"]]
+    shape = np.asarray(ids, np.int32)[sc["shape"]]
+    solver.add_particles(shape, sc["pos"], sc["quat"], sc["inv_mass"], sc["inv_inertia"], sc["kn"], sc["ks"],
+                         sc["mu"], sc["e"], vel=sc["vel"], scale=sc["scale"])
+    solver.set_periodic(sc["periodic"])

@@ -238,6 +238,7 @@ def main(outdir):
     Bk = np.abs(rng.normal(1.0, 0.3, size=(nbond, 4))) * np.array([1e4, 1e-2, 1e-2, 1e-2])
     geo = np.stack([np.full(nbond, 1e-3), np.full(nbond, 2e-4), rng.uniform(0, 2e5, nbond), rng.uniform(0, 2e5, nbond),
                     rng.uniform(0, 0.5, nbond)], 1)
+    geo[::3, 2:4] = 0.0  # zero tensile strength and cohesion: no failure check, these bonds survive
     frames = rng.normal(0, 1, size=(nbond, 8, 3))
     for a in (0, 1, 2, 4, 5, 6):
         frames[:, a] /= np.linalg.norm(frames[:, a], axis=1, keepdims=True)
