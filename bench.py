@@ -104,7 +104,7 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def build_scene(lsdem, workload: str, rank: int):
+def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000):
     from lsdem_b200 import scenes
     if workload == "small":
         sc = scenes.ellipsoid_falling(seed=scenes.seed_for(0) + rank)
@@ -119,10 +119,12 @@ def build_scene(lsdem, workload: str, rank: int):
         T = scenes.unit_templates(48, 2000)
         cache.parent.mkdir(exist_ok=True)
         np.savez(cache, T=np.array(T, dtype=object))
-    sc = scenes.polydisperse_periodic(lsdem, seed=scenes.seed_for(1) + rank, templates=T)
-    return sc, {"workload": "polydisperse-100k-4templates-periodic", "particles": 100000, "nodes_per_particle": 2000,
+    box = 0.1 * (particles / 1e5) ** (1.0 / 3.0)
+    sc = scenes.polydisperse_periodic(lsdem, n=particles, box=box, seed=scenes.seed_for(1) + rank, templates=T)
+    name = "polydisperse-100k-4templates-periodic" if particles == 100_000 else f"polydisperse-{particles}-4templates-periodic"
+    return sc, {"workload": name, "particles": particles, "nodes_per_particle": 2000,
                 "sdf_grid": "48^3 fp64", "templates": 4, "size": "lognormal(median 2 mm, sigma 0.25)",
-                "box_m": 0.1, "periodic": "xyz", "dt_s": 5e-7}
+                "box_m": round(box, 6), "periodic": "xyz", "dt_s": 5e-7}
 
 
 def load(lsdem, sc, workload, device):
@@ -188,10 +190,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     lsdem = _package()
-    sc, cfg = build_scene(lsdem, args.workload, 0)
-    vals = []
-    for _ in range(max(1, args.warmup and 1)):
-        pass
+    sc, cfg = build_scene(lsdem, args.workload, 0, args.particles)
     cb = cpu_baseline(lsdem, sc, args.workload, steps=max(1, min(args.steps, 3)))
     line = {"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
@@ -211,6 +210,7 @@ def main():
     ap.add_argument("--workload", default="polydisperse", choices=["polydisperse", "small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--particles", type=int, default=100_000, help="polydisperse workload size (profiling cases)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -234,7 +234,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     lsdem = _package()
-    sc, cfg = build_scene(lsdem, args.workload, rank)
+    sc, cfg = build_scene(lsdem, args.workload, rank, args.particles)
     sv = load(lsdem, sc, args.workload, local)
     n = sv.n_particles
     dt = float(sc["dt"])
@@ -322,6 +322,7 @@ def main():
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": n * (3 * 24 + 32),
                     "d2h_bytes_per_step": n * (5 * 24 + 32)},
             "gpu_launches": launches,
+            "overflow_reruns": sv.num(7),
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:

@@ -17,12 +17,14 @@ enum { FIX_GRADIENT = 1, FIX_SQRTF = 2 };
 // Overflow bits of the device status word.
 enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8 };
 
+// Largest demands seen during a batch (whether or not they overflowed), used
+// to grow capacities ahead of an overflow.
 struct Status {
   int flags;
-  int need_pp;       // largest per-particle particle-candidate count seen
+  int need_pp;       // largest per-particle particle-candidate count
   int need_wall;     // largest per-particle wall-candidate count
   int need_ghost;    // largest per-particle ghost-candidate count
-  int need_contact;  // largest contact total requested
+  int need_contact;  // largest contact total
   int pad[3];
 };
 
@@ -92,6 +94,8 @@ struct GhostView {
   int mask[7];         // axes of each set (bit 0 x, 1 y, 2 z)
   double3* gpos;       // nsets * n
   int* gkey;           // nsets * n, clamped cell or -1
+  int* list;           // nsets * n: visible images (set * n + particle), compacted
+  int* count;          // number of entries in list
 };
 
 struct BucketScratch {

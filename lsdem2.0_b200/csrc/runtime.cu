@@ -315,12 +315,13 @@ struct lsdem_solver {
   int cap_pp = 32, cap_w = 4, cap_g = 16;
   long long cap_c = 0;
   int batch = 16;
+  int cur_batch = 1;         // adaptive batch length, doubled after each clean batch
   bool record = false;
   // periodic
   int nsets = 0;
   int set_mask[7] = {0};
   DArr<double3> gpos;
-  DArr<int> gkey, key2, g2_idx, g2_start, g2_end;
+  DArr<int> gkey, key2, g2_idx, g2_start, g2_end, glist, gcount;
   // bonds
   DArr<int> b_ids, b_bonded;
   DArr<double> b_B, b_geo, b_state;
@@ -335,6 +336,7 @@ struct lsdem_solver {
   DArr<double3> bk_cspring;
   int bk_cap[3] = {0, 0, 0};
   long long hist_count = 0;  // contacts in the history buffer hp
+  bool grow_contacts = false;
   long long steps = 0, reruns = 0, launches = 0;
   double time = 0.0;
   // optional per-phase device timing (CUDA events on the solver stream)
@@ -620,6 +622,8 @@ void initialize(lsdem_solver* s) {
   if (s->nsets > 0) {
     CK(s->gpos.alloc((size_t)s->nsets * std::max(n, 1)));
     CK(s->gkey.alloc((size_t)s->nsets * std::max(n, 1)));
+    CK(s->glist.alloc((size_t)s->nsets * std::max(n, 1)));
+    CK(s->gcount.alloc(1));
     CK(s->key2.alloc(std::max(n, 1)));
     CK(s->g2_idx.alloc(std::max(n, 1)));
     CK(s->g2_start.alloc(s->pg.ncells));
@@ -692,6 +696,8 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   for (int k = 0; k < 7; ++k) a.G.mask[k] = s->set_mask[k];
   a.G.gpos = s->gpos.p;
   a.G.gkey = s->gkey.p;
+  a.G.list = s->glist.p;
+  a.G.count = s->gcount.p;
   a.status = s->status.p;
   a.dt = dt;
   a.gravity = make_double3(s->grav[0], s->grav[1], s->grav[2]);
@@ -840,22 +846,40 @@ void restore(lsdem_solver* s, int hp0) {
   cp(s->con[hp0].spring, s->bk_cspring, nc);
 }
 
-// Grows capacities after an overflow. Slot arrays of both parities and both
-// contact lists are reallocated (their contents come back from the backup).
-void grow(lsdem_solver* s, const Status& st) {
-  if (st.flags & OVF_PP) s->cap_pp = std::max(s->cap_pp * 2, st.need_pp + st.need_pp / 4 + 1);
-  if (st.flags & OVF_WALL) s->cap_w = std::max(s->cap_w * 2, st.need_wall + 1);
-  if (st.flags & OVF_GHOST) s->cap_g = std::max(s->cap_g * 2, st.need_ghost + st.need_ghost / 4 + 1);
-  if (st.flags & OVF_CONTACT)
-    s->cap_c = std::max<long long>(s->cap_c * 2, (long long)st.need_contact + st.need_contact / 4 + 1);
-  // history slots must keep the old contents until restore: they are restored from backup
+// New capacities from the largest demands of the last batch: a capacity
+// grows when it overflowed or when the demand passed 80 % of it (so that the
+// next batch is unlikely to overflow). Returns true when any capacity changes.
+bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
+  bool changed = false;
+  auto up = [&](int& cap, int need, bool ovf) {
+    if (ovf || need * 5 > cap * 4) {
+      const int nc = std::max(cap * 2, need + need / 2 + 4);
+      if (nc != cap) { cap = nc; changed = true; }
+    }
+  };
+  up(s->cap_pp, st.need_pp, st.flags & OVF_PP);
+  if (s->W.n() > 0) up(s->cap_w, st.need_wall, st.flags & OVF_WALL);
+  if (s->nsets > 0) up(s->cap_g, st.need_ghost, st.flags & OVF_GHOST);
+  const long long needc = std::max<long long>(st.need_contact, last_contacts);
+  if ((st.flags & OVF_CONTACT) || needc * 5 > s->cap_c * 4) {
+    s->cap_c = std::max<long long>(s->cap_c * 2, needc + needc / 2 + 1024);
+    changed = true;
+    s->grow_contacts = true;
+  }
+  return changed;
+}
+
+// Reallocates slot arrays of both parities (and both contact lists when they
+// grow); their contents come back from the backup by restore().
+void grow(lsdem_solver* s) {
   alloc_slots(s);
-  if (st.flags & OVF_CONTACT) {
+  if (s->grow_contacts) {
     const bool g0 = s->con[0].geom, g1 = s->con[1].geom;
     alloc_contacts(s, s->con[0], s->cap_c);
     alloc_contacts(s, s->con[1], s->cap_c);
     if (g0) ensure_geom(s, s->con[0]);
     if (g1) ensure_geom(s, s->con[1]);
+    s->grow_contacts = false;
   }
 }
 
@@ -865,9 +889,10 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
   cudaStream_t st = s->stream;
   long long done = 0;
   while (done < nsteps) {
-    const long long B = std::min<long long>(s->batch, nsteps - done);
+    const long long B = std::min<long long>(std::max(1, std::min(s->cur_batch, s->batch)), nsteps - done);
     const int hp0 = s->hp;
     backup(s);
+    Status stat{};
     for (int attempt = 0;; ++attempt) {
       CK(cudaMemsetAsync(s->status.p, 0, sizeof(Status), st));
       double t = s->time;
@@ -879,20 +904,31 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
       CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(Status), cudaMemcpyDeviceToHost, st));
       CK(cudaMemcpyAsync(s->h_count, s->con[s->hp].count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
-      const Status stat = *s->h_status;
+      stat = *s->h_status;
       resolve_profile(s, stat.flags == 0);
       if (stat.flags == 0) {
         s->hist_count = *s->h_count;
         break;
       }
       if (attempt > 8) throw Fail{LSDEM_ERR_NOMEM, "capacity growth did not converge"};
-      grow(s, stat);
+      plan_growth(s, stat, *s->h_count);
+      grow(s);
       restore(s, hp0);
       s->reruns++;
+      s->cur_batch = 1;
     }
     done += B;
     s->steps += B;
     s->time += dt * (double)B;
+    // grow ahead of an overflow: keep the history just written
+    if (plan_growth(s, stat, s->hist_count)) {
+      const int hp1 = s->hp;
+      backup(s);
+      grow(s);
+      restore(s, hp1);
+    } else {
+      s->cur_batch = std::min(s->batch, s->cur_batch * 2);
+    }
   }
   return LSDEM_OK;
 }

@@ -49,7 +49,12 @@ LD double coord_slack(double3 a, double3 b) {
 // Integration, first half of the step (reference step order, LSSolver.h:1000-1011).
 __global__ void k_integrate_first(StepArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *a.C.count = 0;
+  if (i == 0) {
+    // contacts of the previous step: largest demand of the batch, then reset
+    if (a.C_old.count) atomicMax(&a.status->need_contact, *a.C_old.count);
+    *a.C.count = 0;
+    if (a.G.count) *a.G.count = 0;
+  }
   if (i < a.P.n) {
     const BodyView& P = a.P;
     const double h = 0.5 * a.dt;
@@ -126,9 +131,7 @@ LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
 // node's 27-cell window since cells are at least 2 max radius wide).
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
-__global__ void k_candidates(StepArgs a) {
-  const int A = blockIdx.x * blockDim.x + threadIdx.x;
-  if (A >= a.P.n) return;
+LD void candidates_of(const StepArgs& a, int A, int& n_out, int& nw_out) {
   const double3 xA = a.P.pos[A];
   const double rA = a.P.radius[A];
   const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
@@ -161,10 +164,8 @@ __global__ void k_candidates(StepArgs a) {
     }
   }
   a.pp.cnt[A] = n < cap ? n : cap;
-  if (n > cap) {
-    atomicOr(&a.status->flags, OVF_PP);
-    atomicMax(&a.status->need_pp, n);
-  }
+  if (n > cap) atomicOr(&a.status->flags, OVF_PP);
+  n_out = n;
   // walls
   int nw = 0;
   const int capw = a.pw.cap;
@@ -179,11 +180,23 @@ __global__ void k_candidates(StepArgs a) {
     ++nw;
   }
   if (capw > 0) a.pw.cnt[A] = nw < capw ? nw : capw;
-  if (nw > capw) {
-    atomicOr(&a.status->flags, OVF_WALL);
-    atomicMax(&a.status->need_wall, nw);
+  if (nw > capw) atomicOr(&a.status->flags, OVF_WALL);
+  nw_out = nw;
+}
+
+__global__ void k_candidates(StepArgs a) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  int npp = 0, nwall = 0;
+  if (A < a.P.n) candidates_of(a, A, npp, nwall);
+  // largest demand of the warp, one atomic per warp
+  npp = __reduce_max_sync(FULL, npp);
+  nwall = __reduce_max_sync(FULL, nwall);
+  if ((threadIdx.x & 31) == 0) {
+    if (npp > 0) atomicMax(&a.status->need_pp, npp);
+    if (nwall > 0) atomicMax(&a.status->need_wall, nwall);
   }
 }
+
 
 void launch_candidates(const StepArgs& a, cudaStream_t s) {
   if (a.P.n > 0) k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
@@ -420,10 +433,7 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
   __syncwarp();
   const size_t sidx = (size_t)A * cur.cap + slot;
   int base = 0;
-  if (lane == 0 && total > 0) {
-    base = atomicAdd(a.C.count, total);
-    atomicMax(&a.status->need_contact, base + total);
-  }
+  if (lane == 0 && total > 0) base = atomicAdd(a.C.count, total);
   base = __shfl_sync(FULL, base, 0);
   const bool can_write = (base + total <= a.C.cap);
   if (lane == 0) {
@@ -524,10 +534,12 @@ __global__ void __launch_bounds__(NP_WARPS * 32) k_narrowphase(StepArgs a) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int ng_max = 0;
   for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
     const int npp = (KINDS & 1) ? a.pp.cnt[A] : 0;
     const int nw = (KINDS & 2) ? (a.pw.cap > 0 ? a.pw.cnt[A] : 0) : 0;
     const int ng = (KINDS & 4) ? a.pgh.cnt[A] : 0;
+    ng_max = ng > ng_max ? ng : ng_max;
     const int ngc = ng < a.pgh.cap ? ng : a.pgh.cap;
     if (npp + nw + ngc == 0) continue;
     SelfCtx S;
@@ -552,6 +564,7 @@ __global__ void __launch_bounds__(NP_WARPS * 32) k_narrowphase(StepArgs a) {
       atomic_add3(a.P.torque, A, TA);
     }
   }
+  if ((KINDS & 4) && lane == 0 && ng_max > 0) atomicMax(&a.status->need_ghost, ng_max);
 }
 
 static int g_num_sms = 0;
@@ -641,46 +654,61 @@ void launch_clamped_keys(const StepArgs& a, int* key2, cudaStream_t s) {
   if (a.P.n > 0) k_clamped_keys<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, key2);
 }
 
-// Ghost partners, searched from each visible ghost image G: a node of A can
+// Visible images (ghost key >= 0) are compacted into a list first: only a
+// few percent of (set, particle) pairs are images, so a thread per pair would
+// leave almost every lane idle.
+__global__ void k_ghost_compact(StepArgs a) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool vis = t < (long long)a.G.nsets * a.P.n && a.G.gkey[t] >= 0;
+  const unsigned m = __ballot_sync(FULL, vis);
+  if (m == 0) return;
+  int base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == __ffs(m) - 1) base = atomicAdd(a.G.count, __popc(m));
+  base = __shfl_sync(FULL, base, __ffs(m) - 1);
+  if (vis) a.G.list[base + __popc(m & lanemask_lt())] = (int)t;
+}
+
+// Ghost partners, searched with one warp per visible image G: a node of A can
 // only reach G's cell window when A's clamped cell is within 2 cells of G's
-// cell, and only when A's bounding sphere reaches G's SDF grid box.
+// cell, and only when A's bounding sphere reaches G's SDF grid box. The lanes
+// walk the occupants of those cells.
 __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, const int* __restrict__ g2_start,
                                    const int* __restrict__ g2_end) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int nvis = *a.G.count;
   const int n = a.P.n;
-  if (t >= (long long)a.G.nsets * n) return;
-  const int s = (int)(t / n), i = (int)(t % n);
-  const int gk = a.G.gkey[t];
-  if (gk < 0) return;
-  const double3 xg = a.G.gpos[t];
   const GridP& g = a.pg;
-  const int cx = gk % g.size.x, cy = (gk / g.size.x) % g.size.y, cz = gk / (g.size.x * g.size.y);
-  // circumradius of the ghost's SDF grid box about its centre
-  double3 lo, hi;
-  grid_box(a.P.origin[i], a.P.invh[i], a.S.gsize[a.P.shape[i]], lo, hi);
-  const double3 far = d3(fmax(fabs(lo.x), fabs(hi.x)), fmax(fabs(lo.y), fabs(hi.y)), fmax(fabs(lo.z), fabs(hi.z)));
-  const double Rg = len(far);
-  const int pid = (i << 3) | s;
-  for (int z = cz - 2; z <= cz + 2; ++z) {
-    if (z < 0 || z >= g.size.z) continue;
-    for (int y = cy - 2; y <= cy + 2; ++y) {
-      if (y < 0 || y >= g.size.y) continue;
-      for (int x = cx - 2; x <= cx + 2; ++x) {
-        if (x < 0 || x >= g.size.x) continue;
-        const int h = lin3(make_int3(x, y, z), g.size);
-        const int st = g2_start[h];
-        if (st < 0) continue;
-        const int en = g2_end[h];
-        for (int k = st; k < en; ++k) {
-          const int A = g2_idx[k];
-          const double3 xA = a.P.pos[A];
-          const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
-          if (len2(xA - xg) > R * R) continue;
-          const int slot = atomicAdd(&a.pgh.cnt[A], 1);
-          if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
-          else {
-            atomicOr(&a.status->flags, OVF_GHOST);
-            atomicMax(&a.status->need_ghost, slot + 1);
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nvis; v += (gridDim.x * blockDim.x) >> 5) {
+    const int t = a.G.list[v];
+    const int s = t / n, i = t % n;
+    const int gk = a.G.gkey[t];
+    const double3 xg = a.G.gpos[t];
+    const int cx = gk % g.size.x, cy = (gk / g.size.x) % g.size.y, cz = gk / (g.size.x * g.size.y);
+    // circumradius of the image's SDF grid box about its centre
+    double3 lo, hi;
+    grid_box(a.P.origin[i], a.P.invh[i], a.S.gsize[a.P.shape[i]], lo, hi);
+    const double3 far = d3(fmax(fabs(lo.x), fabs(hi.x)), fmax(fabs(lo.y), fabs(hi.y)), fmax(fabs(lo.z), fabs(hi.z)));
+    const double Rg = len(far);
+    const int pid = (i << 3) | s;
+    for (int z = cz - 2; z <= cz + 2; ++z) {
+      if (z < 0 || z >= g.size.z) continue;
+      for (int y = cy - 2; y <= cy + 2; ++y) {
+        if (y < 0 || y >= g.size.y) continue;
+        for (int x = cx - 2; x <= cx + 2; ++x) {
+          if (x < 0 || x >= g.size.x) continue;
+          const int h = lin3(make_int3(x, y, z), g.size);
+          const int st = g2_start[h];
+          if (st < 0) continue;
+          const int en = g2_end[h];
+          for (int k = st + lane; k < en; k += 32) {
+            const int A = g2_idx[k];
+            const double3 xA = a.P.pos[A];
+            const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
+            if (len2(xA - xg) > R * R) continue;
+            const int slot = atomicAdd(&a.pgh.cnt[A], 1);
+            if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
+            else atomicOr(&a.status->flags, OVF_GHOST);
           }
         }
       }
@@ -691,7 +719,10 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
 void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,
                              const int* /*g2_key*/, cudaStream_t s) {
   long long n = (long long)a.G.nsets * a.P.n;
-  if (n > 0) k_ghost_candidates<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, g2_idx, g2_start, g2_end);
+  if (n <= 0) return;
+  k_ghost_compact<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+  int blocks = num_sms() * 16;
+  k_ghost_candidates<<<blocks, 128, 0, s>>>(a, g2_idx, g2_start, g2_end);
 }
 
 // ---------------------------------------------------------------------------
