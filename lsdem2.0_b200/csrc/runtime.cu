@@ -454,7 +454,7 @@ void push_body(lsdem_solver* s, BodyHost& B, int shape, double scale, const doub
 
 // ---------------------------------------------------------------------------
 // Device set-up.
-void alloc_slots(lsdem_solver* s) {
+void alloc_slots(lsdem_solver* s, bool keep_unchanged = false) {
   const int n = s->P.n();
   const int caps[3] = {s->cap_pp, s->P.n() ? s->cap_w : 0, s->cap_g};
   for (int h = 0; h < 2; ++h)
@@ -466,10 +466,12 @@ void alloc_slots(lsdem_solver* s) {
         sl.cnt.release(); sl.id.release(); sl.seg_start.release(); sl.seg_cnt.release();
         continue;
       }
+      const size_t m = (size_t)std::max(n, 1) * std::max(cap, 1);
+      // unchanged kind: keep the arrays (restore rewrites their contents)
+      if (keep_unchanged && sl.cap == cap && sl.id.n == m && sl.cnt.n == (size_t)std::max(n, 1)) continue;
       sl.cap = cap;
       CK(sl.cnt.alloc((size_t)std::max(n, 1)));
       CK(sl.cnt.zero(s->stream));
-      const size_t m = (size_t)std::max(n, 1) * std::max(cap, 1);
       CK(sl.id.alloc(m));
       CK(sl.seg_start.alloc(m));
       CK(sl.seg_cnt.alloc(m));
@@ -630,7 +632,7 @@ void initialize(lsdem_solver* s) {
     CK(s->g2_end.alloc(s->pg.ncells));
   }
   // history buffers
-  if (s->cap_c <= 0) s->cap_c = std::max<long long>(1 << 16, (long long)n * 64);
+  if (s->cap_c <= 0) s->cap_c = std::max<long long>(1 << 16, (long long)n * 128);
   alloc_slots(s);
   alloc_contacts(s, s->con[0], s->cap_c);
   alloc_contacts(s, s->con[1], s->cap_c);
@@ -795,8 +797,9 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
 void backup(lsdem_solver* s) {
   cudaStream_t st = s->stream;
   const size_t n = (size_t)s->P.n(), nw = (size_t)s->W.n();
+  // backup buffers grow geometrically (never per batch: a free synchronises the device)
   auto cp = [&](auto& dst, auto& src, size_t m) {
-    if (dst.n < m) CK(dst.alloc(m));
+    if (dst.n < m) CK(dst.alloc(std::max(m + m / 2, (size_t)1024)));
     if (m) CK(cudaMemcpyAsync(dst.p, src.p, m * sizeof(*src.p), cudaMemcpyDeviceToDevice, st));
   };
   cp(s->bk_pos, s->dP.pos, n); cp(s->bk_vel, s->dP.vel, n); cp(s->bk_angvel, s->dP.angvel, n);
@@ -872,7 +875,7 @@ bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
 // Reallocates slot arrays of both parities (and both contact lists when they
 // grow); their contents come back from the backup by restore().
 void grow(lsdem_solver* s) {
-  alloc_slots(s);
+  alloc_slots(s, true);
   if (s->grow_contacts) {
     const bool g0 = s->con[0].geom, g1 = s->con[1].geom;
     alloc_contacts(s, s->con[0], s->cap_c);
