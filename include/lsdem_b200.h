@@ -188,6 +188,23 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4);
 int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic,
                    unsigned long long seed, int max_tries, double* pos_out);
 
+/* Broadphase cell sort that allocates no device memory: cell keys of n body
+ * centres (pos_dev: device array of n x 3 doubles), their stable sorted order
+ * and per-cell [start, end) (-1 when empty) for the grid (min, max, inverse
+ * cell size, cell counts), written to caller-provided device arrays
+ * (sorted_key_dev may be NULL) on `stream` (a cudaStream_t, NULL = legacy default).
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory when they call in (latency-critical loops in which an allocation
+ * may block or synchronise, hosts whose device memory belongs to their own pool
+ * or fixed budget). Its scratch is one fixed device array of the library, which
+ * limits a call to 262,144 bodies and 262,144 cells (LSDEM_ERR_ARG beyond, with
+ * a message on stderr). The first call on a device looks up that array's device
+ * address, so it should come before any stream capture. All calls share the
+ * array; calls that overlap on the GPU race. */
+int lsdem_cell_sort_static(const void* pos_dev, int n, const double* min3, const double* max3, const double* inv3,
+                           const int* size3, int* key_dev, int* sorted_idx_dev, int* sorted_key_dev,
+                           int* cell_start_dev, int* cell_end_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

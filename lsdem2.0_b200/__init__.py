@@ -93,6 +93,7 @@ _SIGS = {
     "lsdem_get_profile": (C.c_int, [P, DP, LP]),
     "lsdem_step_stats": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, DP]),
+    "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
