@@ -121,6 +121,10 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000):
         np.savez(cache, T=np.array(T, dtype=object))
     box = 0.1 * (particles / 1e5) ** (1.0 / 3.0)
     sc = scenes.polydisperse_periodic(lsdem, n=particles, box=box, seed=scenes.seed_for(1) + rank, templates=T)
+    # deep initial overlaps (many surface nodes inside a neighbour) would exceed the stability
+    # limit of the explicit step; re-place those particles, keep shallow contacts
+    iters = scenes.resolve_deep_overlaps(lsdem, sc, device=int(os.environ.get("LOCAL_RANK", "0")))
+    sc["resolve_iterations"] = iters
     name = "polydisperse-100k-4templates-periodic" if particles == 100_000 else f"polydisperse-{particles}-4templates-periodic"
     return sc, {"workload": name, "particles": particles, "nodes_per_particle": 2000,
                 "sdf_grid": "48^3 fp64", "templates": 4, "size": "lognormal(median 2 mm, sigma 0.25)",

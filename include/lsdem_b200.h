@@ -101,6 +101,16 @@ int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3,
 int lsdem_create_bonds_from_contacts(lsdem_solver* s, double radius, double initial_length, double youngs,
                                      double poisson, double tensile, double cohesion, double mu);
 
+/* Arithmetic form of the narrowphase and contact forces (no counterpart in the
+ * reference, which is FP64 throughout): LSDEM_PREC_FP64 (default, the reference's
+ * arithmetic), LSDEM_PREC_FP32_FP16 / LSDEM_PREC_FP32_BF16 (FP32 geometry and contact
+ * law on SDF templates stored as phi / spacing in FP16 / BF16; positions, quaternions,
+ * integration and the tangential-spring history stay FP64). Takes effect at initialize. */
+#define LSDEM_PREC_FP64 0
+#define LSDEM_PREC_FP32_FP16 1
+#define LSDEM_PREC_FP32_BF16 2
+int lsdem_set_precision(lsdem_solver* s, int mode);
+
 /* Periodic axes bit mask (bit 0 x, 1 y, 2 z). x and y follow
  * addPeriodicBoundaryXD/YD (LSSolver.h:426-447); z applies the same rule. 0 removes
  * periodicity (removePeriodicBoundary, LSSolver.h:459-464). */
@@ -184,9 +194,10 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4);
 
 /* Scene set-up helper: random sequential addition of spheres (in the given
  * order) in [lo, hi), periodic or not (the reference's sphere-packing helper,
- * FunDEM/kernel/helper/SpherePackingGenerator.h:75-217, does the same job on the host). */
+ * FunDEM/kernel/helper/SpherePackingGenerator.h:75-217, does the same job on the host).
+ * keep (nullable): spheres with keep[i] != 0 stay at pos_out[i] and are placed around. */
 int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic,
-                   unsigned long long seed, int max_tries, double* pos_out);
+                   unsigned long long seed, int max_tries, const int* keep, double* pos_out);
 
 /* Broadphase cell sort that allocates no device memory: cell keys of n body
  * centres (pos_dev: device array of n x 3 doubles), their stable sorted order

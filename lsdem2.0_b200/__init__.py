@@ -22,6 +22,7 @@ OK = 0
 FIX_GRADIENT = 1
 FIX_SQRTF = 2
 CONTACT_PARTICLE, CONTACT_WALL, CONTACT_GHOST = 0, 1, 2
+PREC_FP64, PREC_FP32_FP16, PREC_FP32_BF16 = 0, 1, 2
 
 _ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "call out of order",
            5: "no CUDA device"}
@@ -68,6 +69,7 @@ _SIGS = {
     "lsdem_create_bonds_from_contacts": (C.c_int, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                                    C.c_double, C.c_double]),
     "lsdem_set_periodic": (C.c_int, [P, C.c_int]),
+    "lsdem_set_precision": (C.c_int, [P, C.c_int]),
     "lsdem_initialize": (C.c_int, [P, DP, DP, DP]),
     "lsdem_step": (C.c_int, [P, C.c_double, C.c_longlong, HOOK, P]),
     "lsdem_set_record_contacts": (C.c_int, [P, C.c_int]),
@@ -92,7 +94,7 @@ _SIGS = {
     "lsdem_set_profiling": (C.c_int, [P, C.c_int]),
     "lsdem_get_profile": (C.c_int, [P, DP, LP]),
     "lsdem_step_stats": (C.c_int, [P, LP]),
-    "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, DP]),
+    "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
 }
 for _name, (_res, _args) in _SIGS.items():
@@ -125,11 +127,14 @@ def _ip(a):
     return None if a is None else a.ctypes.data_as(IP)
 
 
-def pack_rsa(radius, lo, hi, periodic=False, seed=12345, max_tries=1000):
-    """Random sequential addition of spheres with the given radii (placed in order)."""
+def pack_rsa(radius, lo, hi, periodic=False, seed=12345, max_tries=1000, keep=None, pos=None):
+    """Random sequential addition of spheres with the given radii (placed in order); with `keep`,
+    spheres where keep is nonzero stay at `pos` and the others are placed around them."""
     r = np.ascontiguousarray(radius, np.float64)
-    out = np.zeros((len(r), 3))
-    rc = lib.lsdem_pack_rsa(len(r), _d(r), _d(lo), _d(hi), 1 if periodic else 0, int(seed), int(max_tries), _dp(out))
+    out = np.zeros((len(r), 3)) if pos is None else np.array(pos, np.float64, copy=True, order="C")
+    kp = None if keep is None else np.ascontiguousarray(keep, np.int32)
+    rc = lib.lsdem_pack_rsa(len(r), _d(r), _d(lo), _d(hi), 1 if periodic else 0, int(seed), int(max_tries),
+                            _ip(kp), _dp(out))
     if rc:
         raise LSDEMError(rc, "pack_rsa: could not place every sphere")
     return out
@@ -228,6 +233,10 @@ class Solver:
         self._chk(lib.lsdem_create_bonds_from_contacts(self.h, float(radius), float(length), float(youngs),
                                                        float(poisson), float(tensile), float(cohesion), float(mu)),
                   "create_bonds_from_contacts")
+
+    def set_precision(self, mode: int):
+        """PREC_FP64 (default), PREC_FP32_FP16 or PREC_FP32_BF16; takes effect at initialize."""
+        self._chk(lib.lsdem_set_precision(self.h, int(mode)), "set_precision")
 
     def set_periodic(self, axes: int):
         self._chk(lib.lsdem_set_periodic(self.h, int(axes)), "set_periodic")

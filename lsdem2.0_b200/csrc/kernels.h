@@ -40,7 +40,13 @@ struct ShapeView {
   const double3* node_pos;    // node store, cluster order, unscaled
   const int* node_orig;       // original node index within the shape
   const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
+  // precision form: SDF values / template spacing in 16-bit floats, FP32 nodes
+  const unsigned short* sdf16;  // same offsets as sdf; FP16 or BF16 bits
+  const float4* node_pos_f;     // FP32 copy of node_pos
 };
+
+// Arithmetic form of the narrowphase and contact forces.
+enum { PREC_FP64 = 0, PREC_FP32_FP16 = 1, PREC_FP32_BF16 = 2 };
 
 // A set of rigid bodies (particles or walls).
 struct BodyView {
@@ -131,6 +137,7 @@ struct StepArgs {
   double dt;
   double3 gravity;
   int flags;        // FIX_* bits
+  int precision;    // PREC_*
 };
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);

@@ -17,6 +17,8 @@
 #include <unordered_map>
 #include <vector>
 #include "../../include/lsdem_b200.h"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include "kernels.h"
 
 using namespace lsdem;
@@ -287,6 +289,7 @@ struct lsdem_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
   int flags = 0;
+  int precision = PREC_FP64;
   std::string err;
   // model
   std::vector<ShapeHost> shapes;
@@ -305,6 +308,8 @@ struct lsdem_solver {
   DArr<int> s_node_off, s_node_cnt, s_cl_off, s_cl_cnt, s_node_orig;
   DArr<double3> s_node_pos;
   DArr<double4> s_cl;
+  DArr<unsigned short> s_sdf16;
+  DArr<float4> s_node_f;
   std::vector<int> h_node_off, h_cl_off;
   GridP pg{}, wg{};
   DArr<int> cell_idx, cell_start, cell_end, sorted_key;
@@ -594,6 +599,27 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_pos.upload(node_pos.data(), node_pos.size(), st));
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
+  if (s->precision != PREC_FP64) {
+    // precision form: phi / h of each template in 16 bits, FP32 node copy
+    std::vector<unsigned short> sdf16(sdf.size());
+    size_t k = 0;
+    for (const ShapeHost& sh : s->shapes)
+      for (double v : sh.sdf) {
+        const float u = (float)(v / sh.h);
+        if (s->precision == PREC_FP32_BF16) {
+          const __nv_bfloat16 b = __float2bfloat16_rn(u);
+          std::memcpy(&sdf16[k++], &b, 2);
+        } else {
+          const __half hh = __float2half_rn(u);
+          std::memcpy(&sdf16[k++], &hh, 2);
+        }
+      }
+    std::vector<float4> nf(node_pos.size());
+    for (size_t i = 0; i < node_pos.size(); ++i)
+      nf[i] = make_float4((float)node_pos[i].x, (float)node_pos[i].y, (float)node_pos[i].z, 0.f);
+    CK(s->s_sdf16.upload(sdf16.data(), sdf16.size(), st));
+    CK(s->s_node_f.upload(nf.data(), nf.size(), st));
+  }
   // node ids (LSBoundaryNode order: particle by particle, caller node order)
   s->P.node_base.resize(s->P.n());
   long long nb = 0;
@@ -673,6 +699,8 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.node_off = s->s_node_off.p; a.S.node_cnt = s->s_node_cnt.p; a.S.cl_off = s->s_cl_off.p;
   a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
   a.S.cl_sphere = s->s_cl.p;
+  a.S.sdf16 = s->s_sdf16.p;
+  a.S.node_pos_f = s->s_node_f.p;
   a.pg = s->pg;
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
@@ -704,6 +732,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.dt = dt;
   a.gravity = make_double3(s->grav[0], s->grav[1], s->grav[2]);
   a.flags = s->flags;
+  a.precision = s->precision;
   return a;
 }
 
@@ -785,10 +814,10 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
   }
   if (hook) hook(user, t);
   { PhaseTimer pt(s, 7); launch_kick(a, st); }
-  // kernels launched by this step: kick/drift/keys, cell sort (8), candidates,
-  // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (7),
-  // ghost candidates, ghost narrowphase; bonds
-  if (a.P.n > 0) s->launches += 12 + (s->nsets > 0 ? 11 : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  // kernels launched by this step: kick/drift/keys, cell sort (9), candidates,
+  // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (8),
+  // image compaction + candidates, ghost narrowphase; bonds
+  if (a.P.n > 0) s->launches += 13 + (s->nsets > 0 ? 13 : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
 }
@@ -1142,6 +1171,13 @@ int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3,
   return add_bond_impl(s, master, slave, &s->P.pos[3 * (size_t)master], &s->P.quat[4 * (size_t)master],
                        &s->P.pos[3 * (size_t)slave], &s->P.quat[4 * (size_t)slave], point3, normal3, radius,
                        initial_length, youngs, poisson, tensile, cohesion, mu);
+}
+
+int lsdem_set_precision(lsdem_solver* s, int mode) {
+  if (!s || mode < PREC_FP64 || mode > PREC_FP32_BF16) return LSDEM_ERR_ARG;
+  s->precision = mode;
+  s->ready = false;
+  return LSDEM_OK;
 }
 
 int lsdem_set_periodic(lsdem_solver* s, int axes) {
@@ -1526,7 +1562,7 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4) {
 // in the box [lo, hi), optionally periodic, using a uniform cell list.
 // Returns LSDEM_ERR_ARG when a sphere cannot be placed in max_tries.
 int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic, unsigned long long seed,
-                   int max_tries, double* pos_out) {
+                   int max_tries, const int* keep, double* pos_out) {
   if (n < 0 || !radius || !lo || !hi || !pos_out) return LSDEM_ERR_ARG;
   if (n == 0) return LSDEM_OK;
   double rmax = 0.;
@@ -1547,7 +1583,20 @@ int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* 
     z ^= z >> 31;
     return (double)(z >> 11) * (1.0 / 9007199254740992.0);
   };
+  auto cell_index = [&](const double* p) {
+    int c[3];
+    for (int a = 0; a < 3; ++a) {
+      double u = (p[a] - lo[a]) / L[a];
+      if (periodic) u -= std::floor(u);
+      c[a] = std::min(dims[a] - 1, std::max(0, (int)(u * dims[a])));
+    }
+    return ((size_t)c[2] * dims[1] + c[1]) * dims[0] + c[0];
+  };
+  if (keep)
+    for (int i = 0; i < n; ++i)
+      if (keep[i]) cells[cell_index(pos_out + 3 * (size_t)i)].push_back(i);
   for (int i = 0; i < n; ++i) {
+    if (keep && keep[i]) continue;
     const double r = radius[i];
     bool placed = false;
     for (int t = 0; t < max_tries && !placed; ++t) {

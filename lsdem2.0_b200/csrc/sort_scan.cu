@@ -141,8 +141,35 @@ __global__ void k_bucket_scatter(const int* __restrict__ key, int n, int ncells,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int b = bucket_of(key[i], ncells);
+  if (b == 0 || b == ncells + 1) return;  // placed in index order by k_special_buckets
   int p = offs[b] + atomicAdd(&fill[b], 1);
   sorted_idx[p] = i;
+}
+
+// Bodies outside every cell (bucket 0: key -1; last bucket: key past the last
+// cell) can be numerous, e.g. bodies that left a non-periodic domain, so they
+// are placed directly in ascending index order by one block walking the bodies
+// in tiles: two block-wide scans of the membership flags give each member its
+// rank. Exits at once when both buckets are empty.
+__global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells, const int* __restrict__ offs,
+                                  int* __restrict__ sorted_idx) {
+  __shared__ int sw[32];
+  const int L = ncells + 1;
+  const int n0 = offs[1] - offs[0], nL = offs[L + 1] - offs[L];
+  if (n0 == 0 && nL == 0) return;
+  int base0 = offs[0], baseL = offs[L];
+  for (int t0 = 0; t0 < n; t0 += blockDim.x) {
+    const int i = t0 + threadIdx.x;
+    const int b = i < n ? bucket_of(key[i], ncells) : -1;
+    const int f0 = b == 0, fL = b == L;
+    int tot0, totL;
+    const int r0 = block_exclusive_scan<int>(f0, sw, &tot0);
+    const int rL = block_exclusive_scan<int>(fL, sw, &totL);
+    if (f0) sorted_idx[base0 + r0] = i;
+    if (fL) sorted_idx[baseL + rL] = i;
+    base0 += tot0;
+    baseL += totL;
+  }
 }
 
 // One thread per bucket: restore ascending particle order inside the bucket
@@ -159,7 +186,7 @@ __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int nce
     start[b - 1] = L > 0 ? s : -1;
     end[b - 1] = L > 0 ? e : -1;
   }
-  if (L <= 1) return;
+  if (L <= 1 || b == 0 || b == ncells + 1) return;  // special buckets are already in index order
   if (L > 64) {
     int slot = atomicAdd(big_count, 1);
     big_list[slot] = b;
@@ -205,7 +232,10 @@ void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorte
   if (n > 0) k_bucket_hist<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.counts);
   // exclusive scan over nb + 1 entries: offs[nb] = n
   scan_i32(w.counts, w.offs, nb + 1, w.scan_tmp, false, s);
-  if (n > 0) k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx);
+  if (n > 0) {
+    k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx);
+    k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx);
+  }
   k_bucket_fix<<<(nb + 255) / 256, 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list, w.big_count);
   // at most n / 65 buckets can exceed 64 members
   int max_big = n / 65 + 1;

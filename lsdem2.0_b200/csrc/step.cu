@@ -13,6 +13,8 @@
 //   k_kick             second half kick (particleIntegrationKernel.cu:3-24)
 //   k_periodic         wrap + ghost images + ghost keys (mySpatialGrid.cu:28-56, 87-152, 214-240)
 //   k_bonds            V-bond forces (contactKernel.cuh:138-199, contactKernel.cu:273-351)
+#include <cuda_fp16.h>
+
 #include "kernels.h"
 
 namespace lsdem {
@@ -20,6 +22,7 @@ namespace lsdem {
 static constexpr unsigned FULL = 0xffffffffu;
 static constexpr int NP_WARPS = 4;     // warps per narrowphase block
 static constexpr int MAXCL = 256;      // clusters of 32 nodes per shape (8192 nodes)
+static constexpr int OLDCAP = 256;     // previous-segment node ids staged in shared memory per warp
 
 LD unsigned lanemask_lt() {
   unsigned m;
@@ -210,9 +213,14 @@ enum { KIND_PP = 0, KIND_WALL = 1, KIND_GHOST = 2 };
 struct SelfCtx {
   double3 x, v, w;
   Quat q;
-  Mat3 R;
-  double sc, invm, kn, ks, mu, res;
+  double sc;
   int n0, nn, cl0, ncl;
+};
+
+// Contact constants of one pair (contactKernel.cu:99-104 / :176-179 and the damping
+// terms of LinearContact, contactKernel.cuh:50-58), evaluated once per pair.
+struct PairK {
+  double kn, ks, mu, cn, cs;
 };
 
 // The SDF side of a test.
@@ -344,33 +352,53 @@ LD bool cluster_may_hit(double3 wc, double rad, const Partner& P) {
 
 LD double sqrt_damp(double v, int flags) { return (flags & FIX_SQRTF) ? sqrt(v) : (double)sqrtf((float)v); }
 
-// integrateSlidingSpring + LinearContact (contactKernel.cuh:4-77).
-LD void linear_contact(double3& F, double3& spring, double3 vc, double3 n, double delta, double dt, double kn,
-                       double ks, double mu, double e, double effM, int flags) {
+template <int KIND>
+LD PairK pair_constants(const StepArgs& a, int A, const Partner& P) {
+  const double invmA = a.P.invmass[A], knA = a.P.kn[A], ksA = a.P.ks[A], muA = a.P.mu[A], resA = a.P.res[A];
+  double kn = 0., ks = 0., effM = 0., mu, res;
+  if (KIND == KIND_WALL) {
+    kn = knA; ks = ksA;
+    if (invmA > 0.) effM = 1. / invmA;
+    mu = fmin(muA, P.mu);
+    res = fmin(resA, P.res);
+  } else {
+    if (knA > 0. && P.kn > 0.) kn = knA * P.kn / (knA + P.kn);
+    if (ksA > 0. && P.ks > 0.) ks = ksA * P.ks / (ksA + P.ks);
+    if (invmA > 0. || P.invm > 0.) effM = 1. / (invmA + P.invm);
+    res = fmin(resA, P.res);
+    mu = fmin(muA, P.mu);
+  }
+  const double logRes = log(res);
+  const double diss = -logRes / sqrt_damp(logRes * logRes + M_PI * M_PI, a.flags);
+  PairK k;
+  k.kn = kn; k.ks = ks; k.mu = mu;
+  k.cn = 2. * diss * sqrt_damp(effM * kn, a.flags);
+  k.cs = 2. * diss * sqrt_damp(effM * ks, a.flags);
+  return k;
+}
+
+// integrateSlidingSpring + LinearContact (contactKernel.cuh:4-77) with the pair constants.
+LD void linear_contact(double3& F, double3& spring, double3 vc, double3 n, double delta, double dt, const PairK& k) {
   if (delta > 0.) {
-    const double logRes = log(e);
-    const double diss = -logRes / sqrt_damp(logRes * logRes + M_PI * M_PI, flags);
-    const double cn = 2. * diss * sqrt_damp(effM * kn, flags);
     const double3 vn = dot(vc, n) * n;
-    const double3 fn = kn * delta * n - cn * vn;
-    const double cs = 2. * diss * sqrt_damp(effM * ks, flags);
+    const double3 fn = k.kn * delta * n - k.cn * vn;
     const double3 vs = vc - vn;
     double3 s = d3(0., 0., 0.);
-    if (mu > 0. && ks > 0.) {
+    if (k.mu > 0. && k.ks > 0.) {
       double3 p1 = spring - dot(spring, n) * n;
       const double a1 = len(p1);
       if (!is_zero(a1)) p1 *= len(spring) / a1;
       s = p1 + vs * dt;
-      double3 fs = -ks * s - cs * vs;
+      double3 fs = -k.ks * s - k.cs * vs;
       const double afs = len(fs), afn = len(fn);
-      if (!is_zero(afs) && afs > mu * afn) {
-        const double ratio = mu * afn / afs;
+      if (!is_zero(afs) && afs > k.mu * afn) {
+        const double ratio = k.mu * afn / afs;
         fs *= ratio;
-        s = -(fs + cs * vs) / ks;
+        s = -(fs + k.cs * vs) / k.ks;
       }
     }
     spring = s;
-    const double3 fsl = -ks * spring - cs * vs;
+    const double3 fsl = -k.ks * spring - k.cs * vs;
     F = fn + fsl;
   } else {
     spring = d3(0., 0., 0.);
@@ -394,7 +422,7 @@ LD const SlotView& slots_of(const StepArgs& a, bool old) {
 // added with one atomic per component.
 template <int KIND>
 LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, int* s_cl, unsigned* s_mask,
-                double3& FA, double3& TA) {
+                int* s_old, double3& FA, double3& TA) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's second sweep may still read s_cl / s_mask
   const Partner P = load_partner<KIND>(a, pid);
@@ -406,7 +434,7 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
     bool keep = false;
     if (c < S.ncl) {
       const double4 sp = a.S.cl_sphere[S.cl0 + c];
-      const double3 wc = mat_mul(S.R, d3(sp.x, sp.y, sp.z) * S.sc) + S.x;
+      const double3 wc = rotate(S.q, d3(sp.x, sp.y, sp.z) * S.sc) + S.x;
       keep = cluster_may_hit<KIND>(wc, sp.w * S.sc, P);
     }
     const unsigned m = __ballot_sync(FULL, keep);
@@ -459,6 +487,12 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
       }
     }
   }
+  // the previous segment's node ids in shared memory (binary-searched by every contact)
+  const bool staged = ocnt <= OLDCAP;
+  if (staged)
+    for (int j = lane; j < ocnt; j += 32) s_old[j] = a.C_old.node[ostart + j];
+  __syncwarp();
+  const PairK K = pair_constants<KIND>(a, A, P);
   // sweep 2
   double3 FB = d3(0., 0., 0.), TB = d3(0., 0., 0.);
   int off = 0;
@@ -479,27 +513,14 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
       int lo = 0, hi = ocnt - 1;
       while (lo <= hi) {
         const int mid = (lo + hi) >> 1;
-        const int v = a.C_old.node[ostart + mid];
+        const int v = staged ? s_old[mid] : a.C_old.node[ostart + mid];
         if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
         if (v < ni) lo = mid + 1; else hi = mid - 1;
       }
       // contact force (contactKernel.cu:75-117 / :155-190 / :225-270)
       const double3 vc = S.v + cross(S.w, pc - S.x) - (P.v + cross(P.w, pc - P.x));
-      double kn = 0., ks = 0., effM = 0., mu, res;
-      if (KIND == KIND_WALL) {
-        kn = S.kn; ks = S.ks;
-        if (S.invm > 0.) effM = 1. / S.invm;
-        mu = fmin(S.mu, P.mu);
-        res = fmin(S.res, P.res);
-      } else {
-        if (S.kn > 0. && P.kn > 0.) kn = S.kn * P.kn / (S.kn + P.kn);
-        if (S.ks > 0. && P.ks > 0.) ks = S.ks * P.ks / (S.ks + P.ks);
-        if (S.invm > 0. || P.invm > 0.) effM = 1. / (S.invm + P.invm);
-        res = fmin(S.res, P.res);
-        mu = fmin(S.mu, P.mu);
-      }
       double3 F;
-      linear_contact(F, spring, vc, n, ov, a.dt, kn, ks, mu, res, effM, a.flags);
+      linear_contact(F, spring, vc, n, ov, a.dt, K);
       const int pos = base + off + __popc(m & lanemask_lt());
       if (can_write) {
         a.C.node[pos] = ni;
@@ -508,8 +529,8 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
           a.C.point[pos] = pc;
           a.C.normal[pos] = n;
           a.C.overlap[pos] = ov;
-          a.C.en_n[pos] = 0.5 * ov * ov * kn;
-          a.C.en_s[pos] = 0.5 * len2(spring) * ks;
+          a.C.en_n[pos] = 0.5 * ov * ov * K.kn;
+          a.C.en_s[pos] = 0.5 * len2(spring) * K.ks;
         }
       }
       FA += F;
@@ -530,9 +551,10 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
 }
 
 template <int KINDS>
-__global__ void __launch_bounds__(NP_WARPS * 32) k_narrowphase(StepArgs a) {
+__global__ void __launch_bounds__(NP_WARPS * 32, 2) k_narrowphase(StepArgs a) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  __shared__ int s_old[NP_WARPS][OLDCAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ng_max = 0;
   for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
@@ -544,24 +566,362 @@ __global__ void __launch_bounds__(NP_WARPS * 32) k_narrowphase(StepArgs a) {
     if (npp + nw + ngc == 0) continue;
     SelfCtx S;
     S.x = a.P.pos[A]; S.v = a.P.vel[A]; S.w = a.P.angvel[A]; S.q = a.P.quat[A];
-    S.R = quat_to_mat(S.q);
-    S.sc = a.P.scale[A]; S.invm = a.P.invmass[A]; S.kn = a.P.kn[A]; S.ks = a.P.ks[A];
-    S.mu = a.P.mu[A]; S.res = a.P.res[A];
+    S.sc = a.P.scale[A];
     const int sh = a.P.shape[A];
     S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
     S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
     double3 FA = d3(0., 0., 0.), TA = d3(0., 0., 0.);
     for (int j = 0; j < npp; ++j)
-      do_pair<KIND_PP>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+      do_pair<KIND_PP>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
     for (int j = 0; j < nw; ++j)
-      do_pair<KIND_WALL>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+      do_pair<KIND_WALL>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
     for (int j = 0; j < ngc; ++j)
-      do_pair<KIND_GHOST>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], S, s_cl[warp], s_mask[warp], FA, TA);
+      do_pair<KIND_GHOST>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
     FA = warp_sum3(FA);
     TA = warp_sum3(TA);
     if (lane == 0) {
       atomic_add3(a.P.force, A, FA);
       atomic_add3(a.P.torque, A, TA);
+    }
+  }
+  if ((KINDS & 4) && lane == 0 && ng_max > 0) atomicMax(&a.status->need_ghost, ng_max);
+}
+
+// ---------------------------------------------------------------------------
+// Precision form: FP32 geometry and contact law on 16-bit SDF templates.
+//
+// Positions stay FP64: each pair forms d = xA - xB in FP64 and rounds it to FP32,
+// so node coordinates relative to the partner keep FP32 precision at any
+// distance from the origin. SDF values are stored as phi / h of the template in
+// FP16 or BF16 and scaled by the particle's spacing after interpolation. The
+// tangential spring is carried over and integrated in FP64; forces are summed in
+// FP32 per warp and added to the FP64 particle sums.
+LD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+LD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+LD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+LD float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+LD float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+LD float3 operator*(float s, float3 a) { return f3(a.x * s, a.y * s, a.z * s); }
+LD float3& operator+=(float3& a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+LD float3& operator-=(float3& a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
+LD float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+LD float3 crossf(float3 a, float3 b) { return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+LD float3 tof(double3 v) { return f3((float)v.x, (float)v.y, (float)v.z); }
+LD double3 tod(float3 v) { return d3(v.x, v.y, v.z); }
+LD float4 toq(Quat q) { return make_float4((float)q.q0, (float)q.q1, (float)q.q2, (float)q.q3); }
+// rotation by q = (x: scalar, y, z, w: vector part) and by its conjugate
+LD float3 rotf(float4 q, float3 v) {
+  const float3 qv = f3(q.y, q.z, q.w);
+  const float3 t = crossf(qv, v) * 2.0f;
+  return v + t * q.x + crossf(qv, t);
+}
+LD float3 rotinvf(float3 v, float4 q) {
+  const float3 qv = f3(-q.y, -q.z, -q.w);
+  const float3 t = crossf(qv, v) * 2.0f;
+  return v + t * q.x + crossf(qv, t);
+}
+
+template <int SDFK>
+LD float decode16(unsigned short b) {
+  if (SDFK == PREC_FP32_BF16) return __uint_as_float(((unsigned)b) << 16);
+  return __half2float(__ushort_as_half(b));
+}
+
+struct SelfF {
+  double3 x;   // FP64 centre (cell-window tests of walls and images)
+  float3 v, w;
+  float4 q;
+  float sc;
+  int n0, nn, cl0, ncl;
+};
+
+struct PartnerF {
+  float3 d;     // xA - x(partner)
+  float4 q;
+  float r;
+  float3 o;
+  float invh, h;
+  int3 gs;
+  const unsigned short* sdf;
+  int key, real;
+  float3 v, w;
+};
+
+template <int KIND>
+LD PartnerF partner_f(const StepArgs& a, const Partner& P, const SelfF& S) {
+  PartnerF F;
+  F.d = tof(S.x - P.x);
+  F.q = toq(P.q);
+  F.r = (float)P.r;
+  F.o = tof(P.o);
+  F.invh = (float)P.invh;
+  F.h = (float)(1.0 / P.invh);
+  F.gs = P.gs;
+  F.sdf = a.S.sdf16 + (P.sdf - a.S.sdf);
+  F.key = P.key;
+  F.real = P.real;
+  F.v = tof(P.v);
+  F.w = tof(P.w);
+  return F;
+}
+
+// Trilinear evaluation in FP32; returns the overlap (in length units) through ov.
+template <int SDFK>
+LD bool sdf_eval_f(float3 r, const PartnerF& P, float& ov, float& fx, float& fy, float& fz, float* c) {
+  const float3 l = rotinvf(r, P.q);
+  const float gx = (l.x - P.o.x) * P.invh, gy = (l.y - P.o.y) * P.invh, gz = (l.z - P.o.z) * P.invh;
+  const int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
+  if (i0 < 0 || j0 < 0 || k0 < 0) return false;
+  if (i0 >= P.gs.x - 1 || j0 >= P.gs.y - 1 || k0 >= P.gs.z - 1) return false;
+  fx = gx - (float)i0;
+  fy = gy - (float)j0;
+  fz = gz - (float)k0;
+  const int sy = P.gs.x, sz = P.gs.x * P.gs.y;
+  const unsigned short* b = P.sdf + (k0 * sz + j0 * sy + i0);
+  c[0] = decode16<SDFK>(__ldg(b));
+  c[1] = decode16<SDFK>(__ldg(b + 1));
+  c[2] = decode16<SDFK>(__ldg(b + sy));
+  c[3] = decode16<SDFK>(__ldg(b + sy + 1));
+  c[4] = decode16<SDFK>(__ldg(b + sz));
+  c[5] = decode16<SDFK>(__ldg(b + sz + 1));
+  c[6] = decode16<SDFK>(__ldg(b + sz + sy));
+  c[7] = decode16<SDFK>(__ldg(b + sz + sy + 1));
+  const float wx0 = 1.f - fx, wx1 = fx, wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
+  const float phi = c[0] * wx0 * wy0 * wz0 + c[1] * wx1 * wy0 * wz0 + c[2] * wx0 * wy1 * wz0 +
+                    c[3] * wx1 * wy1 * wz0 + c[4] * wx0 * wy0 * wz1 + c[5] * wx1 * wy0 * wz1 +
+                    c[6] * wx0 * wy1 * wz1 + c[7] * wx1 * wy1 * wz1;
+  ov = -phi * P.h;
+  return ov >= 0.f;
+}
+
+LD float3 sdf_grad_f(float fx, float fy, float fz, const float* c, int flags) {
+  const float x = (flags & FIX_GRADIENT) ? fx : (float)(int)fx;
+  const float wx0 = 1.f - x, wx1 = x, wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
+  return f3((c[1] - c[0]) * wy0 * wz0 + (c[3] - c[2]) * wy1 * wz0 + (c[5] - c[4]) * wy0 * wz1 + (c[7] - c[6]) * wy1 * wz1,
+            (c[2] - c[0]) * wx0 * wz0 + (c[3] - c[1]) * wx1 * wz0 + (c[6] - c[4]) * wx0 * wz1 + (c[7] - c[5]) * wx1 * wz1,
+            (c[4] - c[0]) * wx0 * wy0 + (c[5] - c[1]) * wx1 * wy0 + (c[6] - c[2]) * wx0 * wy1 + (c[7] - c[3]) * wx1 * wy1);
+}
+
+template <int KIND>
+LD bool node_admitted_f(const StepArgs& a, float3 ra, float3 r, const SelfF& S, const PartnerF& P) {
+  if (KIND == KIND_PP) return !(dotf(r, r) > P.r * P.r);
+  const double3 w = S.x + tod(ra);
+  int3 c, lo, hi;
+  node_window(w, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
+  return in_window(P.key, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
+}
+
+template <int KIND>
+LD bool cluster_may_hit_f(float3 wc, float rad, const PartnerF& P) {
+  const float slack = 1e-6f * (fabsf(P.d.x) + fabsf(P.d.y) + fabsf(P.d.z));
+  if (KIND == KIND_PP) {
+    const float R = (P.r + rad) * (1.0f + 1e-5f) + slack;
+    return dotf(wc, wc) <= R * R;
+  }
+  const float3 l = rotinvf(wc, P.q);
+  const float3 hi = f3(P.o.x + (P.gs.x - 1) * P.h, P.o.y + (P.gs.y - 1) * P.h, P.o.z + (P.gs.z - 1) * P.h);
+  const float dx = fmaxf(fmaxf(P.o.x - l.x, l.x - hi.x), 0.f);
+  const float dy = fmaxf(fmaxf(P.o.y - l.y, l.y - hi.y), 0.f);
+  const float dz = fmaxf(fmaxf(P.o.z - l.z, l.z - hi.z), 0.f);
+  const float ext = (hi.x - P.o.x) + (hi.y - P.o.y) + (hi.z - P.o.z);
+  return sqrtf(dx * dx + dy * dy + dz * dz) <= rad * (1.0f + 1e-5f) + 1e-5f * ext + slack;
+}
+
+// Linear contact in FP32 with the tangential spring carried and integrated in FP64.
+LD void linear_contact_f(float3& F, double3& spring, float3 vc, float3 n, float delta, float dt, const PairK& K) {
+  if (delta > 0.f) {
+    const float kn = (float)K.kn, ks = (float)K.ks, mu = (float)K.mu, cn = (float)K.cn, cs = (float)K.cs;
+    const float3 vn = dotf(vc, n) * n;
+    const float3 fn = kn * delta * n - cn * vn;
+    const float3 vs = vc - vn;
+    double3 s = d3(0., 0., 0.);
+    if (mu > 0.f && ks > 0.f) {
+      const double3 nd = tod(n);
+      double3 p1 = spring - dot(spring, nd) * nd;
+      const double a1 = len(p1);
+      if (!is_zero(a1)) p1 *= len(spring) / a1;
+      s = p1 + tod(vs) * (double)dt;
+      float3 fs = -ks * tof(s) - cs * vs;
+      const float afs = sqrtf(dotf(fs, fs)), afn = sqrtf(dotf(fn, fn));
+      if (afs > 1e-30f && afs > mu * afn) {
+        fs = fs * (mu * afn / afs);
+        s = -(tod(fs) + K.cs * tod(vs)) / K.ks;
+      }
+    }
+    spring = s;
+    F = fn + (-ks * tof(spring) - cs * vs);
+  } else {
+    spring = d3(0., 0., 0.);
+    F = f3(0.f, 0.f, 0.f);
+  }
+}
+
+LD float3 warp_sum3f(float3 v) { return f3(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)); }
+
+template <int KIND, int SDFK>
+LD void do_pair_f(const StepArgs& a, int A, int slot, int pid, const SelfF& S, int* s_cl, unsigned* s_mask,
+                  int* s_old, float3& FA, float3& TA) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  const Partner P64 = load_partner<KIND>(a, pid);
+  const PartnerF P = partner_f<KIND>(a, P64, S);
+  const SlotView& cur = slots_of<KIND>(a, false);
+  int nsurv = 0;
+  for (int c0 = 0; c0 < S.ncl; c0 += 32) {
+    const int c = c0 + lane;
+    bool keep = false;
+    if (c < S.ncl) {
+      const double4 sp = a.S.cl_sphere[S.cl0 + c];
+      const float3 wc = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc) + P.d;
+      keep = cluster_may_hit_f<KIND>(wc, (float)sp.w * S.sc, P);
+    }
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
+    nsurv += __popc(m);
+  }
+  __syncwarp();
+  int total = 0;
+  for (int k = 0; k < nsurv; ++k) {
+    const int ni = s_cl[k] * 32 + lane;
+    bool hit = false;
+    if (ni < S.nn) {
+      const float4 nd = a.S.node_pos_f[S.n0 + ni];
+      const float3 ra = rotf(S.q, f3(nd.x, nd.y, nd.z) * S.sc);
+      const float3 r = ra + P.d;
+      if (node_admitted_f<KIND>(a, ra, r, S, P)) {
+        float ov, fx, fy, fz, cr[8];
+        hit = sdf_eval_f<SDFK>(r, P, ov, fx, fy, fz, cr);
+      }
+    }
+    const unsigned m = __ballot_sync(FULL, hit);
+    if (lane == 0) s_mask[k] = m;
+    total += __popc(m);
+  }
+  __syncwarp();
+  const size_t sidx = (size_t)A * cur.cap + slot;
+  int base = 0;
+  if (lane == 0 && total > 0) base = atomicAdd(a.C.count, total);
+  base = __shfl_sync(FULL, base, 0);
+  const bool can_write = (base + total <= a.C.cap);
+  if (lane == 0) {
+    cur.seg_start[sidx] = base;
+    cur.seg_cnt[sidx] = can_write ? total : 0;
+    if (!can_write) atomicOr(&a.status->flags, OVF_CONTACT);
+  }
+  if (total == 0) return;
+  const SlotView& old = slots_of<KIND>(a, true);
+  int ostart = 0, ocnt = 0;
+  if (old.cnt != nullptr) {
+    const int on = old.cnt[A] < old.cap ? old.cnt[A] : old.cap;
+    for (int j0 = 0; j0 < on; j0 += 32) {
+      const int j = j0 + lane;
+      const bool match = j < on && old.id[(size_t)A * old.cap + j] == pid;
+      const unsigned m = __ballot_sync(FULL, match);
+      if (m) {
+        const int src = j0 + __ffs(m) - 1;
+        ostart = old.seg_start[(size_t)A * old.cap + src];
+        ocnt = old.seg_cnt[(size_t)A * old.cap + src];
+        break;
+      }
+    }
+  }
+  const bool staged = ocnt <= OLDCAP;
+  if (staged)
+    for (int j = lane; j < ocnt; j += 32) s_old[j] = a.C_old.node[ostart + j];
+  __syncwarp();
+  const PairK K = pair_constants<KIND>(a, A, P64);
+  float3 FB = f3(0.f, 0.f, 0.f), TB = f3(0.f, 0.f, 0.f);
+  int off = 0;
+  for (int k = 0; k < nsurv; ++k) {
+    const unsigned m = s_mask[k];
+    if (m == 0) continue;
+    if ((m >> lane) & 1u) {
+      const int ni = s_cl[k] * 32 + lane;
+      const float4 nd = a.S.node_pos_f[S.n0 + ni];
+      const float3 ra = rotf(S.q, f3(nd.x, nd.y, nd.z) * S.sc);
+      const float3 r = ra + P.d;
+      float ov, fx, fy, fz, cr[8];
+      sdf_eval_f<SDFK>(r, P, ov, fx, fy, fz, cr);
+      float3 n = rotf(P.q, sdf_grad_f(fx, fy, fz, cr, a.flags));
+      const float l2 = dotf(n, n);
+      n = l2 > 1e-30f ? n * rsqrtf(l2) : f3(0.f, 0.f, 0.f);
+      const float3 pcA = ra + 0.5f * ov * n;
+      const float3 pcB = r + 0.5f * ov * n;
+      double3 spring = d3(0., 0., 0.);
+      int lo = 0, hi = ocnt - 1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int v = staged ? s_old[mid] : a.C_old.node[ostart + mid];
+        if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
+        if (v < ni) lo = mid + 1; else hi = mid - 1;
+      }
+      const float3 vc = S.v + crossf(S.w, pcA) - (P.v + crossf(P.w, pcB));
+      float3 F;
+      linear_contact_f(F, spring, vc, n, ov, (float)a.dt, K);
+      const int pos = base + off + __popc(m & lanemask_lt());
+      if (can_write) {
+        a.C.node[pos] = ni;
+        a.C.spring[pos] = spring;
+        if (a.C.point) {
+          a.C.point[pos] = S.x + tod(pcA);
+          a.C.normal[pos] = tod(n);
+          a.C.overlap[pos] = ov;
+          a.C.en_n[pos] = 0.5 * (double)ov * (double)ov * K.kn;
+          a.C.en_s[pos] = 0.5 * len2(spring) * K.ks;
+        }
+      }
+      FA += F;
+      TA += crossf(pcA, F);
+      FB -= F;
+      TB += crossf(pcB, -F);
+    }
+    off += __popc(m);
+  }
+  if (KIND != KIND_WALL && !(KIND == KIND_GHOST && P.real == A)) {
+    FB = warp_sum3f(FB);
+    TB = warp_sum3f(TB);
+    if (lane == 0) {
+      atomic_add3(a.P.force, P.real, tod(FB));
+      atomic_add3(a.P.torque, P.real, tod(TB));
+    }
+  }
+}
+
+template <int KINDS, int SDFK>
+__global__ void __launch_bounds__(NP_WARPS * 32, 3) k_narrowphase_f(StepArgs a) {
+  __shared__ int s_cl[NP_WARPS][MAXCL];
+  __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  __shared__ int s_old[NP_WARPS][OLDCAP];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int ng_max = 0;
+  for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
+    const int npp = (KINDS & 1) ? a.pp.cnt[A] : 0;
+    const int nw = (KINDS & 2) ? (a.pw.cap > 0 ? a.pw.cnt[A] : 0) : 0;
+    const int ng = (KINDS & 4) ? a.pgh.cnt[A] : 0;
+    ng_max = ng > ng_max ? ng : ng_max;
+    const int ngc = ng < a.pgh.cap ? ng : a.pgh.cap;
+    if (npp + nw + ngc == 0) continue;
+    SelfF S;
+    S.x = a.P.pos[A];
+    S.v = tof(a.P.vel[A]);
+    S.w = tof(a.P.angvel[A]);
+    S.q = toq(a.P.quat[A]);
+    S.sc = (float)a.P.scale[A];
+    const int sh = a.P.shape[A];
+    S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
+    S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
+    float3 FA = f3(0.f, 0.f, 0.f), TA = f3(0.f, 0.f, 0.f);
+    for (int j = 0; j < npp; ++j)
+      do_pair_f<KIND_PP, SDFK>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
+    for (int j = 0; j < nw; ++j)
+      do_pair_f<KIND_WALL, SDFK>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
+    for (int j = 0; j < ngc; ++j)
+      do_pair_f<KIND_GHOST, SDFK>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
+    FA = warp_sum3f(FA);
+    TA = warp_sum3f(TA);
+    if (lane == 0) {
+      atomic_add3(a.P.force, A, tod(FA));
+      atomic_add3(a.P.torque, A, tod(TA));
     }
   }
   if ((KINDS & 4) && lane == 0 && ng_max > 0) atomicMax(&a.status->need_ghost, ng_max);
@@ -583,10 +943,23 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   int want = (a.P.n + NP_WARPS - 1) / NP_WARPS;
   int cap = num_sms() * 16;
   int blocks = want < cap ? want : cap;
-  if (kinds == 3) k_narrowphase<3><<<blocks, NP_WARPS * 32, 0, s>>>(a);
-  else if (kinds == 1) k_narrowphase<1><<<blocks, NP_WARPS * 32, 0, s>>>(a);
-  else if (kinds == 4) k_narrowphase<4><<<blocks, NP_WARPS * 32, 0, s>>>(a);
-  else k_narrowphase<7><<<blocks, NP_WARPS * 32, 0, s>>>(a);
+  const dim3 g(blocks), b(NP_WARPS * 32);
+  if (a.precision == PREC_FP32_FP16) {
+    if (kinds == 3) k_narrowphase_f<3, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
+    else if (kinds == 1) k_narrowphase_f<1, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
+    else if (kinds == 4) k_narrowphase_f<4, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
+    else k_narrowphase_f<7, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
+  } else if (a.precision == PREC_FP32_BF16) {
+    if (kinds == 3) k_narrowphase_f<3, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
+    else if (kinds == 1) k_narrowphase_f<1, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
+    else if (kinds == 4) k_narrowphase_f<4, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
+    else k_narrowphase_f<7, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
+  } else {
+    if (kinds == 3) k_narrowphase<3><<<g, b, 0, s>>>(a);
+    else if (kinds == 1) k_narrowphase<1><<<g, b, 0, s>>>(a);
+    else if (kinds == 4) k_narrowphase<4><<<g, b, 0, s>>>(a);
+    else k_narrowphase<7><<<g, b, 0, s>>>(a);
+  }
 }
 
 // ---------------------------------------------------------------------------

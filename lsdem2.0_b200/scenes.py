@@ -356,6 +356,59 @@ def polydisperse_periodic(lsdem, n=100_000, box=0.1, median=2e-3, sigma=0.25, n_
             "dt": dt, "min": np.zeros(3), "max": np.full(3, box), "gravity": np.zeros(3), "periodic": 7}
 
 
+def resolve_deep_overlaps(lsdem, sc, threshold=0.02, exclusion=0.8, max_iter=40, device=0, seed=None):
+    """Re-places particles whose body overlaps a neighbour by more than `threshold` x the
+    smaller bounding radius, until none does (shallow contacts stay).
+
+    The reference's contact law applies the normal stiffness once per surface node inside the
+    partner, so a deep initial overlap (many nodes inside) multiplies the contact stiffness and
+    can exceed the stability limit of the explicit step. Overlaps are measured by the solver's
+    own detection (one step of 1e-12 s from rest); the re-placed particles get new random
+    positions (sequential addition around the others, spheres of `exclusion` x the bounding
+    radius) and orientations. Updates sc["pos"] and sc["quat"] in place; returns the number of
+    iterations."""
+    rng = np.random.default_rng(seed_for(7) if seed is None else seed)
+    n = len(sc["pos"])
+    rest = dict(sc, vel=np.zeros((n, 3)))
+    sv = lsdem.Solver(device=device)
+    load_polydisperse(sv, rest)
+    sv.set_record_contacts(True)
+    sv.initialize(sc["min"], sc["max"], sc["gravity"])
+    pp = sv.particle_params()
+    radius = pp["radius"]
+    nb = np.concatenate([pp["node_base"], [np.iinfo(np.int64).max]])
+    zero = np.zeros((n, 3))
+    it = 0
+    for it in range(1, max_iter + 1):
+        sv.set_state(pos=sc["pos"], vel=zero, angvel=zero, quat=sc["quat"])
+        sv.step(1e-12, 1)
+        bad = set()
+        for kind in (lsdem.CONTACT_PARTICLE, lsdem.CONTACT_GHOST):
+            c = sv.contacts(kind, geometry=True)
+            if len(c["node"]) == 0:
+                continue
+            owner = np.searchsorted(nb, c["node"], side="right") - 1
+            partner = c["partner"]
+            rmin = np.minimum(radius[owner], radius[partner])
+            deep = c["overlap"] > threshold * rmin
+            if kind == lsdem.CONTACT_GHOST:
+                deep &= owner != partner
+            bad.update(np.maximum(owner[deep], partner[deep]).tolist())
+        if not bad:
+            break
+        bad = np.fromiter(bad, np.int64)
+        keep = np.ones(n, np.int32)
+        keep[bad] = 0
+        # re-placed spheres may come a little closer than the first packing (0.75 x radius)
+        rad = 0.5 * exclusion * sc["scale"]
+        rad = np.where(keep == 0, rad * (0.75 / exclusion), rad)
+        sc["pos"] = lsdem.pack_rsa(rad, sc["min"], sc["max"], periodic=bool(sc["periodic"]),
+                                   seed=int(rng.integers(1 << 62)), max_tries=20000, keep=keep, pos=sc["pos"])
+        sc["quat"][bad] = random_quaternions(rng, len(bad))
+    sv.close()
+    return it
+
+
 def load_polydisperse(solver, sc):
     ids = [solver.add_shape(t["nodes"], t["sdf"], t["size"], t["origin"], t["spacing"]) for t in sc["templates"]]
     shape = np.asarray(ids, np.int32)[sc["shape"]]
