@@ -1,13 +1,20 @@
 """Benchmark of the level-set DEM time step (particle-steps/s).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload polydisperse|small]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload polydisperse|small] [--form fp32-bf16|fp32-fp16|fp64]
 
-Workload (default "polydisperse", the precision-form configuration that fits one
+Workload (default "polydisperse", the precision-form configuration, which fits one
 GPU): 100,000 particles from 4 templates (ellipsoid 1:0.8:0.6, superquadric
 exponent 4, rounded cube, capsule of aspect 2) with log-normal bounding
 diameters (median 2 mm, sigma 0.25), 48^3 SDF grids, 2,000 surface nodes each,
 0.1 m triply periodic cube, velocities N(0, 0.1 m/s), linear contact (kn 1e5,
 kt 0.8 kn, mu 0.5, e 0.6), dt 5e-7 s. Synthetic, seeded (no dataset).
+
+The headline form is the configuration's own: FP32 narrowphase and contact law
+on BF16 SDF templates, FP64 positions, integration and spring history. The same
+run times the FP16-template form and the plain FP64 form (the reference's
+arithmetic, bit-exact pair lists) and states each FP32 form's force error
+against the FP64 path from the same state.
 
 One step = one full time step (half kick, drift, cell sort, candidates,
 narrowphase + contact forces, periodic images, half kick) of the whole scene.
@@ -30,6 +37,9 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 
+FORMS = {"fp32-bf16": 2, "fp32-fp16": 1, "fp64": 0}
+DTYPE = {"fp32-bf16": "f32 (bf16 SDF, f64 state)", "fp32-fp16": "f32 (fp16 SDF, f64 state)", "fp64": "f64"}
+
 
 def _package():
     pkg = ROOT / "lsdem2.0_b200"
@@ -50,12 +60,14 @@ def _peaks():
 
 
 # Algorithmic bytes of the fused narrowphase + contact-force kernel (k_narrowphase):
-# per owner particle, per candidate pair and per contact ("roofline").
+# per owner particle (pose, velocities, slot counts, force/torque write: 208 B), per
+# candidate pair (partner id, pose, velocities, shape and material scalars, segment
+# bookkeeping, reaction atomics: 236 B) and per contact (node id, FP64 spring read and
+# write, history lookup: 56 B).
 B_PARTICLE = 208
 B_PAIR = 236
 B_CONTACT = 56
-# whole-step algorithmic bytes per particle for the other phases (state read+write,
-# keys, sort, candidates): see DESIGN.md
+# whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
 
 
@@ -83,7 +95,14 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
+
+    def mark(self, start: bool):
+        """Brackets the timed region (host clock, after a device synchronize)."""
+        if start:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
     def __exit__(self, *a):
         if self.proc:
@@ -94,27 +113,27 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        rows = [r for t, r in self.rows if t0 <= t <= t1]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 3 + k and r[3 + k] == "Active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 3 + k and r[3 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
-def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000):
+def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000, device: int = 0):
     from lsdem_b200 import scenes
     if workload == "small":
         sc = scenes.ellipsoid_falling(seed=scenes.seed_for(0) + rank)
         return sc, {"workload": "ellipsoids-2000-floor", "particles": 2000, "nodes_per_particle": 1000,
-                    "sdf_grid": "32^3 fp64", "box_m": [0.2, 0.2, 0.4], "dt_s": 1e-6}
+                    "sdf_grid": "32^3", "box_m": [0.2, 0.2, 0.4], "dt_s": 1e-6}
     cache = ROOT / "_build" / "templates_48_2000.npz"
-    T = None
     if cache.exists():
-        z = np.load(cache, allow_pickle=True)
-        T = list(z["T"])
+        T = list(np.load(cache, allow_pickle=True)["T"])
     else:
         T = scenes.unit_templates(48, 2000)
         cache.parent.mkdir(exist_ok=True)
@@ -123,28 +142,53 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000):
     sc = scenes.polydisperse_periodic(lsdem, n=particles, box=box, seed=scenes.seed_for(1) + rank, templates=T)
     # deep initial overlaps (many surface nodes inside a neighbour) would exceed the stability
     # limit of the explicit step; re-place those particles, keep shallow contacts
-    iters = scenes.resolve_deep_overlaps(lsdem, sc, device=int(os.environ.get("LOCAL_RANK", "0")))
-    sc["resolve_iterations"] = iters
-    name = "polydisperse-100k-4templates-periodic" if particles == 100_000 else f"polydisperse-{particles}-4templates-periodic"
-    return sc, {"workload": name, "particles": particles, "nodes_per_particle": 2000,
-                "sdf_grid": "48^3 fp64", "templates": 4, "size": "lognormal(median 2 mm, sigma 0.25)",
-                "box_m": round(box, 6), "periodic": "xyz", "dt_s": 5e-7}
+    iters = scenes.resolve_deep_overlaps(lsdem, sc, device=device)
+    name = ("polydisperse-100k-4templates-periodic" if particles == 100_000
+            else f"polydisperse-{particles}-4templates-periodic")
+    return sc, {"workload": name, "particles": particles, "nodes_per_particle": 2000, "sdf_grid": "48^3",
+                "templates": 4, "size": "lognormal(median 2 mm, sigma 0.25)", "box_m": round(box, 6),
+                "periodic": "xyz", "dt_s": 5e-7,
+                "initial_state": f"random sequential addition, deep overlaps re-placed ({iters} passes)"}
 
 
-def load(lsdem, sc, workload, device):
+def load(lsdem, sc, workload, device, prec):
     from lsdem_b200 import scenes
     sv = lsdem.Solver(device=device)
     if workload == "small":
         scenes.load_into(sv, sc)
     else:
         scenes.load_polydisperse(sv, sc)
+    sv.set_precision(prec)
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
     return sv
 
 
+def force_error(lsdem, sc, workload, device, prec, warm=20):
+    """Force / torque error of an FP32 form against the FP64 path, from the same state: both
+    run `warm` FP64 steps, then one step each; forces are captured in the external hook."""
+    import torch
+    out = {}
+    sv = load(lsdem, sc, workload, device, 0)
+    sv.step(sc["dt"], warm)
+    st = sv.state()
+    sv.close()
+    for p in (0, prec):
+        sv = load(lsdem, sc, workload, device, p)
+        sv.set_state(pos=st["pos"], vel=st["vel"], angvel=st["angvel"], quat=st["quat"])
+        box = {}
+        sv.step(sc["dt"], 1, hook=lambda t, sv=sv: box.update(sv.state()))
+        torch.cuda.synchronize()
+        out[p] = box
+        sv.close()
+    F64, T64 = out[0]["force"], out[0]["torque"]
+    return {"force_l2": float(np.linalg.norm(out[prec]["force"] - F64) / np.linalg.norm(F64)),
+            "torque_l2": float(np.linalg.norm(out[prec]["torque"] - T64) / np.linalg.norm(T64)),
+            "force_max": float(np.abs(out[prec]["force"] - F64).max() / np.abs(F64).max())}
+
+
 def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
     """FP64 oracle step (the reference algorithm restated on the CPU, all host threads) on a
-    bounded sample: the particles inside a sub-box of the same scene holding ~target_particles."""
+    bounded sample: the particles inside a corner sub-box of the same scene."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as ora  # the checker, timed here as the CPU baseline
 
@@ -153,8 +197,7 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
     lo, hi = np.asarray(sc["min"]), np.asarray(sc["max"])
     frac = min(1.0, (target_particles / n) ** (1.0 / 3.0))
     sub_hi = lo + (hi - lo) * frac
-    sel = np.all((pos >= lo) & (pos < sub_hi), axis=1)
-    idx = np.nonzero(sel)[0]
+    idx = np.nonzero(np.all((pos >= lo) & (pos < sub_hi), axis=1))[0]
     sv = lsdem.Solver()
     from lsdem_b200 import scenes
     if workload == "small":
@@ -194,6 +237,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     lsdem = _package()
+    import torch  # noqa: F401  (device 0 hosts the scene preparation)
     sc, cfg = build_scene(lsdem, args.workload, 0, args.particles)
     cb = cpu_baseline(lsdem, sc, args.workload, steps=max(1, min(args.steps, 3)))
     line = {"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
@@ -205,15 +249,53 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
+    """W warm-up steps, then exactly K timed steps (CUDA events on the solver's stream =
+    torch's current stream, the legacy default stream); max over ranks."""
+    sv = load(lsdem, sc, args.workload, local, prec)
+    dt = float(sc["dt"])
+    if clocks is not None:
+        clocks.__enter__()  # the sampler starts up during the warm-up
+    sv.step(dt, max(3, args.warmup))
+    launches0 = sv.num(8)
+    reruns0 = sv.num(7)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if clocks is not None:
+        clocks.mark(True)
+    ev0.record()
+    sv.step(dt, args.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.mark(False)
+        clocks.__exit__()
+    ms = ev0.elapsed_time(ev1)
+    res = {"ms": ms, "launches": sv.num(8) - launches0, "reruns": sv.num(7) - reruns0, "stats": sv.step_stats()}
+    # per-phase device times (CUDA events between phases) from a separate, shorter run
+    res["profile_steps"] = min(args.steps, 20)
+    sv.set_profiling(True)
+    sv.step(dt, res["profile_steps"])
+    res["profile"] = sv.profile()
+    sv.set_profiling(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        res["ms"] = float(t.item())
+    return sv, res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="polydisperse", choices=["polydisperse", "small"])
+    ap.add_argument("--form", default="fp32-bf16", choices=list(FORMS))
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true", help="skip the other forms and the error check")
     ap.add_argument("--particles", type=int, default=100_000, help="polydisperse workload size (profiling cases)")
     args = ap.parse_args()
 
@@ -222,8 +304,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         if world > 1:
+            import datetime
             import torch.distributed as dist
-            dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
         run_reference(args, rank, world)
         if world > 1:
             dist.destroy_process_group()
@@ -238,13 +321,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     lsdem = _package()
-    sc, cfg = build_scene(lsdem, args.workload, rank, args.particles)
-    sv = load(lsdem, sc, args.workload, local)
-    n = sv.n_particles
-    dt = float(sc["dt"])
-    sv.step(dt, max(3, args.warmup))
-    sv.set_profiling(True)
-    launches0 = sv.num(8)
+    sc, cfg = build_scene(lsdem, args.workload, rank, args.particles, local)
 
     def barrier():
         torch.cuda.synchronize()
@@ -252,24 +329,11 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record()
-        sv.step(dt, args.steps)
-        ev1.record()
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = sv.num(8) - launches0
-    prof = sv.profile()
-    stats = sv.step_stats()
-    sv.set_profiling(False)
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = n * world * args.steps / (ms_max * 1e-3)
+    prec = FORMS[args.form]
+    clk = Clocks(local)
+    sv, head = time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clk)
+    n = sv.n_particles
+    value = n * world * args.steps / (head["ms"] * 1e-3)
 
     # end-to-end through the C ABI: per step, pinned host state -> device, one step,
     # state + forces back to pinned host memory
@@ -279,17 +343,15 @@ def main():
     st = sv.state()
     for k in h:
         h[k][:] = st[k]
-    import ctypes as C
     dp = lambda a: a.ctypes.data_as(lsdem.DP)
+    dt = float(sc["dt"])
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        rc = lsdem.lib.lsdem_set_state(sv.h, dp(h["pos"]), dp(h["vel"]), dp(h["angvel"]), dp(h["quat"]))
-        assert rc == 0
+        assert lsdem.lib.lsdem_set_state(sv.h, dp(h["pos"]), dp(h["vel"]), dp(h["angvel"]), dp(h["quat"])) == 0
         sv.step(dt, 1)
-        rc = lsdem.lib.lsdem_get_state(sv.h, dp(h["pos"]), dp(h["vel"]), dp(h["angvel"]), dp(h["quat"]),
-                                       dp(h["force"]), dp(h["torque"]))
-        assert rc == 0
+        assert lsdem.lib.lsdem_get_state(sv.h, dp(h["pos"]), dp(h["vel"]), dp(h["angvel"]), dp(h["quat"]),
+                                         dp(h["force"]), dp(h["torque"])) == 0
     barrier()
     e2e_s = time.perf_counter() - t0
     if dist is not None:
@@ -297,42 +359,60 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = n * world * args.e2e_steps / e2e_s
+    sv.close()
+
+    forms = {}
+    if not args.headline_only:
+        for name, p in FORMS.items():
+            if name == args.form:
+                continue
+            svf, r = time_form(lsdem, torch, sc, args, local, p, dist, barrier, None)
+            svf.close()
+            forms[name] = {"value": n * world * args.steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / args.steps}
+        for name, p in FORMS.items():
+            if p != 0:
+                err = force_error(lsdem, sc, args.workload, local, p)
+                forms.setdefault(name, {})["error_vs_fp64"] = err
 
     if rank == 0:
         peak, peak_kind = _peaks()
+        prof, stats = head["profile"], head["stats"]
         np_ms, np_calls = prof["narrowphase"]
         g_ms, g_calls = prof["ghost_narrowphase"]
         pairs = stats["pairs_particle"] + stats["pairs_wall"] + stats["pairs_ghost"]
-        launches_np = np_calls + g_calls
-        avg_ms = (np_ms + g_ms) / max(1, launches_np)
-        # one step runs the particle/wall launch and the ghost launch: per-launch bytes = per-step / 2
-        bytes_step_np = B_PARTICLE * n * 2 + B_PAIR * pairs + B_CONTACT * stats["contacts"]
-        bytes_launch = bytes_step_np / 2.0
+        avg_ms = (np_ms + g_ms) / max(1, np_calls + g_calls)
+        # a step runs the particle/wall launch and the image launch: per-launch bytes = per-step / 2
+        launches_per_step = 2 if g_calls else 1
+        bytes_launch = (B_PARTICLE * n * launches_per_step + B_PAIR * pairs + B_CONTACT * stats["contacts"]) / \
+            launches_per_step
         achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
         b_step = B_STEP_PARTICLE * n + B_CONTACT * stats["contacts"] + 16 * pairs
+        ms_step = head["ms"] / args.steps
+        forms[args.form] = dict(forms.get(args.form, {}), value=value, ms_per_step=ms_step)
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.form],
             "data": "synthetic (seeded)",
-            "config": dict(cfg, form="plain grid (FP64)", parallelism=f"replicas x{world}",
-                           l2=f"not flushed: per-step algorithmic traffic {b_step / 1e6:.0f} MB vs 126 MB L2",
+            "config": dict(cfg, form=args.form, parallelism=f"replicas x{world}",
+                           l2=f"not flushed: per-step algorithmic traffic {b_step / 1e6:.0f} MB "
+                              f"({'>' if b_step > 126e6 else '<'} 126 MB L2)",
                            contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs),
+            "forms": forms,
             "roofline": {"bound": "hbm", "kernel": "k_narrowphase", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
-            "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_max / args.steps * 1e-3) / 1e9},
-            "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof.items()},
+            "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_step * 1e-3) / 1e9},
+            "phases_ms_per_step": {k: v[0] / head["profile_steps"] for k, v in prof.items()},
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": n * (3 * 24 + 32),
                     "d2h_bytes_per_step": n * (5 * 24 + 32)},
-            "gpu_launches": launches,
-            "overflow_reruns": sv.num(7),
+            "gpu_launches": head["launches"],
+            "overflow_reruns": head["reruns"],
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(lsdem, sc, args.workload)
         print(json.dumps(line), flush=True)
-    sv.close()
     if dist is not None:
         dist.destroy_process_group()
 

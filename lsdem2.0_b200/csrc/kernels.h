@@ -138,6 +138,7 @@ struct StepArgs {
   double3 gravity;
   int flags;        // FIX_* bits
   int precision;    // PREC_*
+  double rmax;      // largest particle bounding radius
 };
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);

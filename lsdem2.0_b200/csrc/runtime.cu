@@ -290,6 +290,7 @@ struct lsdem_solver {
   cudaStream_t stream = nullptr;
   int flags = 0;
   int precision = PREC_FP64;
+  double rmax_p = 0.;        // largest particle bounding radius (set at initialize)
   std::string err;
   // model
   std::vector<ShapeHost> shapes;
@@ -632,6 +633,7 @@ void initialize(lsdem_solver* s) {
   // grids: cell = 2 x max bounding radius (LSParticle.h:241-256)
   double rp = 0., rw = 0.;
   for (double r : s->P.radius) rp = std::max(rp, r);
+  s->rmax_p = rp;
   for (double r : s->W.radius) rw = std::max(rw, r);
   set_grid(s->pg, s->dmin, s->dmax, s->P.n() ? 2.0 * rp : 0.0);
   set_grid(s->wg, s->dmin, s->dmax, s->W.n() ? 2.0 * rw : 0.0);
@@ -733,6 +735,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.gravity = make_double3(s->grav[0], s->grav[1], s->grav[2]);
   a.flags = s->flags;
   a.precision = s->precision;
+  a.rmax = s->rmax_p;
   return a;
 }
 

@@ -128,78 +128,76 @@ LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi
   hi = d3(o.x + (gs.x - 1) / invh, o.y + (gs.y - 1) / invh, o.z + (gs.z - 1) / invh);
 }
 
-// Candidate partners of each particle A (one thread per particle).
+// Candidate partners of each particle A.
 // Particle partners: B > A, visible (in a cell), bounding spheres within
 // reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
 // node's 27-cell window since cells are at least 2 max radius wide).
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
-LD void candidates_of(const StepArgs& a, int A, int& n_out, int& nw_out) {
-  const double3 xA = a.P.pos[A];
-  const double rA = a.P.radius[A];
-  const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
-  int n = 0;
-  const int cap = a.pp.cap;
-  int* out = a.pp.id + (size_t)A * cap;
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int z = c.z + dz;
-    if (z < 0 || z >= a.pg.size.z) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int y = c.y + dy;
-      if (y < 0 || y >= a.pg.size.y) continue;
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int x = c.x + dx;
-        if (x < 0 || x >= a.pg.size.x) continue;
-        const int h = lin3(make_int3(x, y, z), a.pg.size);
-        const int st = a.cell_start[h];
-        if (st < 0) continue;
-        const int en = a.cell_end[h];
-        for (int k = st; k < en; ++k) {
-          const int B = a.cell_idx[k];
-          if (B <= A) continue;
-          const double3 xB = a.P.pos[B];
-          const double R = (rA + a.P.radius[B]) * (1.0 + 1e-9) + coord_slack(xA, xB);
-          if (len2(xA - xB) > R * R) continue;
-          if (n < cap) out[n] = B;
-          ++n;
+// One thread per particle, threads in cell-sorted order: the lanes of a warp
+// mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
+// and their occupant loads are broadcasts. Slots are filled in cell-walk then
+// sorted-occupant order.
+__global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = 0, nw = 0;
+  if (t < a.P.n) {
+    const int A = a.cell_idx[t];
+    const double3 xA = a.P.pos[A];
+    const double rA = a.P.radius[A];
+    const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
+    const int cap = a.pp.cap;
+    int* out = a.pp.id + (size_t)A * cap;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= a.pg.size.z) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= a.pg.size.y) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int x = c.x + dx;
+          if (x < 0 || x >= a.pg.size.x) continue;
+          const int h = lin3(make_int3(x, y, z), a.pg.size);
+          const int st = a.cell_start[h];
+          if (st < 0) continue;
+          const int en = a.cell_end[h];
+          for (int k = st; k < en; ++k) {
+            const int B = a.cell_idx[k];
+            if (B <= A) continue;
+            const double3 xB = a.P.pos[B];
+            const double R = (rA + a.P.radius[B]) * (1.0 + 1e-9) + coord_slack(xA, xB);
+            if (len2(xA - xB) > R * R) continue;
+            if (n < cap) out[n] = B;
+            ++n;
+          }
         }
       }
     }
+    a.pp.cnt[A] = n < cap ? n : cap;
+    if (n > cap) atomicOr(&a.status->flags, OVF_PP);
+    // walls (few), in wall order
+    const int capw = a.pw.cap;
+    for (int w = 0; w < a.W.n; ++w) {
+      if (a.W.key[w] < 0) continue;
+      const double3 l = rotate_inv(xA - a.W.pos[w], a.W.quat[w]);
+      double3 lo, hi;
+      grid_box(a.W.origin[w], a.W.invh[w], a.S.gsize[a.W.shape[w]], lo, hi);
+      const double reach = rA * (1.0 + 1e-9) + coord_slack(xA, a.W.pos[w]) + 1e-12 * len(hi - lo);
+      if (box_dist(l, lo, hi) > reach) continue;
+      if (nw < capw) a.pw.id[(size_t)A * capw + nw] = w;
+      ++nw;
+    }
+    if (capw > 0) a.pw.cnt[A] = nw < capw ? nw : capw;
+    if (nw > capw) atomicOr(&a.status->flags, OVF_WALL);
   }
-  a.pp.cnt[A] = n < cap ? n : cap;
-  if (n > cap) atomicOr(&a.status->flags, OVF_PP);
-  n_out = n;
-  // walls
-  int nw = 0;
-  const int capw = a.pw.cap;
-  for (int w = 0; w < a.W.n; ++w) {
-    if (a.W.key[w] < 0) continue;
-    const double3 l = rotate_inv(xA - a.W.pos[w], a.W.quat[w]);
-    double3 lo, hi;
-    grid_box(a.W.origin[w], a.W.invh[w], a.S.gsize[a.W.shape[w]], lo, hi);
-    const double reach = rA * (1.0 + 1e-9) + coord_slack(xA, a.W.pos[w]) + 1e-12 * len(hi - lo);
-    if (box_dist(l, lo, hi) > reach) continue;
-    if (nw < capw) a.pw.id[(size_t)A * capw + nw] = w;
-    ++nw;
-  }
-  if (capw > 0) a.pw.cnt[A] = nw < capw ? nw : capw;
-  if (nw > capw) atomicOr(&a.status->flags, OVF_WALL);
-  nw_out = nw;
-}
-
-__global__ void k_candidates(StepArgs a) {
-  const int A = blockIdx.x * blockDim.x + threadIdx.x;
-  int npp = 0, nwall = 0;
-  if (A < a.P.n) candidates_of(a, A, npp, nwall);
   // largest demand of the warp, one atomic per warp
-  npp = __reduce_max_sync(FULL, npp);
-  nwall = __reduce_max_sync(FULL, nwall);
+  n = __reduce_max_sync(FULL, n);
+  nw = __reduce_max_sync(FULL, nw);
   if ((threadIdx.x & 31) == 0) {
-    if (npp > 0) atomicMax(&a.status->need_pp, npp);
-    if (nwall > 0) atomicMax(&a.status->need_wall, nwall);
+    if (n > 0) atomicMax(&a.status->need_pp, n);
+    if (nw > 0) atomicMax(&a.status->need_wall, nw);
   }
 }
-
 
 void launch_candidates(const StepArgs& a, cudaStream_t s) {
   if (a.P.n > 0) k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
@@ -1042,6 +1040,19 @@ __global__ void k_ghost_compact(StepArgs a) {
   if (vis) a.G.list[base + __popc(m & lanemask_lt())] = (int)t;
 }
 
+// Cell range along one axis of a ball (centre p, radius r) on the clamped grid,
+// intersected with [c - 2, c + 2].
+LD int axis_lo(double p, double mn, double inv, int size, double r, int c) {
+  int v = (int)floor((p - mn - r) * inv);
+  v = v < 0 ? 0 : (v > size - 1 ? size - 1 : v);
+  return v > c - 2 ? v : c - 2;
+}
+LD int axis_hi(double p, double mn, double inv, int size, double r, int c) {
+  int v = (int)floor((p - mn + r) * inv);
+  v = v < 0 ? 0 : (v > size - 1 ? size - 1 : v);
+  return v < c + 2 ? v : c + 2;
+}
+
 // Ghost partners, searched with one warp per visible image G: a node of A can
 // only reach G's cell window when A's clamped cell is within 2 cells of G's
 // cell, and only when A's bounding sphere reaches G's SDF grid box. The lanes
@@ -1064,12 +1075,17 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
     const double3 far = d3(fmax(fabs(lo.x), fabs(hi.x)), fmax(fabs(lo.y), fabs(hi.y)), fmax(fabs(lo.z), fabs(hi.z)));
     const double Rg = len(far);
     const int pid = (i << 3) | s;
-    for (int z = cz - 2; z <= cz + 2; ++z) {
-      if (z < 0 || z >= g.size.z) continue;
-      for (int y = cy - 2; y <= cy + 2; ++y) {
-        if (y < 0 || y >= g.size.y) continue;
-        for (int x = cx - 2; x <= cx + 2; ++x) {
-          if (x < 0 || x >= g.size.x) continue;
+    // A candidate lies within rmax + Rg of the image, so its clamped cell lies in
+    // the per-axis cell range of that ball (edge cells are open outward: they
+    // also hold clamped bodies outside the domain), intersected with the 2-cell
+    // window.
+    const double reach = (a.rmax + Rg) * (1.0 + 1e-6) + coord_slack(xg, xg);
+    const int x0 = axis_lo(xg.x, g.mn.x, g.inv.x, g.size.x, reach, cx), x1 = axis_hi(xg.x, g.mn.x, g.inv.x, g.size.x, reach, cx);
+    const int y0 = axis_lo(xg.y, g.mn.y, g.inv.y, g.size.y, reach, cy), y1 = axis_hi(xg.y, g.mn.y, g.inv.y, g.size.y, reach, cy);
+    const int z0 = axis_lo(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz), z1 = axis_hi(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz);
+    for (int z = z0; z <= z1; ++z) {
+      for (int y = y0; y <= y1; ++y) {
+        for (int x = x0; x <= x1; ++x) {
           const int h = lin3(make_int3(x, y, z), g.size);
           const int st = g2_start[h];
           if (st < 0) continue;
