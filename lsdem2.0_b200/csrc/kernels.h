@@ -43,6 +43,7 @@ struct ShapeView {
   // precision form: SDF values / template spacing in 16-bit floats, FP32 nodes
   const unsigned short* sdf16;  // same offsets as sdf; FP16 or BF16 bits
   const float4* node_pos_f;     // FP32 copy of node_pos
+  const float* lip;             // per shape: largest |phi| difference of grid neighbours, in spacings
 };
 
 // Arithmetic form of the narrowphase and contact forces.
@@ -120,6 +121,17 @@ void scan_i64(const long long* in, long long* out, long long n, long long* tmp, 
 void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorted_idx, int* sorted_key, int* start,
                  int* end, cudaStream_t s);
 
+// Precision form: nodes the FP32 screen could not reject, by pair, for the FP64
+// contact pass. One node cursor per step; one pair list per narrowphase launch
+// (0: particles and walls, 1: periodic images).
+struct MaybeView {
+  int* node;    // cap node ids
+  int cap;
+  int4* pair;   // 2 * pcap entries {A, kind << 24 | slot, node start, node count}
+  int pcap;
+  int* ctr;     // [0] node cursor, [1 + launch] pairs queued
+};
+
 struct StepArgs {
   BodyView P;       // particles
   BodyView W;       // walls
@@ -139,6 +151,7 @@ struct StepArgs {
   int flags;        // FIX_* bits
   int precision;    // PREC_*
   double rmax;      // largest particle bounding radius
+  MaybeView mb;
 };
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);

@@ -311,6 +311,11 @@ struct lsdem_solver {
   DArr<double4> s_cl;
   DArr<unsigned short> s_sdf16;
   DArr<float4> s_node_f;
+  DArr<float> s_lip;
+  // precision form: screened nodes and queued pairs (per-step scratch)
+  DArr<int> mb_node, mb_ctr;
+  DArr<int4> mb_pair;
+  long long mb_cap = 0, mb_pcap = 0;
   std::vector<int> h_node_off, h_cl_off;
   GridP pg{}, wg{};
   DArr<int> cell_idx, cell_start, cell_end, sorted_key;
@@ -495,6 +500,19 @@ void alloc_contacts(lsdem_solver* s, ContactsDev& c, long long cap) {
   c.geom = false;
 }
 
+// Scratch of the precision form, sized with the contact capacity.
+void alloc_maybe(lsdem_solver* s) {
+  if (s->precision == PREC_FP64) return;
+  const long long cap = std::min<long long>(s->cap_c, 0x7fffffffLL);
+  if (s->mb_cap == cap && s->mb_node.p) return;
+  s->mb_cap = cap;
+  s->mb_pcap = std::max<long long>(cap / 2, 1024);
+  CK(s->mb_node.alloc((size_t)cap));
+  CK(s->mb_pair.alloc((size_t)(2 * s->mb_pcap)));
+  CK(s->mb_ctr.alloc(4));
+  CK(s->mb_ctr.zero(s->stream));
+}
+
 void ensure_geom(lsdem_solver* s, ContactsDev& c) {
   if (c.geom) return;
   const size_t m = (size_t)std::max(c.cap, 1LL);
@@ -618,8 +636,26 @@ void initialize(lsdem_solver* s) {
     std::vector<float4> nf(node_pos.size());
     for (size_t i = 0; i < node_pos.size(); ++i)
       nf[i] = make_float4((float)node_pos[i].x, (float)node_pos[i].y, (float)node_pos[i].z, 0.f);
+    // per template: largest difference of neighbouring SDF values, in spacings
+    // (Lipschitz bound of the trilinear interpolant per grid unit and axis)
+    std::vector<float> lip;
+    for (const ShapeHost& sh : s->shapes) {
+      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
+      double m = 0.;
+      for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+          for (int x = 0; x < nx; ++x) {
+            const size_t i = (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z);
+            const double v = sh.sdf[i];
+            if (x + 1 < nx) m = std::max(m, std::fabs(sh.sdf[i + 1] - v));
+            if (y + 1 < ny) m = std::max(m, std::fabs(sh.sdf[i + nx] - v));
+            if (z + 1 < nz) m = std::max(m, std::fabs(sh.sdf[i + (size_t)nx * ny] - v));
+          }
+      lip.push_back((float)(m / sh.h * (1.0 + 1e-6)));
+    }
     CK(s->s_sdf16.upload(sdf16.data(), sdf16.size(), st));
     CK(s->s_node_f.upload(nf.data(), nf.size(), st));
+    CK(s->s_lip.upload(lip.data(), lip.size(), st));
   }
   // node ids (LSBoundaryNode order: particle by particle, caller node order)
   s->P.node_base.resize(s->P.n());
@@ -664,6 +700,7 @@ void initialize(lsdem_solver* s) {
   alloc_slots(s);
   alloc_contacts(s, s->con[0], s->cap_c);
   alloc_contacts(s, s->con[1], s->cap_c);
+  alloc_maybe(s);
   s->hp = 0;
   s->hist_count = 0;
   // bonds
@@ -703,6 +740,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.cl_sphere = s->s_cl.p;
   a.S.sdf16 = s->s_sdf16.p;
   a.S.node_pos_f = s->s_node_f.p;
+  a.S.lip = s->s_lip.p;
   a.pg = s->pg;
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
@@ -736,6 +774,9 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.flags = s->flags;
   a.precision = s->precision;
   a.rmax = s->rmax_p;
+  a.mb.node = s->mb_node.p; a.mb.cap = (int)s->mb_cap;
+  a.mb.pair = s->mb_pair.p; a.mb.pcap = (int)s->mb_pcap;
+  a.mb.ctr = s->precision == PREC_FP64 ? nullptr : s->mb_ctr.p;
   return a;
 }
 
@@ -820,7 +861,9 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
   // kernels launched by this step: kick/drift/keys, cell sort (9), candidates,
   // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (8),
   // image compaction + candidates, ghost narrowphase; bonds
-  if (a.P.n > 0) s->launches += 13 + (s->nsets > 0 ? 13 : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  // (the precision form adds one contact pass per narrowphase)
+  const int nf = s->precision == PREC_FP64 ? 0 : 1;
+  if (a.P.n > 0) s->launches += 13 + nf + (s->nsets > 0 ? 13 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
 }
@@ -914,6 +957,7 @@ void grow(lsdem_solver* s) {
     alloc_contacts(s, s->con[1], s->cap_c);
     if (g0) ensure_geom(s, s->con[0]);
     if (g1) ensure_geom(s, s->con[1]);
+    alloc_maybe(s);
     s->grow_contacts = false;
   }
 }

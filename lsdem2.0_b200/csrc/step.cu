@@ -57,6 +57,7 @@ __global__ void k_integrate_first(StepArgs a) {
     if (a.C_old.count) atomicMax(&a.status->need_contact, *a.C_old.count);
     *a.C.count = 0;
     if (a.G.count) *a.G.count = 0;
+    if (a.mb.ctr) a.mb.ctr[0] = a.mb.ctr[1] = a.mb.ctr[2] = 0;
   }
   if (i < a.P.n) {
     const BodyView& P = a.P;
@@ -411,52 +412,72 @@ LD const SlotView& slots_of(const StepArgs& a, bool old) {
   return old ? a.pgh_old : a.pgh;
 }
 
-// Processes one (A, partner) pair with the whole warp. Contacts are found in
-// two sweeps over the surviving node clusters: the first counts them (ballot),
-// one atomic reserves a contiguous segment ordered by node, the second
-// recomputes the contact geometry, carries the tangential spring over from the
-// previous step's segment of the same pair, evaluates the linear contact force
-// and writes the contact. The partner's reaction is reduced over the warp and
-// added with one atomic per component.
+// The reference's per-node test in FP64: admission, then node inside the
+// partner's SDF grid with phi <= 0.
 template <int KIND>
-LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, int* s_cl, unsigned* s_mask,
-                int* s_old, double3& FA, double3& TA) {
+LD bool node_hits(const StepArgs& a, const SelfCtx& S, const Partner& P, int ni) {
+  const double3 w = node_world(a, S, ni);
+  if (!node_admitted<KIND>(a, w, P)) return false;
+  double ov, fx, fy, fz, cr[8];
+  return sdf_eval(w, P, ov, fx, fy, fz, cr);
+}
+
+// Contact geometry, carried-over spring and linear contact force of one
+// admitted node (LSParticleContactDetectionKernel.cu:63-115, contactKernel.cu:75-117 /
+// :155-190 / :225-270); writes the contact at pos.
+template <int KIND>
+LD void contact_node(const StepArgs& a, const SelfCtx& S, const Partner& P, const PairK& K, int ni, int ostart,
+                     int ocnt, bool staged, const int* s_old, int pos, bool can_write, double3& FA, double3& TA,
+                     double3& FB, double3& TB) {
+  const double3 w = node_world(a, S, ni);
+  double ov, fx, fy, fz, cr[8];
+  sdf_eval(w, P, ov, fx, fy, fz, cr);
+  double3 n = sdf_grad(fx, fy, fz, cr, a.flags);
+  n = rotate(P.q, n);
+  n = normalize_dev(n);
+  const double3 pc = w + 0.5 * ov * n;
+  // carried-over spring: binary search of node ni in the old segment (sorted by node)
+  double3 spring = d3(0., 0., 0.);
+  int lo = 0, hi = ocnt - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = staged ? s_old[mid] : a.C_old.node[ostart + mid];
+    if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
+    if (v < ni) lo = mid + 1; else hi = mid - 1;
+  }
+  const double3 vc = S.v + cross(S.w, pc - S.x) - (P.v + cross(P.w, pc - P.x));
+  double3 F;
+  linear_contact(F, spring, vc, n, ov, a.dt, K);
+  if (can_write) {
+    a.C.node[pos] = ni;
+    a.C.spring[pos] = spring;
+    if (a.C.point) {
+      a.C.point[pos] = pc;
+      a.C.normal[pos] = n;
+      a.C.overlap[pos] = ov;
+      a.C.en_n[pos] = 0.5 * ov * ov * K.kn;
+      a.C.en_s[pos] = 0.5 * len2(spring) * K.ks;
+    }
+  }
+  FA += F;
+  TA += cross(pc - S.x, F);
+  FB -= F;
+  TB += cross(pc - P.x, -F);
+}
+
+// Second half of a pair, shared by both arithmetic forms: given the ballots of
+// admitted nodes per chunk of 32 (s_mask; node_at(k) is this lane's node of
+// chunk k, chunks in ascending node order), one
+// atomic reserves a contiguous segment ordered by node, the previous step's
+// segment of the same pair is located, and the contacts are evaluated and
+// written in FP64. The partner's reaction is reduced over the warp and added
+// with one atomic per component.
+template <int KIND, class NodeAt>
+LD void finish_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, const Partner& P,
+                    NodeAt node_at, const unsigned* s_mask, int* s_old, int nsurv, int total, double3& FA,
+                    double3& TA) {
   const int lane = threadIdx.x & 31;
-  __syncwarp();  // the previous pair's second sweep may still read s_cl / s_mask
-  const Partner P = load_partner<KIND>(a, pid);
   const SlotView& cur = slots_of<KIND>(a, false);
-  // cluster culling
-  int nsurv = 0;
-  for (int c0 = 0; c0 < S.ncl; c0 += 32) {
-    const int c = c0 + lane;
-    bool keep = false;
-    if (c < S.ncl) {
-      const double4 sp = a.S.cl_sphere[S.cl0 + c];
-      const double3 wc = rotate(S.q, d3(sp.x, sp.y, sp.z) * S.sc) + S.x;
-      keep = cluster_may_hit<KIND>(wc, sp.w * S.sc, P);
-    }
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
-    nsurv += __popc(m);
-  }
-  __syncwarp();
-  // sweep 1: admission + SDF test
-  int total = 0;
-  for (int k = 0; k < nsurv; ++k) {
-    const int ni = s_cl[k] * 32 + lane;
-    bool hit = false;
-    if (ni < S.nn) {
-      const double3 w = node_world(a, S, ni);
-      if (node_admitted<KIND>(a, w, P)) {
-        double ov, fx, fy, fz, cr[8];
-        hit = sdf_eval(w, P, ov, fx, fy, fz, cr);
-      }
-    }
-    const unsigned m = __ballot_sync(FULL, hit);
-    if (lane == 0) s_mask[k] = m;
-    total += __popc(m);
-  }
-  __syncwarp();
   const size_t sidx = (size_t)A * cur.cap + slot;
   int base = 0;
   if (lane == 0 && total > 0) base = atomicAdd(a.C.count, total);
@@ -491,51 +512,14 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
     for (int j = lane; j < ocnt; j += 32) s_old[j] = a.C_old.node[ostart + j];
   __syncwarp();
   const PairK K = pair_constants<KIND>(a, A, P);
-  // sweep 2
   double3 FB = d3(0., 0., 0.), TB = d3(0., 0., 0.);
   int off = 0;
   for (int k = 0; k < nsurv; ++k) {
     const unsigned m = s_mask[k];
     if (m == 0) continue;
-    if ((m >> lane) & 1u) {
-      const int ni = s_cl[k] * 32 + lane;
-      const double3 w = node_world(a, S, ni);
-      double ov, fx, fy, fz, cr[8];
-      sdf_eval(w, P, ov, fx, fy, fz, cr);
-      double3 n = sdf_grad(fx, fy, fz, cr, a.flags);
-      n = rotate(P.q, n);
-      n = normalize_dev(n);
-      const double3 pc = w + 0.5 * ov * n;
-      // carried-over spring: binary search of node ni in the old segment (sorted by node)
-      double3 spring = d3(0., 0., 0.);
-      int lo = 0, hi = ocnt - 1;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const int v = staged ? s_old[mid] : a.C_old.node[ostart + mid];
-        if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
-        if (v < ni) lo = mid + 1; else hi = mid - 1;
-      }
-      // contact force (contactKernel.cu:75-117 / :155-190 / :225-270)
-      const double3 vc = S.v + cross(S.w, pc - S.x) - (P.v + cross(P.w, pc - P.x));
-      double3 F;
-      linear_contact(F, spring, vc, n, ov, a.dt, K);
-      const int pos = base + off + __popc(m & lanemask_lt());
-      if (can_write) {
-        a.C.node[pos] = ni;
-        a.C.spring[pos] = spring;
-        if (a.C.point) {
-          a.C.point[pos] = pc;
-          a.C.normal[pos] = n;
-          a.C.overlap[pos] = ov;
-          a.C.en_n[pos] = 0.5 * ov * ov * K.kn;
-          a.C.en_s[pos] = 0.5 * len2(spring) * K.ks;
-        }
-      }
-      FA += F;
-      TA += cross(pc - S.x, F);
-      FB -= F;
-      TB += cross(pc - P.x, -F);
-    }
+    if ((m >> lane) & 1u)
+      contact_node<KIND>(a, S, P, K, node_at(k), ostart, ocnt, staged, s_old,
+                         base + off + __popc(m & lanemask_lt()), can_write, FA, TA, FB, TB);
     off += __popc(m);
   }
   if (KIND != KIND_WALL && !(KIND == KIND_GHOST && P.real == A)) {
@@ -546,6 +530,44 @@ LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, i
       atomic_add3(a.P.torque, P.real, TB);
     }
   }
+}
+
+// Processes one (A, partner) pair with the whole warp in FP64: cluster culling,
+// then a first sweep over the surviving clusters that ballots the admitted
+// nodes, then finish_pair.
+template <int KIND>
+LD void do_pair(const StepArgs& a, int A, int slot, int pid, const SelfCtx& S, int* s_cl, unsigned* s_mask,
+                int* s_old, double3& FA, double3& TA) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();  // the previous pair's second sweep may still read s_cl / s_mask
+  const Partner P = load_partner<KIND>(a, pid);
+  // cluster culling
+  int nsurv = 0;
+  for (int c0 = 0; c0 < S.ncl; c0 += 32) {
+    const int c = c0 + lane;
+    bool keep = false;
+    if (c < S.ncl) {
+      const double4 sp = a.S.cl_sphere[S.cl0 + c];
+      const double3 wc = rotate(S.q, d3(sp.x, sp.y, sp.z) * S.sc) + S.x;
+      keep = cluster_may_hit<KIND>(wc, sp.w * S.sc, P);
+    }
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
+    nsurv += __popc(m);
+  }
+  __syncwarp();
+  // sweep 1: admission + SDF test
+  int total = 0;
+  for (int k = 0; k < nsurv; ++k) {
+    const int ni = s_cl[k] * 32 + lane;
+    const bool hit = ni < S.nn && node_hits<KIND>(a, S, P, ni);
+    const unsigned m = __ballot_sync(FULL, hit);
+    if (lane == 0) s_mask[k] = m;
+    total += __popc(m);
+  }
+  __syncwarp();
+  finish_pair<KIND>(a, A, slot, pid, S, P, [&](int k) { return s_cl[k] * 32 + lane; }, s_mask, s_old, nsurv, total,
+                    FA, TA);
 }
 
 template <int KINDS>
@@ -586,24 +608,36 @@ __global__ void __launch_bounds__(NP_WARPS * 32, 2) k_narrowphase(StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Precision form: FP32 geometry and contact law on 16-bit SDF templates.
+// Precision form: certified FP32 screening on 16-bit SDF templates.
 //
-// Positions stay FP64: each pair forms d = xA - xB in FP64 and rounds it to FP32,
-// so node coordinates relative to the partner keep FP32 precision at any
-// distance from the origin. SDF values are stored as phi / h of the template in
-// FP16 or BF16 and scaled by the particle's spacing after interpolation. The
-// tangential spring is carried over and integrated in FP64; forces are summed in
-// FP32 per warp and added to the FP64 particle sums.
+// Almost every node the narrowphase visits is rejected (outside the partner's
+// bounding sphere or cell window, or phi > 0). The precision form makes those
+// rejections in FP32 against SDF templates stored as phi / h in FP16 or BF16,
+// and rejects a node only when error bounds prove that the FP64 test
+// (node_hits) rejects it too. Every node it cannot reject is decided by
+// node_hits itself, and every contact is evaluated by the FP64 code of
+// finish_pair. Pair lists, contact segments and forces are therefore those of
+// the FP64 form; the 16-bit store and FP32 arithmetic only make the rejections
+// cheaper.
+//
+// Error bounds (unit roundoff u = 2^-24; |.|_1 norms bound the Euclidean ones):
+// a node offset ra = q_A (x) node * scale and the partner-relative position
+// r = ra + d, d = xA - xB rounded from FP64, carry at most ~20u |ra|_1 + 2u |d|_1
+// rounding each; the rotation into the partner frame and the grid transform
+// add ~20u |r|_1 + u |o|_1 + 2u |g|_1. EPS_F = 1.6e-5 (~270u) bounds all of it
+// with a wide margin. The interpolated phi / h of the 16-bit store differs from
+// the FP64 value at the same grid point by at most Q max|c| (Q = 2^-11 for FP16,
+// 2^-8 for BF16, round to nearest, plus the FP32 rounding of phi / h), and a
+// grid-point error eg moves the piecewise-trilinear phi / h by at most
+// 3 L eg, L = the largest difference between neighbouring SDF values of the
+// partner's template in spacings.
 LD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
 LD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
 LD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
-LD float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
 LD float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
-LD float3 operator*(float s, float3 a) { return f3(a.x * s, a.y * s, a.z * s); }
-LD float3& operator+=(float3& a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
-LD float3& operator-=(float3& a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
 LD float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 LD float3 crossf(float3 a, float3 b) { return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+LD float n1f(float3 v) { return fabsf(v.x) + fabsf(v.y) + fabsf(v.z); }
 LD float3 tof(double3 v) { return f3((float)v.x, (float)v.y, (float)v.z); }
 LD double3 tod(float3 v) { return d3(v.x, v.y, v.z); }
 LD float4 toq(Quat q) { return make_float4((float)q.q0, (float)q.q1, (float)q.q2, (float)q.q3); }
@@ -619,15 +653,19 @@ LD float3 rotinvf(float3 v, float4 q) {
   return v + t * q.x + crossf(qv, t);
 }
 
+static constexpr float EPS_F = 1.6e-5f;
+
 template <int SDFK>
 LD float decode16(unsigned short b) {
   if (SDFK == PREC_FP32_BF16) return __uint_as_float(((unsigned)b) << 16);
   return __half2float(__ushort_as_half(b));
 }
+// relative quantisation bound of the 16-bit store (with margin)
+template <int SDFK>
+LD constexpr float quant16() { return SDFK == PREC_FP32_BF16 ? 3.95e-3f : 4.95e-4f; }
 
 struct SelfF {
   double3 x;   // FP64 centre (cell-window tests of walls and images)
-  float3 v, w;
   float4 q;
   float sc;
   int n0, nn, cl0, ncl;
@@ -635,85 +673,96 @@ struct SelfF {
 
 struct PartnerF {
   float3 d;     // xA - x(partner)
+  float n1d;    // |d|_1
   float4 q;
   float r;
   float3 o;
+  float n1o;    // |o|_1
   float invh, h;
+  float lip;    // largest neighbour difference of the template's phi / h
   int3 gs;
   const unsigned short* sdf;
-  int key, real;
-  float3 v, w;
+  int key;
 };
 
 template <int KIND>
-LD PartnerF partner_f(const StepArgs& a, const Partner& P, const SelfF& S) {
+LD PartnerF partner_f(const StepArgs& a, const Partner& P, const SelfF& S, int shape) {
   PartnerF F;
   F.d = tof(S.x - P.x);
+  F.n1d = n1f(F.d);
   F.q = toq(P.q);
   F.r = (float)P.r;
   F.o = tof(P.o);
+  F.n1o = n1f(F.o);
   F.invh = (float)P.invh;
   F.h = (float)(1.0 / P.invh);
+  F.lip = a.S.lip[shape];
   F.gs = P.gs;
   F.sdf = a.S.sdf16 + (P.sdf - a.S.sdf);
   F.key = P.key;
-  F.real = P.real;
-  F.v = tof(P.v);
-  F.w = tof(P.w);
   return F;
 }
 
-// Trilinear evaluation in FP32; returns the overlap (in length units) through ov.
-template <int SDFK>
-LD bool sdf_eval_f(float3 r, const PartnerF& P, float& ov, float& fx, float& fy, float& fz, float* c) {
+// Cell-window admission of walls and images from the FP32 node offset:
+// 0 = certainly rejected, 1 = certainly admitted, 2 = the FP64 node may lie in
+// a neighbouring cell (within the error bound of a cell boundary).
+template <int KIND>
+LD int window_state(const StepArgs& a, double3 x, float3 ra, float n1ra, int key) {
+  const GridP& g = KIND == KIND_WALL ? a.wg : a.pg;
+  const double3 w = x + tod(ra);
+  const double e = (double)(EPS_F * n1ra) + 1e-14 * (fabs(w.x) + fabs(w.y) + fabs(w.z));
+  const double ux = (w.x - g.mn.x) * g.inv.x, uy = (w.y - g.mn.y) * g.inv.y, uz = (w.z - g.mn.z) * g.inv.z;
+  if (fabs(ux - rint(ux)) <= e * g.inv.x + 1e-9 || fabs(uy - rint(uy)) <= e * g.inv.y + 1e-9 ||
+      fabs(uz - rint(uz)) <= e * g.inv.z + 1e-9)
+    return 2;
+  int3 c, lo, hi;
+  node_window(w, g, c, lo, hi);
+  return in_window(key, g, c, lo, hi) ? 1 : 0;
+}
+
+// False only when node_hits certainly rejects the node.
+template <int KIND, int SDFK>
+LD bool node_may_hit_f(const StepArgs& a, const SelfF& S, const PartnerF& P, float3 ra, float3 r) {
+  const float n1ra = n1f(ra);
+  const float el = EPS_F * (n1ra + P.n1d);
+  if (KIND == KIND_PP) {
+    const float R = P.r * (1.0f + 1e-6f) + el;
+    if (dotf(r, r) > R * R) return false;
+  } else {
+    if (window_state<KIND>(a, S.x, ra, n1ra, P.key) == 0) return false;
+  }
   const float3 l = rotinvf(r, P.q);
   const float gx = (l.x - P.o.x) * P.invh, gy = (l.y - P.o.y) * P.invh, gz = (l.z - P.o.z) * P.invh;
+  const float eg = P.invh * EPS_F * (n1ra + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
+  // the FP64 test rejects g < 0 or g >= size - 1 on any axis
+  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
+  if (gx < -eg || gy < -eg || gz < -eg || gx >= ux + eg || gy >= uy + eg || gz >= uz + eg) return false;
+  if (gx < eg || gy < eg || gz < eg || gx >= ux - eg || gy >= uy - eg || gz >= uz - eg) return true;
   const int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
-  if (i0 < 0 || j0 < 0 || k0 < 0) return false;
-  if (i0 >= P.gs.x - 1 || j0 >= P.gs.y - 1 || k0 >= P.gs.z - 1) return false;
-  fx = gx - (float)i0;
-  fy = gy - (float)j0;
-  fz = gz - (float)k0;
+  const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
   const int sy = P.gs.x, sz = P.gs.x * P.gs.y;
   const unsigned short* b = P.sdf + (k0 * sz + j0 * sy + i0);
-  c[0] = decode16<SDFK>(__ldg(b));
-  c[1] = decode16<SDFK>(__ldg(b + 1));
-  c[2] = decode16<SDFK>(__ldg(b + sy));
-  c[3] = decode16<SDFK>(__ldg(b + sy + 1));
-  c[4] = decode16<SDFK>(__ldg(b + sz));
-  c[5] = decode16<SDFK>(__ldg(b + sz + 1));
-  c[6] = decode16<SDFK>(__ldg(b + sz + sy));
-  c[7] = decode16<SDFK>(__ldg(b + sz + sy + 1));
-  const float wx0 = 1.f - fx, wx1 = fx, wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
-  const float phi = c[0] * wx0 * wy0 * wz0 + c[1] * wx1 * wy0 * wz0 + c[2] * wx0 * wy1 * wz0 +
-                    c[3] * wx1 * wy1 * wz0 + c[4] * wx0 * wy0 * wz1 + c[5] * wx1 * wy0 * wz1 +
-                    c[6] * wx0 * wy1 * wz1 + c[7] * wx1 * wy1 * wz1;
-  ov = -phi * P.h;
-  return ov >= 0.f;
+  const float c0 = decode16<SDFK>(__ldg(b)), c1 = decode16<SDFK>(__ldg(b + 1));
+  const float c2 = decode16<SDFK>(__ldg(b + sy)), c3 = decode16<SDFK>(__ldg(b + sy + 1));
+  const float c4 = decode16<SDFK>(__ldg(b + sz)), c5 = decode16<SDFK>(__ldg(b + sz + 1));
+  const float c6 = decode16<SDFK>(__ldg(b + sz + sy)), c7 = decode16<SDFK>(__ldg(b + sz + sy + 1));
+  const float wx0 = 1.f - fx, wy0 = 1.f - fy, wz0 = 1.f - fz;
+  const float phi = ((c0 * wx0 + c1 * fx) * wy0 + (c2 * wx0 + c3 * fx) * fy) * wz0 +
+                    ((c4 * wx0 + c5 * fx) * wy0 + (c6 * wx0 + c7 * fx) * fy) * fz;
+  const float cmax = fmaxf(fmaxf(fmaxf(fabsf(c0), fabsf(c1)), fmaxf(fabsf(c2), fabsf(c3))),
+                           fmaxf(fmaxf(fabsf(c4), fabsf(c5)), fmaxf(fabsf(c6), fabsf(c7))));
+  const float band = cmax * (quant16<SDFK>() + 4e-6f) + 3.0f * P.lip * eg + 1e-7f;
+  return !(phi > band);  // NaN / Inf corners are never rejected
 }
 
-LD float3 sdf_grad_f(float fx, float fy, float fz, const float* c, int flags) {
-  const float x = (flags & FIX_GRADIENT) ? fx : (float)(int)fx;
-  const float wx0 = 1.f - x, wx1 = x, wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
-  return f3((c[1] - c[0]) * wy0 * wz0 + (c[3] - c[2]) * wy1 * wz0 + (c[5] - c[4]) * wy0 * wz1 + (c[7] - c[6]) * wy1 * wz1,
-            (c[2] - c[0]) * wx0 * wz0 + (c[3] - c[1]) * wx1 * wz0 + (c[6] - c[4]) * wx0 * wz1 + (c[7] - c[5]) * wx1 * wz1,
-            (c[4] - c[0]) * wx0 * wy0 + (c[5] - c[1]) * wx1 * wy0 + (c[6] - c[2]) * wx0 * wy1 + (c[7] - c[3]) * wx1 * wy1);
-}
-
+// Conservative cluster cull in FP32 (the bounds of node_may_hit_f applied to the
+// cluster's bounding sphere).
 template <int KIND>
-LD bool node_admitted_f(const StepArgs& a, float3 ra, float3 r, const SelfF& S, const PartnerF& P) {
-  if (KIND == KIND_PP) return !(dotf(r, r) > P.r * P.r);
-  const double3 w = S.x + tod(ra);
-  int3 c, lo, hi;
-  node_window(w, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
-  return in_window(P.key, KIND == KIND_WALL ? a.wg : a.pg, c, lo, hi);
-}
-
-template <int KIND>
-LD bool cluster_may_hit_f(float3 wc, float rad, const PartnerF& P) {
-  const float slack = 1e-6f * (fabsf(P.d.x) + fabsf(P.d.y) + fabsf(P.d.z));
+LD bool cluster_may_hit_f(float3 cA, float rad, const PartnerF& P) {
+  const float3 wc = cA + P.d;
+  const float e = EPS_F * (n1f(cA) + P.n1d);
   if (KIND == KIND_PP) {
-    const float R = (P.r + rad) * (1.0f + 1e-5f) + slack;
+    const float R = (P.r + rad) * (1.0f + 1e-6f) + e;
     return dotf(wc, wc) <= R * R;
   }
   const float3 l = rotinvf(wc, P.q);
@@ -722,56 +771,48 @@ LD bool cluster_may_hit_f(float3 wc, float rad, const PartnerF& P) {
   const float dy = fmaxf(fmaxf(P.o.y - l.y, l.y - hi.y), 0.f);
   const float dz = fmaxf(fmaxf(P.o.z - l.z, l.z - hi.z), 0.f);
   const float ext = (hi.x - P.o.x) + (hi.y - P.o.y) + (hi.z - P.o.z);
-  return sqrtf(dx * dx + dy * dy + dz * dz) <= rad * (1.0f + 1e-5f) + 1e-5f * ext + slack;
+  const float R = rad * (1.0f + 1e-6f) + e + EPS_F * (ext + P.n1o);
+  return dx * dx + dy * dy + dz * dz <= R * R;
 }
 
-// Linear contact in FP32 with the tangential spring carried and integrated in FP64.
-LD void linear_contact_f(float3& F, double3& spring, float3 vc, float3 n, float delta, float dt, const PairK& K) {
-  if (delta > 0.f) {
-    const float kn = (float)K.kn, ks = (float)K.ks, mu = (float)K.mu, cn = (float)K.cn, cs = (float)K.cs;
-    const float3 vn = dotf(vc, n) * n;
-    const float3 fn = kn * delta * n - cn * vn;
-    const float3 vs = vc - vn;
-    double3 s = d3(0., 0., 0.);
-    if (mu > 0.f && ks > 0.f) {
-      const double3 nd = tod(n);
-      double3 p1 = spring - dot(spring, nd) * nd;
-      const double a1 = len(p1);
-      if (!is_zero(a1)) p1 *= len(spring) / a1;
-      s = p1 + tod(vs) * (double)dt;
-      float3 fs = -ks * tof(s) - cs * vs;
-      const float afs = sqrtf(dotf(fs, fs)), afn = sqrtf(dotf(fn, fn));
-      if (afs > 1e-30f && afs > mu * afn) {
-        fs = fs * (mu * afn / afs);
-        s = -(tod(fs) + K.cs * tod(vs)) / K.ks;
-      }
-    }
-    spring = s;
-    F = fn + (-ks * tof(spring) - cs * vs);
-  } else {
-    spring = d3(0., 0., 0.);
-    F = f3(0.f, 0.f, 0.f);
-  }
+LD SelfCtx self_ctx(const StepArgs& a, int A) {
+  SelfCtx S;
+  S.x = a.P.pos[A]; S.v = a.P.vel[A]; S.w = a.P.angvel[A]; S.q = a.P.quat[A];
+  S.sc = a.P.scale[A];
+  const int sh = a.P.shape[A];
+  S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
+  S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
+  return S;
 }
 
-LD float3 warp_sum3f(float3 v) { return f3(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)); }
+template <int KIND>
+LD int partner_shape(const StepArgs& a, int pid) {
+  if (KIND == KIND_WALL) return a.W.shape[pid];
+  return a.P.shape[KIND == KIND_GHOST ? (pid >> 3) : pid];
+}
 
+// Screens one (A, partner) pair: FP32 cluster cull and node screen. The nodes
+// the screen cannot reject are written, in node order, to the precision-form
+// node buffer and the pair is queued for k_contacts_f; a pair without such
+// nodes gets its empty contact segment here.
 template <int KIND, int SDFK>
-LD void do_pair_f(const StepArgs& a, int A, int slot, int pid, const SelfF& S, int* s_cl, unsigned* s_mask,
-                  int* s_old, float3& FA, float3& TA) {
+LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const SelfF& S, int* s_cl,
+                      unsigned* s_mask) {
   const int lane = threadIdx.x & 31;
-  __syncwarp();
-  const Partner P64 = load_partner<KIND>(a, pid);
-  const PartnerF P = partner_f<KIND>(a, P64, S);
-  const SlotView& cur = slots_of<KIND>(a, false);
+  __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
+  PartnerF P;
+  {
+    const Partner P64 = load_partner<KIND>(a, pid);
+    P = partner_f<KIND>(a, P64, S, partner_shape<KIND>(a, pid));
+  }
   int nsurv = 0;
   for (int c0 = 0; c0 < S.ncl; c0 += 32) {
     const int c = c0 + lane;
     bool keep = false;
     if (c < S.ncl) {
       const double4 sp = a.S.cl_sphere[S.cl0 + c];
-      const float3 wc = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc) + P.d;
-      keep = cluster_may_hit_f<KIND>(wc, (float)sp.w * S.sc, P);
+      const float3 cA = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc);
+      keep = cluster_may_hit_f<KIND>(cA, (float)sp.w * S.sc, P);
     }
     const unsigned m = __ballot_sync(FULL, keep);
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
@@ -781,115 +822,57 @@ LD void do_pair_f(const StepArgs& a, int A, int slot, int pid, const SelfF& S, i
   int total = 0;
   for (int k = 0; k < nsurv; ++k) {
     const int ni = s_cl[k] * 32 + lane;
-    bool hit = false;
+    bool may = false;
     if (ni < S.nn) {
       const float4 nd = a.S.node_pos_f[S.n0 + ni];
       const float3 ra = rotf(S.q, f3(nd.x, nd.y, nd.z) * S.sc);
-      const float3 r = ra + P.d;
-      if (node_admitted_f<KIND>(a, ra, r, S, P)) {
-        float ov, fx, fy, fz, cr[8];
-        hit = sdf_eval_f<SDFK>(r, P, ov, fx, fy, fz, cr);
-      }
+      may = node_may_hit_f<KIND, SDFK>(a, S, P, ra, ra + P.d);
     }
-    const unsigned m = __ballot_sync(FULL, hit);
+    const unsigned m = __ballot_sync(FULL, may);
     if (lane == 0) s_mask[k] = m;
     total += __popc(m);
   }
   __syncwarp();
+  const SlotView& cur = slots_of<KIND>(a, false);
   const size_t sidx = (size_t)A * cur.cap + slot;
-  int base = 0;
-  if (lane == 0 && total > 0) base = atomicAdd(a.C.count, total);
-  base = __shfl_sync(FULL, base, 0);
-  const bool can_write = (base + total <= a.C.cap);
-  if (lane == 0) {
-    cur.seg_start[sidx] = base;
-    cur.seg_cnt[sidx] = can_write ? total : 0;
-    if (!can_write) atomicOr(&a.status->flags, OVF_CONTACT);
-  }
-  if (total == 0) return;
-  const SlotView& old = slots_of<KIND>(a, true);
-  int ostart = 0, ocnt = 0;
-  if (old.cnt != nullptr) {
-    const int on = old.cnt[A] < old.cap ? old.cnt[A] : old.cap;
-    for (int j0 = 0; j0 < on; j0 += 32) {
-      const int j = j0 + lane;
-      const bool match = j < on && old.id[(size_t)A * old.cap + j] == pid;
-      const unsigned m = __ballot_sync(FULL, match);
-      if (m) {
-        const int src = j0 + __ffs(m) - 1;
-        ostart = old.seg_start[(size_t)A * old.cap + src];
-        ocnt = old.seg_cnt[(size_t)A * old.cap + src];
-        break;
-      }
+  if (total == 0) {
+    if (lane == 0) {
+      cur.seg_start[sidx] = 0;
+      cur.seg_cnt[sidx] = 0;
     }
+    return;
   }
-  const bool staged = ocnt <= OLDCAP;
-  if (staged)
-    for (int j = lane; j < ocnt; j += 32) s_old[j] = a.C_old.node[ostart + j];
-  __syncwarp();
-  const PairK K = pair_constants<KIND>(a, A, P64);
-  float3 FB = f3(0.f, 0.f, 0.f), TB = f3(0.f, 0.f, 0.f);
+  int start = 0;
+  bool ok = false;
+  if (lane == 0) {
+    start = atomicAdd(&a.mb.ctr[0], total);
+    const int pi = atomicAdd(&a.mb.ctr[1 + li], 1);
+    ok = start + total <= a.mb.cap && pi < a.mb.pcap;
+    if (ok) {
+      a.mb.pair[(size_t)li * a.mb.pcap + pi] = make_int4(A, (KIND << 24) | slot, start, total);
+    } else {
+      atomicOr(&a.status->flags, OVF_CONTACT);
+      const long long need = start + total > 2LL * (pi + 1) ? start + total : 2LL * (pi + 1);
+      atomicMax(&a.status->need_contact, (int)(need < 0x7fffffff ? need : 0x7fffffff));
+    }
+    cur.seg_start[sidx] = 0;
+    cur.seg_cnt[sidx] = 0;
+  }
+  start = __shfl_sync(FULL, start, 0);
+  ok = __shfl_sync(FULL, ok, 0);
+  if (!ok) return;
   int off = 0;
   for (int k = 0; k < nsurv; ++k) {
     const unsigned m = s_mask[k];
-    if (m == 0) continue;
-    if ((m >> lane) & 1u) {
-      const int ni = s_cl[k] * 32 + lane;
-      const float4 nd = a.S.node_pos_f[S.n0 + ni];
-      const float3 ra = rotf(S.q, f3(nd.x, nd.y, nd.z) * S.sc);
-      const float3 r = ra + P.d;
-      float ov, fx, fy, fz, cr[8];
-      sdf_eval_f<SDFK>(r, P, ov, fx, fy, fz, cr);
-      float3 n = rotf(P.q, sdf_grad_f(fx, fy, fz, cr, a.flags));
-      const float l2 = dotf(n, n);
-      n = l2 > 1e-30f ? n * rsqrtf(l2) : f3(0.f, 0.f, 0.f);
-      const float3 pcA = ra + 0.5f * ov * n;
-      const float3 pcB = r + 0.5f * ov * n;
-      double3 spring = d3(0., 0., 0.);
-      int lo = 0, hi = ocnt - 1;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const int v = staged ? s_old[mid] : a.C_old.node[ostart + mid];
-        if (v == ni) { spring = a.C_old.spring[ostart + mid]; break; }
-        if (v < ni) lo = mid + 1; else hi = mid - 1;
-      }
-      const float3 vc = S.v + crossf(S.w, pcA) - (P.v + crossf(P.w, pcB));
-      float3 F;
-      linear_contact_f(F, spring, vc, n, ov, (float)a.dt, K);
-      const int pos = base + off + __popc(m & lanemask_lt());
-      if (can_write) {
-        a.C.node[pos] = ni;
-        a.C.spring[pos] = spring;
-        if (a.C.point) {
-          a.C.point[pos] = S.x + tod(pcA);
-          a.C.normal[pos] = tod(n);
-          a.C.overlap[pos] = ov;
-          a.C.en_n[pos] = 0.5 * (double)ov * (double)ov * K.kn;
-          a.C.en_s[pos] = 0.5 * len2(spring) * K.ks;
-        }
-      }
-      FA += F;
-      TA += crossf(pcA, F);
-      FB -= F;
-      TB += crossf(pcB, -F);
-    }
+    if ((m >> lane) & 1u) a.mb.node[start + off + __popc(m & lanemask_lt())] = s_cl[k] * 32 + lane;
     off += __popc(m);
-  }
-  if (KIND != KIND_WALL && !(KIND == KIND_GHOST && P.real == A)) {
-    FB = warp_sum3f(FB);
-    TB = warp_sum3f(TB);
-    if (lane == 0) {
-      atomic_add3(a.P.force, P.real, tod(FB));
-      atomic_add3(a.P.torque, P.real, tod(TB));
-    }
   }
 }
 
 template <int KINDS, int SDFK>
-__global__ void __launch_bounds__(NP_WARPS * 32, 3) k_narrowphase_f(StepArgs a) {
+__global__ void __launch_bounds__(NP_WARPS * 32, 4) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
-  __shared__ int s_old[NP_WARPS][OLDCAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ng_max = 0;
   for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
@@ -901,28 +884,64 @@ __global__ void __launch_bounds__(NP_WARPS * 32, 3) k_narrowphase_f(StepArgs a) 
     if (npp + nw + ngc == 0) continue;
     SelfF S;
     S.x = a.P.pos[A];
-    S.v = tof(a.P.vel[A]);
-    S.w = tof(a.P.angvel[A]);
     S.q = toq(a.P.quat[A]);
     S.sc = (float)a.P.scale[A];
     const int sh = a.P.shape[A];
     S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
     S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
-    float3 FA = f3(0.f, 0.f, 0.f), TA = f3(0.f, 0.f, 0.f);
     for (int j = 0; j < npp; ++j)
-      do_pair_f<KIND_PP, SDFK>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
+      screen_pair_f<KIND_PP, SDFK>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], li, S, s_cl[warp], s_mask[warp]);
     for (int j = 0; j < nw; ++j)
-      do_pair_f<KIND_WALL, SDFK>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
+      screen_pair_f<KIND_WALL, SDFK>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], li, S, s_cl[warp], s_mask[warp]);
     for (int j = 0; j < ngc; ++j)
-      do_pair_f<KIND_GHOST, SDFK>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], S, s_cl[warp], s_mask[warp], s_old[warp], FA, TA);
-    FA = warp_sum3f(FA);
-    TA = warp_sum3f(TA);
-    if (lane == 0) {
-      atomic_add3(a.P.force, A, tod(FA));
-      atomic_add3(a.P.torque, A, tod(TA));
-    }
+      screen_pair_f<KIND_GHOST, SDFK>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], li, S, s_cl[warp], s_mask[warp]);
   }
   if ((KINDS & 4) && lane == 0 && ng_max > 0) atomicMax(&a.status->need_ghost, ng_max);
+}
+
+// Queued pairs of the screen, one warp each, in FP64: the reference's node test
+// on the screened nodes, then finish_pair (segment, history, forces).
+template <int KIND>
+LD void contacts_pair(const StepArgs& a, int A, int slot, int start, int cnt, unsigned* s_mask, int* s_old) {
+  const int lane = threadIdx.x & 31;
+  const int pid = slots_of<KIND>(a, false).id[(size_t)A * slots_of<KIND>(a, false).cap + slot];
+  const SelfCtx S = self_ctx(a, A);
+  const Partner P = load_partner<KIND>(a, pid);
+  const int* nodes = a.mb.node + start;
+  const int nch = (cnt + 31) >> 5;
+  __syncwarp();  // the previous pair may still read s_mask / s_old
+  int total = 0;
+  for (int k = 0; k < nch; ++k) {
+    const int j = k * 32 + lane;
+    const bool hit = j < cnt && node_hits<KIND>(a, S, P, nodes[j]);
+    const unsigned m = __ballot_sync(FULL, hit);
+    if (lane == 0) s_mask[k] = m;
+    total += __popc(m);
+  }
+  __syncwarp();
+  double3 FA = d3(0., 0., 0.), TA = d3(0., 0., 0.);
+  finish_pair<KIND>(a, A, slot, pid, S, P, [&](int k) { return nodes[k * 32 + lane]; }, s_mask, s_old, nch, total,
+                    FA, TA);
+  FA = warp_sum3(FA);
+  TA = warp_sum3(TA);
+  if (lane == 0 && total > 0) {
+    atomic_add3(a.P.force, A, FA);
+    atomic_add3(a.P.torque, A, TA);
+  }
+}
+
+__global__ void __launch_bounds__(NP_WARPS * 32) k_contacts_f(StepArgs a, int li) {
+  __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  __shared__ int s_old[NP_WARPS][OLDCAP];
+  const int warp = threadIdx.x >> 5;
+  const int np = min(a.mb.ctr[1 + li], a.mb.pcap);
+  for (int p = blockIdx.x * NP_WARPS + warp; p < np; p += gridDim.x * NP_WARPS) {
+    const int4 e = a.mb.pair[(size_t)li * a.mb.pcap + p];
+    const int kind = e.y >> 24, slot = e.y & 0xffffff;
+    if (kind == KIND_PP) contacts_pair<KIND_PP>(a, e.x, slot, e.z, e.w, s_mask[warp], s_old[warp]);
+    else if (kind == KIND_WALL) contacts_pair<KIND_WALL>(a, e.x, slot, e.z, e.w, s_mask[warp], s_old[warp]);
+    else contacts_pair<KIND_GHOST>(a, e.x, slot, e.z, e.w, s_mask[warp], s_old[warp]);
+  }
 }
 
 static int g_num_sms = 0;
@@ -942,22 +961,27 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   int cap = num_sms() * 16;
   int blocks = want < cap ? want : cap;
   const dim3 g(blocks), b(NP_WARPS * 32);
-  if (a.precision == PREC_FP32_FP16) {
-    if (kinds == 3) k_narrowphase_f<3, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
-    else if (kinds == 1) k_narrowphase_f<1, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
-    else if (kinds == 4) k_narrowphase_f<4, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
-    else k_narrowphase_f<7, PREC_FP32_FP16><<<g, b, 0, s>>>(a);
-  } else if (a.precision == PREC_FP32_BF16) {
-    if (kinds == 3) k_narrowphase_f<3, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
-    else if (kinds == 1) k_narrowphase_f<1, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
-    else if (kinds == 4) k_narrowphase_f<4, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
-    else k_narrowphase_f<7, PREC_FP32_BF16><<<g, b, 0, s>>>(a);
-  } else {
+  if (a.precision == PREC_FP64) {
     if (kinds == 3) k_narrowphase<3><<<g, b, 0, s>>>(a);
     else if (kinds == 1) k_narrowphase<1><<<g, b, 0, s>>>(a);
     else if (kinds == 4) k_narrowphase<4><<<g, b, 0, s>>>(a);
     else k_narrowphase<7><<<g, b, 0, s>>>(a);
+    return;
   }
+  // precision form: screen, then the FP64 contact pass over the queued pairs
+  const int li = kinds == 4 ? 1 : 0;
+  if (a.precision == PREC_FP32_FP16) {
+    if (kinds == 3) k_screen_f<3, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 1) k_screen_f<1, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 4) k_screen_f<4, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
+    else k_screen_f<7, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
+  } else {
+    if (kinds == 3) k_screen_f<3, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 1) k_screen_f<1, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 4) k_screen_f<4, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
+    else k_screen_f<7, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
+  }
+  k_contacts_f<<<num_sms() * 4, NP_WARPS * 32, 0, s>>>(a, li);
 }
 
 // ---------------------------------------------------------------------------

@@ -18,13 +18,14 @@ def dense_ellipsoid_scene(scenes, n=64, n_nodes=300, n_grid=16, spacing=8.0e-3, 
     return sc
 
 
-def load_scene(lsdem, scenes, sc, **cap):
+def load_scene(lsdem, scenes, sc, precision=0, **cap):
     sv = lsdem.Solver()
     scenes.load_into(sv, sc)
     if "angvel" in sc:
         sv.set_state(angvel=sc["angvel"])
     if cap:
         sv.set_capacity(**cap)
+    sv.set_precision(precision)
     sv.set_record_contacts(True)
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
     return sv

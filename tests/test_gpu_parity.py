@@ -12,6 +12,10 @@ as history) and the results are compared:
 * contact geometry, carried-over springs, forces and torques within a relative
   tolerance of 1e-9 (FP64; the device normalises with rsqrt and contracts FMAs,
   the CPU oracle does neither).
+
+Each step test runs in the plain FP64 form and in both precision forms (FP32
+screening on FP16 / BF16 SDF templates): the screen only rejects nodes that the
+FP64 test provably rejects, so all three must meet the same bounds.
 """
 import numpy as np
 import pytest
@@ -66,11 +70,12 @@ def _compare_lists(gpu, orc, n_tot, label):
     return og, oo
 
 
+@pytest.mark.parametrize("prec", [0, 1, 2])
 @pytest.mark.parametrize("seed", [7, 11])
-def test_step_parity_particles_and_floor(lsdem, seed):
+def test_step_parity_particles_and_floor(lsdem, seed, prec):
     from lsdem_b200 import scenes
     sc = dense_ellipsoid_scene(scenes, n=64, seed=seed)
-    sv = load_scene(lsdem, scenes, sc)
+    sv = load_scene(lsdem, scenes, sc, precision=prec)
     dt = 1e-6
     prev = None
     for step in range(3):

@@ -1,5 +1,6 @@
 """Periodic images on the GPU against the oracle: wrap, image sets, image cell keys,
-contacts with images (per image set) and the resulting forces, from identical state.
+contacts with images (per image set) and the resulting forces, from identical state,
+in the plain FP64 form and in both precision forms.
 
 Uses a small, dense, triply periodic polydisperse scene of the four scaled templates, so
 that many particles touch images across the faces.
@@ -20,12 +21,14 @@ def _scene(lsdem, n=600, seed=21):
     return scenes.polydisperse_periodic(lsdem, n=n, box=box, seed=seed, templates=T, n_grid=16, n_nodes=200)
 
 
-def test_periodic_step_parity(lsdem):
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_periodic_step_parity(lsdem, prec):
     from lsdem_b200 import scenes
     ora = load_oracle()
     sc = _scene(lsdem)
     sv = lsdem.Solver()
     scenes.load_polydisperse(sv, sc)
+    sv.set_precision(prec)
     sv.set_record_contacts(True)
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
     box = {}
