@@ -10,10 +10,12 @@ diameters (median 2 mm, sigma 0.25), 48^3 SDF grids, 2,000 surface nodes each,
 0.1 m triply periodic cube, velocities N(0, 0.1 m/s), linear contact (kn 1e5,
 kt 0.8 kn, mu 0.5, e 0.6), dt 5e-7 s. Synthetic, seeded (no dataset).
 
-The headline form is the configuration's own: FP32 narrowphase and contact law
-on BF16 SDF templates, FP64 positions, integration and spring history. The same
-run times the FP16-template form and the plain FP64 form (the reference's
-arithmetic, bit-exact pair lists) and states each FP32 form's force error
+The headline form is the configuration's own precision form: the narrowphase
+screens nodes in FP32 against BF16 SDF templates, rejecting only nodes that
+error bounds prove the FP64 test rejects; the remaining nodes and all contacts
+are evaluated in FP64 (positions, integration, spring history stay FP64). The
+same run times the FP16-template form and the plain FP64 form (the reference's
+arithmetic, bit-exact pair lists) and states each precision form's force error
 against the FP64 path from the same state.
 
 One step = one full time step (half kick, drift, cell sort, candidates,
@@ -38,7 +40,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 
 FORMS = {"fp32-bf16": 2, "fp32-fp16": 1, "fp64": 0}
-DTYPE = {"fp32-bf16": "f32 (bf16 SDF, f64 state)", "fp32-fp16": "f32 (fp16 SDF, f64 state)", "fp64": "f64"}
+DTYPE = {"fp32-bf16": "f32 screen on bf16 SDF, f64 contacts", "fp32-fp16": "f32 screen on fp16 SDF, f64 contacts",
+         "fp64": "f64"}
 
 
 def _package():
@@ -59,14 +62,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes of the fused narrowphase + contact-force kernel (k_narrowphase):
-# per owner particle (pose, velocities, slot counts, force/torque write: 208 B), per
-# candidate pair (partner id, pose, velocities, shape and material scalars, segment
-# bookkeeping, reaction atomics: 236 B) and per contact (node id, FP64 spring read and
-# write, history lookup: 56 B).
+# Algorithmic bytes of the narrowphase kernel of each form.
+# FP64 form, k_narrowphase (detection and forces fused): per owner particle (pose,
+# velocities, slot counts, force/torque write: 208 B), per candidate pair (partner id,
+# pose, velocities, shape and material scalars, segment bookkeeping, reaction atomics:
+# 236 B) and per contact (node id, FP64 spring read and write, history lookup: 56 B).
+# Precision forms, k_screen_f (the screen; contacts are evaluated by the separate
+# FP64 contact pass): per owner particle (pose, scale, shape, slot count: 72 B) and
+# per candidate pair (partner id, pose, radius, grid origin and spacing, shape,
+# segment words: 120 B).
 B_PARTICLE = 208
 B_PAIR = 236
 B_CONTACT = 56
+B_PARTICLE_SCREEN = 72
+B_PAIR_SCREEN = 120
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
 
@@ -275,9 +284,14 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
     # per-phase device times (CUDA events between phases) from a separate, shorter run
     res["profile_steps"] = min(args.steps, 20)
     sv.set_profiling(True)
+    if prec != 0:
+        sv.set_screen_stats(True)
     sv.step(dt, res["profile_steps"])
     res["profile"] = sv.profile()
     sv.set_profiling(False)
+    if prec != 0:
+        res["screen"] = {k: v / res["profile_steps"] for k, v in sv.screen_stats().items()}
+        sv.set_screen_stats(False)
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -383,8 +397,13 @@ def main():
         avg_ms = (np_ms + g_ms) / max(1, np_calls + g_calls)
         # a step runs the particle/wall launch and the image launch: per-launch bytes = per-step / 2
         launches_per_step = 2 if g_calls else 1
-        bytes_launch = (B_PARTICLE * n * launches_per_step + B_PAIR * pairs + B_CONTACT * stats["contacts"]) / \
-            launches_per_step
+        if prec == 0:
+            kernel = "k_narrowphase"
+            bytes_launch = (B_PARTICLE * n * launches_per_step + B_PAIR * pairs + B_CONTACT * stats["contacts"]) / \
+                launches_per_step
+        else:
+            kernel = "k_screen_f"
+            bytes_launch = (B_PARTICLE_SCREEN * n * launches_per_step + B_PAIR_SCREEN * pairs) / launches_per_step
         achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
         b_step = B_STEP_PARTICLE * n + B_CONTACT * stats["contacts"] + 16 * pairs
         ms_step = head["ms"] / args.steps
@@ -399,13 +418,14 @@ def main():
                               f"({'>' if b_step > 126e6 else '<'} 126 MB L2)",
                            contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs),
             "forms": forms,
-            "roofline": {"bound": "hbm", "kernel": "k_narrowphase", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
             "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_step * 1e-3) / 1e9},
             "phases_ms_per_step": {k: v[0] / head["profile_steps"] for k, v in prof.items()},
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": n * (3 * 24 + 32),
                     "d2h_bytes_per_step": n * (5 * 24 + 32)},
+            "screen_per_step": head.get("screen"),
             "gpu_launches": head["launches"],
             "overflow_reruns": head["reruns"],
             "clocks": clk.summary(),

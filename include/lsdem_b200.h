@@ -184,13 +184,22 @@ void* lsdem_stream(const lsdem_solver* s);
 
 /* Device timing of the step phases with CUDA events on the solver stream
  * (no counterpart in the reference, which has no timers). Phases: 0 kick+drift+keys,
- * 1 cell sort, 2 candidates, 3 particle/wall narrowphase + forces, 4 periodic wrap +
- * ghost images + ghost candidates, 5 ghost narrowphase + forces, 6 bonds,
- * 7 second half kick. Enabling resets the totals. */
+ * 1 cell sort, 2 candidates, 3 particle/wall narrowphase + forces (precision forms:
+ * the FP32 screen), 4 periodic wrap + ghost images + ghost candidates, 5 ghost
+ * narrowphase + forces (precision forms: the screen), 6 bonds, 7 second half kick,
+ * 8 precision forms: FP64 contact pass of both narrowphases. ms and calls hold
+ * LSDEM_NUM_PHASES entries. Enabling resets the totals. */
+#define LSDEM_NUM_PHASES 9
 int lsdem_set_profiling(lsdem_solver* s, int on);
-int lsdem_get_profile(const lsdem_solver* s, double* ms8, long long* calls8);
+int lsdem_get_profile(const lsdem_solver* s, double* ms, long long* calls);
 /* Work counts of the last step: candidate pairs (particle, wall, ghost) and contacts. */
 int lsdem_step_stats(lsdem_solver* s, long long* out4);
+/* Precision forms: counters of the FP32 screen summed over all steps run while
+ * enabled (no counterpart in the reference): pairs screened, clusters tested,
+ * clusters kept by the bounding cull, clusters kept by the SDF cull, node tests,
+ * nodes queued for the FP64 test. Enabling resets them; off by default. */
+int lsdem_set_screen_stats(lsdem_solver* s, int on);
+int lsdem_get_screen_stats(lsdem_solver* s, long long* out6);
 
 /* Scene set-up helper: random sequential addition of spheres (in the given
  * order) in [lo, hi), periodic or not (the reference's sphere-packing helper,

@@ -94,6 +94,8 @@ _SIGS = {
     "lsdem_set_profiling": (C.c_int, [P, C.c_int]),
     "lsdem_get_profile": (C.c_int, [P, DP, LP]),
     "lsdem_step_stats": (C.c_int, [P, LP]),
+    "lsdem_set_screen_stats": (C.c_int, [P, C.c_int]),
+    "lsdem_get_screen_stats": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
 }
@@ -373,14 +375,14 @@ class Solver:
         return {"ids": ids, "bonded": bonded, "state": state}
 
     PHASES = ("kick_drift_keys", "cell_sort", "candidates", "narrowphase", "periodic", "ghost_narrowphase", "bonds",
-              "kick")
+              "kick", "contact_pass")
 
     def set_profiling(self, on=True):
         self._chk(lib.lsdem_set_profiling(self.h, 1 if on else 0), "set_profiling")
 
     def profile(self):
-        ms = np.zeros(8)
-        calls = np.zeros(8, np.int64)
+        ms = np.zeros(len(self.PHASES))
+        calls = np.zeros(len(self.PHASES), np.int64)
         self._chk(lib.lsdem_get_profile(self.h, _dp(ms), calls.ctypes.data_as(LP)), "get_profile")
         return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(self.PHASES)}
 
@@ -388,6 +390,17 @@ class Solver:
         o = np.zeros(4, np.int64)
         self._chk(lib.lsdem_step_stats(self.h, o.ctypes.data_as(LP)), "step_stats")
         return {"pairs_particle": int(o[0]), "pairs_wall": int(o[1]), "pairs_ghost": int(o[2]), "contacts": int(o[3])}
+
+    SCREEN_COUNTERS = ("pairs", "clusters", "clusters_bounding_cull", "clusters_sdf_cull", "node_tests",
+                       "nodes_queued")
+
+    def set_screen_stats(self, on=True):
+        self._chk(lib.lsdem_set_screen_stats(self.h, 1 if on else 0), "set_screen_stats")
+
+    def screen_stats(self):
+        o = np.zeros(6, np.int64)
+        self._chk(lib.lsdem_get_screen_stats(self.h, o.ctypes.data_as(LP)), "get_screen_stats")
+        return dict(zip(self.SCREEN_COUNTERS, (int(v) for v in o)))
 
     def device_pointers(self):
         ptrs = [P() for _ in range(6)]

@@ -43,7 +43,8 @@ struct ShapeView {
   // precision form: SDF values / template spacing in 16-bit floats, FP32 nodes
   const unsigned short* sdf16;  // same offsets as sdf; FP16 or BF16 bits
   const float4* node_pos_f;     // FP32 copy of node_pos
-  const float* lip;             // per shape: largest |phi| difference of grid neighbours, in spacings
+  const float* lip;             // 2 per shape, in spacings: largest |phi| difference of grid
+                                //   neighbours; largest gradient-norm bound of a grid cell
 };
 
 // Arithmetic form of the narrowphase and contact forces.
@@ -132,6 +133,14 @@ struct MaybeView {
   int* ctr;     // [0] node cursor, [1 + launch] pairs queued
 };
 
+// Precision form: flat lists of candidate pairs (A * cap + slot) per partner
+// kind, appended by the candidate searches, so that the screen gives one warp
+// to each pair rather than to each owner particle.
+struct PairLists {
+  int* list[3];  // particles, walls, images: n * cap entries each
+  int* ctr;      // [kind] entries appended this step (nullptr: lists not built)
+};
+
 struct StepArgs {
   BodyView P;       // particles
   BodyView W;       // walls
@@ -152,11 +161,18 @@ struct StepArgs {
   int precision;    // PREC_*
   double rmax;      // largest particle bounding radius
   MaybeView mb;
+  PairLists pl;
+  // precision form, optional: screen counters (pairs, clusters tested, after the
+  // bounding cull, after the SDF cull, node tests, nodes queued for FP64)
+  unsigned long long* screen_stats;
 };
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);
 void launch_candidates(const StepArgs& a, cudaStream_t s);
 void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s);
+// precision form: FP64 contact pass over the pairs queued by the screen of
+// launch li (0: particles and walls, 1: periodic images)
+void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s);
 void launch_kick(const StepArgs& a, cudaStream_t s);
 void launch_periodic(const StepArgs& a, int axes, cudaStream_t s);
 void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,

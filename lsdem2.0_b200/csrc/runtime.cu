@@ -314,6 +314,8 @@ struct lsdem_solver {
   DArr<float> s_lip;
   // precision form: screened nodes and queued pairs (per-step scratch)
   DArr<int> mb_node, mb_ctr;
+  DArr<int> plist[3], pl_ctr;
+  DArr<unsigned long long> scr_stats;  // screen counters (allocated while enabled)
   DArr<int4> mb_pair;
   long long mb_cap = 0, mb_pcap = 0;
   std::vector<int> h_node_off, h_cl_off;
@@ -354,8 +356,8 @@ struct lsdem_solver {
   bool profiling = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
   std::vector<cudaEvent_t> event_pool;
-  double prof_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  long long prof_calls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double prof_ms[LSDEM_NUM_PHASES] = {};
+  long long prof_calls[LSDEM_NUM_PHASES] = {};
 
   ~lsdem_solver() {
     if (h_status) cudaFreeHost(h_status);
@@ -488,6 +490,18 @@ void alloc_slots(lsdem_solver* s, bool keep_unchanged = false) {
       CK(sl.seg_cnt.alloc(m));
       CK(sl.seg_cnt.zero(s->stream));
     }
+  // precision form: flat pair lists, one entry per slot
+  for (int k = 0; k < 3; ++k) {
+    const int cap = s->slots[0][k].cap;
+    const size_t m = (size_t)std::max(n, 1) * std::max(cap, 1);
+    if (s->precision == PREC_FP64 || cap == 0) { s->plist[k].release(); continue; }
+    if ((long long)n * cap > 0x7fffffffLL) throw Fail{LSDEM_ERR_NOMEM, "pair list index exceeds 32 bits"};
+    if (s->plist[k].n != m) CK(s->plist[k].alloc(m));
+  }
+  if (s->precision != PREC_FP64 && !s->pl_ctr.p) {
+    CK(s->pl_ctr.alloc(4));
+    CK(s->pl_ctr.zero(s->stream));
+  }
 }
 
 void alloc_contacts(lsdem_solver* s, ContactsDev& c, long long cap) {
@@ -636,22 +650,31 @@ void initialize(lsdem_solver* s) {
     std::vector<float4> nf(node_pos.size());
     for (size_t i = 0; i < node_pos.size(); ++i)
       nf[i] = make_float4((float)node_pos[i].x, (float)node_pos[i].y, (float)node_pos[i].z, 0.f);
-    // per template: largest difference of neighbouring SDF values, in spacings
-    // (Lipschitz bound of the trilinear interpolant per grid unit and axis)
+    // per template, in spacings: the largest difference of neighbouring SDF values
+    // (bound of each partial derivative of the trilinear interpolant per grid
+    // unit) and the largest gradient-norm bound of a cell, sqrt of the sum over
+    // axes of the cell's largest edge difference squared
     std::vector<float> lip;
     for (const ShapeHost& sh : s->shapes) {
       const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
-      double m = 0.;
-      for (int z = 0; z < nz; ++z)
-        for (int y = 0; y < ny; ++y)
-          for (int x = 0; x < nx; ++x) {
-            const size_t i = (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z);
-            const double v = sh.sdf[i];
-            if (x + 1 < nx) m = std::max(m, std::fabs(sh.sdf[i + 1] - v));
-            if (y + 1 < ny) m = std::max(m, std::fabs(sh.sdf[i + nx] - v));
-            if (z + 1 < nz) m = std::max(m, std::fabs(sh.sdf[i + (size_t)nx * ny] - v));
+      const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+      auto at = [&](int x, int y, int z) { return sh.sdf[(size_t)x + sy * y + sz * z]; };
+      double m = 0., g = 0.;
+      for (int z = 0; z + 1 < nz; ++z)
+        for (int y = 0; y + 1 < ny; ++y)
+          for (int x = 0; x + 1 < nx; ++x) {
+            double e[3] = {0., 0., 0.};
+            for (int b = 0; b < 4; ++b) {
+              const int u = b & 1, v = b >> 1;
+              e[0] = std::max(e[0], std::fabs(at(x + 1, y + u, z + v) - at(x, y + u, z + v)));
+              e[1] = std::max(e[1], std::fabs(at(x + u, y + 1, z + v) - at(x + u, y, z + v)));
+              e[2] = std::max(e[2], std::fabs(at(x + u, y + v, z + 1) - at(x + u, y + v, z)));
+            }
+            m = std::max(m, std::max(e[0], std::max(e[1], e[2])));
+            g = std::max(g, std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]));
           }
       lip.push_back((float)(m / sh.h * (1.0 + 1e-6)));
+      lip.push_back((float)(g / sh.h * (1.0 + 1e-6)));
     }
     CK(s->s_sdf16.upload(sdf16.data(), sdf16.size(), st));
     CK(s->s_node_f.upload(nf.data(), nf.size(), st));
@@ -777,6 +800,9 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.mb.node = s->mb_node.p; a.mb.cap = (int)s->mb_cap;
   a.mb.pair = s->mb_pair.p; a.mb.pcap = (int)s->mb_pcap;
   a.mb.ctr = s->precision == PREC_FP64 ? nullptr : s->mb_ctr.p;
+  for (int k = 0; k < 3; ++k) a.pl.list[k] = s->plist[k].p;
+  a.pl.ctr = s->precision == PREC_FP64 ? nullptr : s->pl_ctr.p;
+  a.screen_stats = s->scr_stats.p;
   return a;
 }
 
@@ -840,6 +866,7 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
   }
   { PhaseTimer pt(s, 2); launch_candidates(a, st); }
   { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
+  if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 0, st); }
   if (s->nsets > 0) {
     {
       PhaseTimer pt(s, 4);
@@ -849,6 +876,7 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
       launch_ghost_candidates(a, s->g2_idx.p, s->g2_start.p, s->g2_end.p, s->key2.p, st);
     }
     { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
+    if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
   }
   if (!s->bonds.bonded.empty()) {
     PhaseTimer pt(s, 6);
@@ -1575,15 +1603,15 @@ void* lsdem_stream(const lsdem_solver* s) { return s ? (void*)s->stream : nullpt
 int lsdem_set_profiling(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   s->profiling = on != 0;
-  for (int k = 0; k < 8; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
+  for (int k = 0; k < LSDEM_NUM_PHASES; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
   return LSDEM_OK;
 }
 
-int lsdem_get_profile(const lsdem_solver* s, double* ms8, long long* calls8) {
+int lsdem_get_profile(const lsdem_solver* s, double* ms, long long* calls) {
   if (!s) return LSDEM_ERR_ARG;
-  for (int k = 0; k < 8; ++k) {
-    if (ms8) ms8[k] = s->prof_ms[k];
-    if (calls8) calls8[k] = s->prof_calls[k];
+  for (int k = 0; k < LSDEM_NUM_PHASES; ++k) {
+    if (ms) ms[k] = s->prof_ms[k];
+    if (calls) calls[k] = s->prof_calls[k];
   }
   return LSDEM_OK;
 }
@@ -1601,6 +1629,32 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4) {
       for (int v : c) pairs[k] += std::min(v, sl.cap);
     }
     out4[0] = pairs[0]; out4[1] = pairs[1]; out4[2] = pairs[2]; out4[3] = s->hist_count;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_set_screen_stats(lsdem_solver* s, int on) {
+  if (!s) return LSDEM_ERR_ARG;
+  return guard(s, [&] {
+    if (on) {
+      CK(s->scr_stats.alloc(6));
+      CK(s->scr_stats.zero(s->stream));
+    } else {
+      CK(cudaStreamSynchronize(s->stream));
+      s->scr_stats.release();
+    }
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_screen_stats(lsdem_solver* s, long long* out6) {
+  if (!s || !out6) return LSDEM_ERR_ARG;
+  return guard(s, [&] {
+    for (int k = 0; k < 6; ++k) out6[k] = 0;
+    if (!s->scr_stats.p) return LSDEM_OK;
+    auto c = dl(s->scr_stats, 6, s->stream);
+    CK(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 6; ++k) out6[k] = (long long)c[k];
     return LSDEM_OK;
   });
 }

@@ -58,6 +58,7 @@ __global__ void k_integrate_first(StepArgs a) {
     *a.C.count = 0;
     if (a.G.count) *a.G.count = 0;
     if (a.mb.ctr) a.mb.ctr[0] = a.mb.ctr[1] = a.mb.ctr[2] = 0;
+    if (a.pl.ctr) a.pl.ctr[0] = a.pl.ctr[1] = a.pl.ctr[2] = 0;
   }
   if (i < a.P.n) {
     const BodyView& P = a.P;
@@ -135,6 +136,22 @@ LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
 // node's 27-cell window since cells are at least 2 max radius wide).
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
+// Appends this lane's entries A * cap + j, j < cnt, to a flat pair list, with
+// one atomic per warp (all lanes of the warp call it).
+LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
+  const int lane = threadIdx.x & 31;
+  int incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int tot = __shfl_sync(FULL, incl, 31);
+  int base = 0;
+  if (lane == 31 && tot > 0) base = atomicAdd(ctr, tot);
+  base = __shfl_sync(FULL, base, 31) + incl - cnt;
+  for (int j = 0; j < cnt; ++j) list[base + j] = A * cap + j;
+}
+
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
 // mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
 // and their occupant loads are broadcasts. Slots are filled in cell-walk then
@@ -190,6 +207,11 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     }
     if (capw > 0) a.pw.cnt[A] = nw < capw ? nw : capw;
     if (nw > capw) atomicOr(&a.status->flags, OVF_WALL);
+  }
+  if (a.pl.ctr) {  // precision form: flat pair lists
+    const int A = t < a.P.n ? a.cell_idx[t] : 0;
+    append_pairs(a.pl.list[0], &a.pl.ctr[0], A, a.pp.cap, t < a.P.n ? min(n, a.pp.cap) : 0);
+    if (a.pw.cap > 0) append_pairs(a.pl.list[1], &a.pl.ctr[1], A, a.pw.cap, t < a.P.n ? min(nw, a.pw.cap) : 0);
   }
   // largest demand of the warp, one atomic per warp
   n = __reduce_max_sync(FULL, n);
@@ -680,6 +702,7 @@ struct PartnerF {
   float n1o;    // |o|_1
   float invh, h;
   float lip;    // largest neighbour difference of the template's phi / h
+  float gmax;   // largest gradient-norm bound of a cell of the template's phi / h
   int3 gs;
   const unsigned short* sdf;
   int key;
@@ -696,7 +719,8 @@ LD PartnerF partner_f(const StepArgs& a, const Partner& P, const SelfF& S, int s
   F.n1o = n1f(F.o);
   F.invh = (float)P.invh;
   F.h = (float)(1.0 / P.invh);
-  F.lip = a.S.lip[shape];
+  F.lip = a.S.lip[2 * shape];
+  F.gmax = a.S.lip[2 * shape + 1];
   F.gs = P.gs;
   F.sdf = a.S.sdf16 + (P.sdf - a.S.sdf);
   F.key = P.key;
@@ -720,24 +744,11 @@ LD int window_state(const StepArgs& a, double3 x, float3 ra, float n1ra, int key
   return in_window(key, g, c, lo, hi) ? 1 : 0;
 }
 
-// False only when node_hits certainly rejects the node.
-template <int KIND, int SDFK>
-LD bool node_may_hit_f(const StepArgs& a, const SelfF& S, const PartnerF& P, float3 ra, float3 r) {
-  const float n1ra = n1f(ra);
-  const float el = EPS_F * (n1ra + P.n1d);
-  if (KIND == KIND_PP) {
-    const float R = P.r * (1.0f + 1e-6f) + el;
-    if (dotf(r, r) > R * R) return false;
-  } else {
-    if (window_state<KIND>(a, S.x, ra, n1ra, P.key) == 0) return false;
-  }
-  const float3 l = rotinvf(r, P.q);
-  const float gx = (l.x - P.o.x) * P.invh, gy = (l.y - P.o.y) * P.invh, gz = (l.z - P.o.z) * P.invh;
-  const float eg = P.invh * EPS_F * (n1ra + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
-  // the FP64 test rejects g < 0 or g >= size - 1 on any axis
-  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
-  if (gx < -eg || gy < -eg || gz < -eg || gx >= ux + eg || gy >= uy + eg || gz >= uz + eg) return false;
-  if (gx < eg || gy < eg || gz < eg || gx >= ux - eg || gy >= uy - eg || gz >= uz - eg) return true;
+// phi / h of the 16-bit store at grid point (gx, gy, gz), known to lie inside
+// the grid by at least eg on every axis, minus the bound on its difference from
+// the FP64 value at the FP64 point: > 0 proves phi > 0 there.
+template <int SDFK>
+LD float phi16_lower(const PartnerF& P, float gx, float gy, float gz, float eg) {
   const int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
   const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
   const int sy = P.gs.x, sz = P.gs.x * P.gs.y;
@@ -752,7 +763,66 @@ LD bool node_may_hit_f(const StepArgs& a, const SelfF& S, const PartnerF& P, flo
   const float cmax = fmaxf(fmaxf(fmaxf(fabsf(c0), fabsf(c1)), fmaxf(fabsf(c2), fabsf(c3))),
                            fmaxf(fmaxf(fabsf(c4), fabsf(c5)), fmaxf(fabsf(c6), fabsf(c7))));
   const float band = cmax * (quant16<SDFK>() + 4e-6f) + 3.0f * P.lip * eg + 1e-7f;
-  return !(phi > band);  // NaN / Inf corners are never rejected
+  return phi - band;  // NaN for NaN / Inf corners: never > 0
+}
+
+// Grid point of a partner-relative position r (offset ra from the owner's
+// centre) and its error bound eg; 0 = certainly outside the grid (the FP64 test
+// rejects), 1 = certainly inside by eg, 2 = within eg of the grid boundary.
+LD int grid_point_f(const PartnerF& P, float3 r, float n1ra, float& gx, float& gy, float& gz, float& eg) {
+  const float3 l = rotinvf(r, P.q);
+  gx = (l.x - P.o.x) * P.invh;
+  gy = (l.y - P.o.y) * P.invh;
+  gz = (l.z - P.o.z) * P.invh;
+  eg = P.invh * EPS_F * (n1ra + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
+  // the FP64 test rejects g < 0 or g >= size - 1 on any axis
+  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
+  if (gx < -eg || gy < -eg || gz < -eg || gx >= ux + eg || gy >= uy + eg || gz >= uz + eg) return 0;
+  if (gx < eg || gy < eg || gz < eg || gx >= ux - eg || gy >= uy - eg || gz >= uz - eg) return 2;
+  return 1;
+}
+
+// False only when node_hits certainly rejects the node.
+template <int KIND, int SDFK>
+LD bool node_may_hit_f(const StepArgs& a, const SelfF& S, const PartnerF& P, float3 ra, float3 r) {
+  const float n1ra = n1f(ra);
+  const float el = EPS_F * (n1ra + P.n1d);
+  if (KIND == KIND_PP) {
+    const float R = P.r * (1.0f + 1e-6f) + el;
+    if (dotf(r, r) > R * R) return false;
+  } else {
+    if (window_state<KIND>(a, S.x, ra, n1ra, P.key) == 0) return false;
+  }
+  float gx, gy, gz, eg;
+  const int in = grid_point_f(P, r, n1ra, gx, gy, gz, eg);
+  if (in != 1) return in == 2;
+  return !(phi16_lower<SDFK>(P, gx, gy, gz, eg) > 0.f);
+}
+
+// Second cluster cull, against the partner's grid and SDF. Nodes outside the
+// grid box [0, size - 1] (grid units) are rejected by the FP64 test, so a cluster
+// sphere wholly outside the box is culled. Otherwise phi / h is evaluated at q,
+// the centre projected into the box shrunk by m >= eg: for a node p inside the
+// box, |p - q| <= |p - c| + sqrt(3) m (projection onto a convex set does not
+// expand distances), the segment p-q lies in the box, and along it phi / h
+// changes by at most gmax per grid unit, so phi(q) - gmax (rad + sqrt(3) m) > 0
+// proves phi > 0 at every node of the cluster.
+template <int SDFK>
+LD bool cluster_sdf_may_hit_f(float3 cA, float rad, const PartnerF& P) {
+  const float3 l = rotinvf(cA + P.d, P.q);
+  const float gx = (l.x - P.o.x) * P.invh, gy = (l.y - P.o.y) * P.invh, gz = (l.z - P.o.z) * P.invh;
+  const float eg = P.invh * EPS_F * (n1f(cA) + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
+  const float radh = rad * P.invh * (1.0f + 1e-6f);
+  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
+  const float dx = fmaxf(fmaxf(-gx, gx - ux), 0.f), dy = fmaxf(fmaxf(-gy, gy - uy), 0.f),
+              dz = fmaxf(fmaxf(-gz, gz - uz), 0.f);
+  const float R = (radh + eg) * (1.0f + 1e-6f);
+  if (dx * dx + dy * dy + dz * dz > R * R) return false;
+  const float m = fmaxf(eg, 1e-3f);  // > 0: q stays below size - 1, so its cell is in the grid
+  if (ux < 4.f * m || uy < 4.f * m || uz < 4.f * m) return true;
+  const float qx = fminf(fmaxf(gx, m), ux - m), qy = fminf(fmaxf(gy, m), uy - m), qz = fminf(fmaxf(gz, m), uz - m);
+  const float reach = P.gmax * (radh + 2.8f * m) + 1e-6f;
+  return !(phi16_lower<SDFK>(P, qx, qy, qz, eg) > reach);
 }
 
 // Conservative cluster cull in FP32 (the bounds of node_may_hit_f applied to the
@@ -797,7 +867,7 @@ LD int partner_shape(const StepArgs& a, int pid) {
 // nodes gets its empty contact segment here.
 template <int KIND, int SDFK>
 LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const SelfF& S, int* s_cl,
-                      unsigned* s_mask) {
+                      unsigned* s_mask, unsigned (&cnt)[6]) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
   PartnerF P;
@@ -819,9 +889,29 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const
     nsurv += __popc(m);
   }
   __syncwarp();
+  // second cull on the survivors, compacted in place (writes never pass reads)
+  int nsurv2 = 0;
+  for (int k0 = 0; k0 < nsurv; k0 += 32) {
+    const int k = k0 + lane;
+    bool keep = false;
+    int c = 0;
+    if (k < nsurv) {
+      c = s_cl[k];
+      const double4 sp = a.S.cl_sphere[S.cl0 + c];
+      const float3 cA = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc);
+      keep = cluster_sdf_may_hit_f<SDFK>(cA, (float)sp.w * S.sc, P);
+    }
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) s_cl[nsurv2 + __popc(m & lanemask_lt())] = c;
+    nsurv2 += __popc(m);
+  }
+  cnt[0] += 1; cnt[1] += S.ncl; cnt[2] += nsurv; cnt[3] += nsurv2;
+  nsurv = nsurv2;
+  __syncwarp();
   int total = 0;
   for (int k = 0; k < nsurv; ++k) {
     const int ni = s_cl[k] * 32 + lane;
+    cnt[4] += min(32, S.nn - s_cl[k] * 32);
     bool may = false;
     if (ni < S.nn) {
       const float4 nd = a.S.node_pos_f[S.n0 + ni];
@@ -832,6 +922,7 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const
     if (lane == 0) s_mask[k] = m;
     total += __popc(m);
   }
+  cnt[5] += total;
   __syncwarp();
   const SlotView& cur = slots_of<KIND>(a, false);
   const size_t sidx = (size_t)A * cur.cap + slot;
@@ -869,34 +960,50 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const
   }
 }
 
+LD SelfF self_f(const StepArgs& a, int A) {
+  SelfF S;
+  S.x = a.P.pos[A];
+  S.q = toq(a.P.quat[A]);
+  S.sc = (float)a.P.scale[A];
+  const int sh = a.P.shape[A];
+  S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
+  S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
+  return S;
+}
+
+// One warp per listed pair: the flat pair lists of the kinds in KINDS, in
+// particle, wall, image order.
 template <int KINDS, int SDFK>
 __global__ void __launch_bounds__(NP_WARPS * 32, 4) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int ng_max = 0;
-  for (int A = blockIdx.x * NP_WARPS + warp; A < a.P.n; A += gridDim.x * NP_WARPS) {
-    const int npp = (KINDS & 1) ? a.pp.cnt[A] : 0;
-    const int nw = (KINDS & 2) ? (a.pw.cap > 0 ? a.pw.cnt[A] : 0) : 0;
-    const int ng = (KINDS & 4) ? a.pgh.cnt[A] : 0;
-    ng_max = ng > ng_max ? ng : ng_max;
-    const int ngc = ng < a.pgh.cap ? ng : a.pgh.cap;
-    if (npp + nw + ngc == 0) continue;
-    SelfF S;
-    S.x = a.P.pos[A];
-    S.q = toq(a.P.quat[A]);
-    S.sc = (float)a.P.scale[A];
-    const int sh = a.P.shape[A];
-    S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
-    S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
-    for (int j = 0; j < npp; ++j)
-      screen_pair_f<KIND_PP, SDFK>(a, A, j, a.pp.id[(size_t)A * a.pp.cap + j], li, S, s_cl[warp], s_mask[warp]);
-    for (int j = 0; j < nw; ++j)
-      screen_pair_f<KIND_WALL, SDFK>(a, A, j, a.pw.id[(size_t)A * a.pw.cap + j], li, S, s_cl[warp], s_mask[warp]);
-    for (int j = 0; j < ngc; ++j)
-      screen_pair_f<KIND_GHOST, SDFK>(a, A, j, a.pgh.id[(size_t)A * a.pgh.cap + j], li, S, s_cl[warp], s_mask[warp]);
+  const int warp = threadIdx.x >> 5;
+  const int n0 = (KINDS & 1) ? min(a.pl.ctr[0], a.P.n * a.pp.cap) : 0;
+  const int n1 = (KINDS & 2) && a.pw.cap > 0 ? min(a.pl.ctr[1], a.P.n * a.pw.cap) : 0;
+  const int n2 = (KINDS & 4) ? min(a.pl.ctr[2], a.P.n * a.pgh.cap) : 0;
+  const int tot = n0 + n1 + n2;
+  unsigned cnt[6] = {0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
+  for (int e = blockIdx.x * NP_WARPS + warp; e < tot; e += gridDim.x * NP_WARPS) {
+    if ((KINDS & 1) && e < n0) {
+      const int idx = a.pl.list[0][e];
+      const int A = idx / a.pp.cap;
+      screen_pair_f<KIND_PP, SDFK>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, self_f(a, A), s_cl[warp],
+                                   s_mask[warp], cnt);
+    } else if ((KINDS & 2) && e < n0 + n1) {
+      const int idx = a.pl.list[1][e - n0];
+      const int A = idx / a.pw.cap;
+      screen_pair_f<KIND_WALL, SDFK>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, self_f(a, A), s_cl[warp],
+                                     s_mask[warp], cnt);
+    } else if (KINDS & 4) {
+      const int idx = a.pl.list[2][e - n0 - n1];
+      const int A = idx / a.pgh.cap;
+      screen_pair_f<KIND_GHOST, SDFK>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, self_f(a, A), s_cl[warp],
+                                      s_mask[warp], cnt);
+    }
   }
-  if ((KINDS & 4) && lane == 0 && ng_max > 0) atomicMax(&a.status->need_ghost, ng_max);
+  if (a.screen_stats && (threadIdx.x & 31) == 0)
+    for (int k = 0; k < 6; ++k)
+      if (cnt[k]) atomicAdd(&a.screen_stats[k], (unsigned long long)cnt[k]);
 }
 
 // Queued pairs of the screen, one warp each, in FP64: the reference's node test
@@ -968,7 +1075,8 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
     else k_narrowphase<7><<<g, b, 0, s>>>(a);
     return;
   }
-  // precision form: screen, then the FP64 contact pass over the queued pairs
+  // precision form: the screen over the flat pair lists (launch_contact_pass
+  // follows it); the grid is sized for the device, the list length is on it
   const int li = kinds == 4 ? 1 : 0;
   if (a.precision == PREC_FP32_FP16) {
     if (kinds == 3) k_screen_f<3, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
@@ -981,6 +1089,10 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
     else if (kinds == 4) k_screen_f<4, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
     else k_screen_f<7, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
   }
+}
+
+void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s) {
+  if (a.P.n <= 0 || a.precision == PREC_FP64) return;
   k_contacts_f<<<num_sms() * 4, NP_WARPS * 32, 0, s>>>(a, li);
 }
 
@@ -1087,6 +1199,7 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
   const int nvis = *a.G.count;
   const int n = a.P.n;
   const GridP& g = a.pg;
+  int need = 0;  // largest per-particle image count seen by this lane
   for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nvis; v += (gridDim.x * blockDim.x) >> 5) {
     const int t = a.G.list[v];
     const int s = t / n, i = t % n;
@@ -1114,19 +1227,35 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
           const int st = g2_start[h];
           if (st < 0) continue;
           const int en = g2_end[h];
-          for (int k = st + lane; k < en; k += 32) {
-            const int A = g2_idx[k];
-            const double3 xA = a.P.pos[A];
-            const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
-            if (len2(xA - xg) > R * R) continue;
-            const int slot = atomicAdd(&a.pgh.cnt[A], 1);
-            if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
-            else atomicOr(&a.status->flags, OVF_GHOST);
+          for (int k0 = st; k0 < en; k0 += 32) {
+            const int k = k0 + lane;
+            int slot = -1, A = 0;
+            if (k < en) {
+              A = g2_idx[k];
+              const double3 xA = a.P.pos[A];
+              const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
+              if (!(len2(xA - xg) > R * R)) {
+                slot = atomicAdd(&a.pgh.cnt[A], 1);
+                if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
+                else atomicOr(&a.status->flags, OVF_GHOST);
+              }
+            }
+            need = max(need, slot + 1);
+            if (a.pl.ctr) {  // precision form: flat pair list
+              const bool ok = slot >= 0 && slot < a.pgh.cap;
+              const unsigned m = __ballot_sync(FULL, ok);
+              int base = 0;
+              if (lane == 0 && m) base = atomicAdd(&a.pl.ctr[2], __popc(m));
+              base = __shfl_sync(FULL, base, 0);
+              if (ok) a.pl.list[2][base + __popc(m & lanemask_lt())] = A * a.pgh.cap + slot;
+            }
           }
         }
       }
     }
   }
+  need = __reduce_max_sync(FULL, need);
+  if (lane == 0 && need > 0) atomicMax(&a.status->need_ghost, need);
 }
 
 void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,
