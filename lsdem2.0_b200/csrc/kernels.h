@@ -40,6 +40,8 @@ struct ShapeView {
   const double3* node_pos;    // node store, cluster order, unscaled
   const int* node_orig;       // original node index within the shape
   const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
+  const double* node_box;     // 8 per shape (unscaled): node bounding box lo xyz, hi xyz,
+                              //   largest node distance from the body origin, 0
   // precision form: SDF values / template spacing in 16-bit floats, FP32 nodes
   const unsigned short* sdf16;  // same offsets as sdf; FP16 or BF16 bits
   const float4* node_pos_f;     // FP32 copy of node_pos
@@ -72,6 +74,8 @@ struct BodyView {
   const double* invh;        // inverse grid spacing (scaled)
   const long long* node_base;  // global id of the first surface node (particles)
   int* key;                  // cell key of this step, -1 outside the domain
+  float4* rotm;              // precision form, particles: rows of the FP32 rotation matrix
+                             //   of quat (3 per body, written by k_integrate_first)
 };
 
 // Per-particle candidate slots of one partner kind, with the contact segment

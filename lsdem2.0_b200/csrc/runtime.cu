@@ -259,6 +259,7 @@ struct BodyHost {
 struct BodyDev {
   DArr<double3> pos, vel, angvel, force, torque, origin;
   DArr<Quat> quat;
+  DArr<float4> rotm;  // precision form, particles: FP32 rotation matrix rows (written each step)
   DArr<double> invm, radius, kn, ks, mu, res, scale, invh;
   DArr<Sym6> invI;
   DArr<int> shape, key;
@@ -309,6 +310,7 @@ struct lsdem_solver {
   DArr<int> s_node_off, s_node_cnt, s_cl_off, s_cl_cnt, s_node_orig;
   DArr<double3> s_node_pos;
   DArr<double4> s_cl;
+  DArr<double> s_nbox;  // per shape: node bounding box (lo xyz, hi xyz), largest node distance, 0
   DArr<unsigned short> s_sdf16;
   DArr<float4> s_node_f;
   DArr<float> s_lip;
@@ -560,6 +562,8 @@ void upload_bodies(lsdem_solver* s, BodyHost& H, BodyDev& D) {
   CK(D.shape.upload(H.shape.data(), n, st));
   CK(D.key.alloc(std::max<size_t>(n, 1)));
   if (!H.node_base.empty()) CK(D.node_base.upload(H.node_base.data(), n, st));
+  if (&D == &s->dP && s->precision != PREC_FP64) CK(D.rotm.alloc(3 * std::max<size_t>(n, 1)));
+  else D.rotm.release();
 }
 
 void set_grid(GridP& g, const double* mn, const double* mx_in, double cell) {  // spatialGrid::set
@@ -632,6 +636,22 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_pos.upload(node_pos.data(), node_pos.size(), st));
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
+  {
+    std::vector<double> nbox;
+    for (const ShapeHost& sh : s->shapes) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, r2 = 0.;
+      for (size_t i = 0; i + 2 < sh.nodes.size(); i += 3) {
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = std::min(lo[k], sh.nodes[i + k]);
+          hi[k] = std::max(hi[k], sh.nodes[i + k]);
+        }
+        r2 = std::max(r2, sh.nodes[i] * sh.nodes[i] + sh.nodes[i + 1] * sh.nodes[i + 1] + sh.nodes[i + 2] * sh.nodes[i + 2]);
+      }
+      if (sh.nodes.empty()) for (int k = 0; k < 3; ++k) lo[k] = hi[k] = 0.;
+      nbox.insert(nbox.end(), {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], std::sqrt(r2) * (1.0 + 1e-12), 0.});
+    }
+    CK(s->s_nbox.upload(nbox.data(), nbox.size(), st));
+  }
   if (s->precision != PREC_FP64) {
     // precision form: phi / h of each template in 16 bits, FP32 node copy
     std::vector<unsigned short> sdf16(sdf.size());
@@ -753,6 +773,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
     v.quat = D.quat.p; v.invmass = D.invm.p; v.invI = D.invI.p; v.radius = D.radius.p; v.kn = D.kn.p;
     v.ks = D.ks.p; v.mu = D.mu.p; v.res = D.res.p; v.shape = D.shape.p; v.scale = D.scale.p;
     v.origin = D.origin.p; v.invh = D.invh.p; v.node_base = D.node_base.p; v.key = D.key.p;
+    v.rotm = D.rotm.p;
     return v;
   };
   a.P = bv(s->dP, s->P.n());
@@ -761,6 +782,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.node_off = s->s_node_off.p; a.S.node_cnt = s->s_node_cnt.p; a.S.cl_off = s->s_cl_off.p;
   a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
   a.S.cl_sphere = s->s_cl.p;
+  a.S.node_box = s->s_nbox.p;
   a.S.sdf16 = s->s_sdf16.p;
   a.S.node_pos_f = s->s_node_f.p;
   a.S.lip = s->s_lip.p;

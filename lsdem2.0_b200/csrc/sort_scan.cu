@@ -176,32 +176,38 @@ __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells
 // (insertion sort for small buckets, deferred to k_bucket_big otherwise) and
 // write the cell range [start, end) of cell b - 1, -1 when empty
 // (findStartAndEnd, buildHashStartEnd.cu:47-67).
+// Cell ranges of every bucket, and the stable order inside each bucket (the
+// scatter leaves members in arbitrary order): one warp per bucket, members of
+// buckets up to 64 long are ranked by particle index in registers; longer
+// buckets go to k_bucket_big.
 __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int ncells, int* __restrict__ sorted_idx,
                              int* __restrict__ start, int* __restrict__ end, int* __restrict__ big_list,
                              int* __restrict__ big_count) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbuckets) return;
-  const int s = offs[b], e = offs[b + 1], L = e - s;
-  if (b > 0 && b <= ncells) {
-    start[b - 1] = L > 0 ? s : -1;
-    end[b - 1] = L > 0 ? e : -1;
-  }
-  if (L <= 1 || b == 0 || b == ncells + 1) return;  // special buckets are already in index order
-  if (L > 64) {
-    int slot = atomicAdd(big_count, 1);
-    big_list[slot] = b;
-    return;
-  }
-  for (int p = s + 1; p < e; ++p) {
-    int v = sorted_idx[p];
-    int q = p - 1;
-    while (q >= s && sorted_idx[q] > v) { sorted_idx[q + 1] = sorted_idx[q]; --q; }
-    sorted_idx[q + 1] = v;
+  const int lane = threadIdx.x & 31;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbuckets; b += (gridDim.x * blockDim.x) >> 5) {
+    const int s = offs[b], e = offs[b + 1], L = e - s;
+    if (lane == 0 && b > 0 && b <= ncells) {
+      start[b - 1] = L > 0 ? s : -1;
+      end[b - 1] = L > 0 ? e : -1;
+    }
+    if (L <= 1 || b == 0 || b == ncells + 1) continue;  // special buckets are already in index order
+    if (L > 64) {
+      if (lane == 0) big_list[atomicAdd(big_count, 1)] = b;
+      continue;
+    }
+    const int v0 = lane < L ? sorted_idx[s + lane] : 0x7fffffff;
+    const int v1 = lane + 32 < L ? sorted_idx[s + 32 + lane] : 0x7fffffff;
+    int r0 = 0, r1 = 0;
+    for (int j = 0; j < 32; ++j) {
+      const int u0 = __shfl_sync(0xffffffffu, v0, j), u1 = __shfl_sync(0xffffffffu, v1, j);
+      r0 += (u0 < v0) + (u1 < v0);
+      r1 += (u0 < v1) + (u1 < v1);
+    }
+    __syncwarp();
+    if (lane < L) sorted_idx[s + r0] = v0;
+    if (lane + 32 < L) sorted_idx[s + r1] = v1;
   }
 }
-
-// One block per large bucket: rank each member by the number of smaller
-// particle indices in the bucket (indices are unique, so ranks are a permutation).
 __global__ void k_bucket_big(const int* __restrict__ offs, const int* __restrict__ big_list,
                              const int* __restrict__ big_count, int* __restrict__ sorted_idx, int* __restrict__ tmp) {
   if ((int)blockIdx.x >= *big_count) return;
@@ -236,7 +242,8 @@ void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorte
     k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx);
     k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx);
   }
-  k_bucket_fix<<<(nb + 255) / 256, 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list, w.big_count);
+  k_bucket_fix<<<(unsigned)((nb + 7) / 8), 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list,
+                                                        w.big_count);
   // at most n / 65 buckets can exceed 64 members
   int max_big = n / 65 + 1;
   k_bucket_big<<<max_big, 256, 0, s>>>(w.offs, w.big_list, w.big_count, sorted_idx, w.tmp);

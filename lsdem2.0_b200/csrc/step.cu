@@ -77,6 +77,12 @@ __global__ void k_integrate_first(StepArgs a) {
     q = quat_integrate(q, w, a.dt);
     P.pos[i] = x;
     P.quat[i] = q;
+    if (P.rotm) {  // precision form: FP32 rotation matrix (columns are rotate(q, e_j))
+      const double3 c0 = rotate(q, d3(1., 0., 0.)), c1 = rotate(q, d3(0., 1., 0.)), c2 = rotate(q, d3(0., 0., 1.));
+      P.rotm[3 * i] = make_float4((float)c0.x, (float)c1.x, (float)c2.x, 0.f);
+      P.rotm[3 * i + 1] = make_float4((float)c0.y, (float)c1.y, (float)c2.y, 0.f);
+      P.rotm[3 * i + 2] = make_float4((float)c0.z, (float)c1.z, (float)c2.z, 0.f);
+    }
     P.force[i] = d3(0., 0., 0.);
     P.torque[i] = d3(0., 0., 0.);
     P.key[i] = hash_key(x, a.pg);
@@ -130,12 +136,6 @@ LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi
   hi = d3(o.x + (gs.x - 1) / invh, o.y + (gs.y - 1) / invh, o.z + (gs.z - 1) / invh);
 }
 
-// Candidate partners of each particle A.
-// Particle partners: B > A, visible (in a cell), bounding spheres within
-// reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
-// reference's |node - xB| <= rB test, which in turn implies B lies in the
-// node's 27-cell window since cells are at least 2 max radius wide).
-// Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
 // Appends this lane's entries A * cap + j, j < cnt, to a flat pair list, with
 // one atomic per warp (all lanes of the warp call it).
 LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
@@ -152,6 +152,12 @@ LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
   for (int j = 0; j < cnt; ++j) list[base + j] = A * cap + j;
 }
 
+// Candidate partners of each particle A.
+// Particle partners: B > A, visible (in a cell), bounding spheres within
+// reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
+// reference's |node - xB| <= rB test, which in turn implies B lies in the
+// node's 27-cell window since cells are at least 2 max radius wide).
+// Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
 // mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
 // and their occupant loads are broadcasts. Slots are filled in cell-walk then
@@ -210,7 +216,7 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
   }
   if (a.pl.ctr) {  // precision form: flat pair lists
     const int A = t < a.P.n ? a.cell_idx[t] : 0;
-    append_pairs(a.pl.list[0], &a.pl.ctr[0], A, a.pp.cap, t < a.P.n ? min(n, a.pp.cap) : 0);
+    append_pairs(a.pl.list[0], &a.pl.ctr[0], A, a.pp.cap, t < a.P.n ? a.pp.cnt[A] : 0);
     if (a.pw.cap > 0) append_pairs(a.pl.list[1], &a.pl.ctr[1], A, a.pw.cap, t < a.P.n ? min(nw, a.pw.cap) : 0);
   }
   // largest demand of the warp, one atomic per warp
@@ -642,38 +648,31 @@ __global__ void __launch_bounds__(NP_WARPS * 32, 2) k_narrowphase(StepArgs a) {
 // the FP64 form; the 16-bit store and FP32 arithmetic only make the rejections
 // cheaper.
 //
+// Per pair, the owner's node offsets n (template units) map to the partner's
+// frame by l = M n + dB, M = R_B^T R_A scale_A, dB = R_B^T (xA - xB), and to its
+// grid by g = l invh + cg, cg = -origin invh. M and dB are formed in FP32 from the
+// step's FP32 rotation matrices (each entry rounded once from FP64) and from
+// xA - xB rounded from FP64.
+//
 // Error bounds (unit roundoff u = 2^-24; |.|_1 norms bound the Euclidean ones):
-// a node offset ra = q_A (x) node * scale and the partner-relative position
-// r = ra + d, d = xA - xB rounded from FP64, carry at most ~20u |ra|_1 + 2u |d|_1
-// rounding each; the rotation into the partner frame and the grid transform
-// add ~20u |r|_1 + u |o|_1 + 2u |g|_1. EPS_F = 1.6e-5 (~270u) bounds all of it
-// with a wide margin. The interpolated phi / h of the 16-bit store differs from
-// the FP64 value at the same grid point by at most Q max|c| (Q = 2^-11 for FP16,
-// 2^-8 for BF16, round to nearest, plus the FP32 rounding of phi / h), and a
-// grid-point error eg moves the piecewise-trilinear phi / h by at most
-// 3 L eg, L = the largest difference between neighbouring SDF values of the
-// partner's template in spacings.
+// l carries at most ~10u (N1 + |d|_1) of rounding, N1 = sqrt(3) x the largest
+// node distance x scale_A, and g adds u |g|_1 + invh u |origin|_1; EPS_F = 1.6e-5
+// (~270u) bounds all of it with a wide margin: el = EPS_F (N1 + 2 |d|_1) in
+// length, eg = invh (el + EPS_F |origin|_1) + EPS_F (sizes summed) in grid units
+// per axis. The 16-bit corners c differ from the FP64 values v by at most
+// Q |v| (Q = 2^-11 for FP16, 2^-8 for BF16, round to nearest, plus the FP32
+// rounding of phi / h and of the interpolation); an error eg in the grid point
+// moves the piecewise-trilinear phi / h by at most 3 L eg, L = the largest
+// difference of neighbouring grid values of the partner's template in spacings;
+// and every corner of the cell lies within 3 L of the interpolated value. So
+// with Q' = Q / (1 - Q), the FP64 phi at the FP64 point is positive whenever the
+// interpolated 16-bit value exceeds
+//   T = (3 L Q' + 3 L eg + 1e-7) / (1 - Q'),
+// a constant of the pair: a node is rejected by one comparison.
 LD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
 LD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
-LD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
-LD float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
-LD float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-LD float3 crossf(float3 a, float3 b) { return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-LD float n1f(float3 v) { return fabsf(v.x) + fabsf(v.y) + fabsf(v.z); }
 LD float3 tof(double3 v) { return f3((float)v.x, (float)v.y, (float)v.z); }
 LD double3 tod(float3 v) { return d3(v.x, v.y, v.z); }
-LD float4 toq(Quat q) { return make_float4((float)q.q0, (float)q.q1, (float)q.q2, (float)q.q3); }
-// rotation by q = (x: scalar, y, z, w: vector part) and by its conjugate
-LD float3 rotf(float4 q, float3 v) {
-  const float3 qv = f3(q.y, q.z, q.w);
-  const float3 t = crossf(qv, v) * 2.0f;
-  return v + t * q.x + crossf(qv, t);
-}
-LD float3 rotinvf(float3 v, float4 q) {
-  const float3 qv = f3(-q.y, -q.z, -q.w);
-  const float3 t = crossf(qv, v) * 2.0f;
-  return v + t * q.x + crossf(qv, t);
-}
 
 static constexpr float EPS_F = 1.6e-5f;
 
@@ -682,59 +681,133 @@ LD float decode16(unsigned short b) {
   if (SDFK == PREC_FP32_BF16) return __uint_as_float(((unsigned)b) << 16);
   return __half2float(__ushort_as_half(b));
 }
-// relative quantisation bound of the 16-bit store (with margin)
+// relative bound of the 16-bit store and FP32 interpolation error (with margin)
 template <int SDFK>
-LD constexpr float quant16() { return SDFK == PREC_FP32_BF16 ? 3.95e-3f : 4.95e-4f; }
+LD constexpr float quant16() { return SDFK == PREC_FP32_BF16 ? 3.95e-3f + 1e-6f : 4.95e-4f + 1e-6f; }
 
-struct SelfF {
-  double3 x;   // FP64 centre (cell-window tests of walls and images)
-  float4 q;
-  float sc;
-  int n0, nn, cl0, ncl;
-};
-
-struct PartnerF {
-  float3 d;     // xA - x(partner)
-  float n1d;    // |d|_1
-  float4 q;
-  float r;
-  float3 o;
-  float n1o;    // |o|_1
-  float invh, h;
-  float lip;    // largest neighbour difference of the template's phi / h
-  float gmax;   // largest gradient-norm bound of a cell of the template's phi / h
-  int3 gs;
+// Constants of one screened pair.
+struct PairF {
+  float M[9];        // R_B^T R_A scale_A, row-major
+  float3 dB;         // R_B^T (xA - xB)
+  float3 cg;         // -origin invh
+  float invh;
+  float ux, uy, uz;  // grid size - 1 per axis
+  float R2;          // particle partners: admission radius (with margin), squared
+  float rB;          // particle partners: bounding radius
+  float el;          // position error bound in the partner frame (length)
+  float eg;          // grid-point error bound per axis (grid units)
+  float T;           // rejection threshold of phi / h
+  float Tq;          // 1 / (1 - Q')
+  float gmax;        // gradient-norm bound of phi / h per grid unit
+  int sy, sz;
   const unsigned short* sdf;
-  int key;
+  int key;           // walls and images: the partner's cell key
+  float RA[9];       // walls and images: R_A scale_A (world offsets of the nodes)
+  float n1w;         // walls and images: error bound of the world node offset
 };
 
-template <int KIND>
-LD PartnerF partner_f(const StepArgs& a, const Partner& P, const SelfF& S, int shape) {
-  PartnerF F;
-  F.d = tof(S.x - P.x);
-  F.n1d = n1f(F.d);
-  F.q = toq(P.q);
-  F.r = (float)P.r;
-  F.o = tof(P.o);
-  F.n1o = n1f(F.o);
+// Rotation matrix columns of q (the images of the unit axes under rotate()).
+LD void rot_cols(Quat q, double3 c[3]) {
+  c[0] = rotate(q, d3(1., 0., 0.));
+  c[1] = rotate(q, d3(0., 1., 0.));
+  c[2] = rotate(q, d3(0., 0., 1.));
+}
+
+template <int KIND, int SDFK>
+LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int pidx) {
+  PairF F;
+  // rows of R_A (FP32, from the step's matrices) and of R_B (particles likewise;
+  // walls from their quaternion)
+  float ra[9], rb[9];
+  {
+    const float4 r0 = a.P.rotm[3 * A], r1 = a.P.rotm[3 * A + 1], r2 = a.P.rotm[3 * A + 2];
+    ra[0] = r0.x; ra[1] = r0.y; ra[2] = r0.z; ra[3] = r1.x; ra[4] = r1.y; ra[5] = r1.z;
+    ra[6] = r2.x; ra[7] = r2.y; ra[8] = r2.z;
+  }
+  if (KIND == KIND_WALL) {
+    double3 cb[3];
+    rot_cols(P.q, cb);
+    for (int j = 0; j < 3; ++j) {
+      rb[j] = (float)cb[j].x; rb[3 + j] = (float)cb[j].y; rb[6 + j] = (float)cb[j].z;
+    }
+  } else {
+    const float4 r0 = a.P.rotm[3 * pidx], r1 = a.P.rotm[3 * pidx + 1], r2 = a.P.rotm[3 * pidx + 2];
+    rb[0] = r0.x; rb[1] = r0.y; rb[2] = r0.z; rb[3] = r1.x; rb[4] = r1.y; rb[5] = r1.z;
+    rb[6] = r2.x; rb[7] = r2.y; rb[8] = r2.z;
+  }
+  const int shA = a.P.shape[A];
+  const float scA = (float)a.P.scale[A];
+  // M = R_B^T R_A scale_A
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      F.M[3 * i + j] = fmaf(rb[i], ra[j], fmaf(rb[3 + i], ra[3 + j], rb[6 + i] * ra[6 + j])) * scA;
+  const double3 d = a.P.pos[A] - P.x;
+  const float3 df = tof(d);
+  F.dB = f3(fmaf(rb[0], df.x, fmaf(rb[3], df.y, rb[6] * df.z)), fmaf(rb[1], df.x, fmaf(rb[4], df.y, rb[7] * df.z)),
+            fmaf(rb[2], df.x, fmaf(rb[5], df.y, rb[8] * df.z)));
   F.invh = (float)P.invh;
-  F.h = (float)(1.0 / P.invh);
-  F.lip = a.S.lip[2 * shape];
-  F.gmax = a.S.lip[2 * shape + 1];
-  F.gs = P.gs;
+  F.cg = tof(-1.0 * P.o * P.invh);
+  F.ux = (float)(P.gs.x - 1); F.uy = (float)(P.gs.y - 1); F.uz = (float)(P.gs.z - 1);
+  const float N1 = 1.7320508f * (float)a.S.node_box[8 * shA + 6] * scA;
+  const float n1d = fabsf(df.x) + fabsf(df.y) + fabsf(df.z);
+  const float el = EPS_F * (N1 + 2.0f * n1d);
+  F.el = el;
+  F.rB = (float)P.r;
+  const float R = F.rB * (1.0f + 1e-6f) + el;
+  F.R2 = R * R * (1.0f + 1e-6f);
+  const float eg = F.invh * (el + EPS_F * (fabsf(F.cg.x) + fabsf(F.cg.y) + fabsf(F.cg.z)) / F.invh) +
+                   EPS_F * (float)(P.gs.x + P.gs.y + P.gs.z);
+  F.eg = eg;
+  const float L = a.S.lip[2 * pshape];
+  const float Q = quant16<SDFK>();
+  const float Qp = Q / (1.0f - Q);
+  F.Tq = 1.0f / (1.0f - Qp);
+  F.T = (3.0f * L * Qp + 3.0f * L * eg + 1e-7f) * F.Tq * (1.0f + 1e-5f);
+  F.gmax = a.S.lip[2 * pshape + 1];
+  F.sy = P.gs.x;
+  F.sz = P.gs.x * P.gs.y;
   F.sdf = a.S.sdf16 + (P.sdf - a.S.sdf);
   F.key = P.key;
+  if (KIND != KIND_PP) {
+    for (int k = 0; k < 9; ++k) F.RA[k] = ra[k] * scA;
+    F.n1w = EPS_F * N1;
+  }
   return F;
 }
 
-// Cell-window admission of walls and images from the FP32 node offset:
-// 0 = certainly rejected, 1 = certainly admitted, 2 = the FP64 node may lie in
-// a neighbouring cell (within the error bound of a cell boundary).
+LD float3 mulf(const float* M, float x, float y, float z) {
+  return f3(fmaf(M[0], x, fmaf(M[1], y, M[2] * z)), fmaf(M[3], x, fmaf(M[4], y, M[5] * z)),
+            fmaf(M[6], x, fmaf(M[7], y, M[8] * z)));
+}
+
+// Interpolated phi / h of the 16-bit store at grid point g, which must lie in
+// [0, size - 1) on every axis.
+template <int SDFK>
+LD float phi16(const PairF& F, float gx, float gy, float gz) {
+  const int i0 = __float2int_rd(gx), j0 = __float2int_rd(gy), k0 = __float2int_rd(gz);
+  const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
+  const unsigned short* b = F.sdf + (k0 * F.sz + j0 * F.sy + i0);
+  const unsigned short* by = b + F.sy;
+  const unsigned short* bz = b + F.sz;
+  const unsigned short* byz = bz + F.sy;
+  const float c0 = decode16<SDFK>(__ldg(b)), c1 = decode16<SDFK>(__ldg(b + 1));
+  const float c2 = decode16<SDFK>(__ldg(by)), c3 = decode16<SDFK>(__ldg(by + 1));
+  const float c4 = decode16<SDFK>(__ldg(bz)), c5 = decode16<SDFK>(__ldg(bz + 1));
+  const float c6 = decode16<SDFK>(__ldg(byz)), c7 = decode16<SDFK>(__ldg(byz + 1));
+  const float x0 = fmaf(fx, c1 - c0, c0), x1 = fmaf(fx, c3 - c2, c2);
+  const float x2 = fmaf(fx, c5 - c4, c4), x3 = fmaf(fx, c7 - c6, c6);
+  const float y0 = fmaf(fy, x1 - x0, x0), y1 = fmaf(fy, x3 - x2, x2);
+  return fmaf(fz, y1 - y0, y0);
+}
+
+// Cell-window admission of walls and images from the FP32 world node offset ra
+// (error bound e): 0 = certainly rejected, 1 = certainly admitted, 2 = the FP64
+// node may lie in a neighbouring cell (within e of a cell boundary).
 template <int KIND>
-LD int window_state(const StepArgs& a, double3 x, float3 ra, float n1ra, int key) {
+LD int window_state(const StepArgs& a, double3 x, float3 ra, float e0, int key) {
   const GridP& g = KIND == KIND_WALL ? a.wg : a.pg;
   const double3 w = x + tod(ra);
-  const double e = (double)(EPS_F * n1ra) + 1e-14 * (fabs(w.x) + fabs(w.y) + fabs(w.z));
+  const double e = (double)e0 + 1e-14 * (fabs(w.x) + fabs(w.y) + fabs(w.z));
   const double ux = (w.x - g.mn.x) * g.inv.x, uy = (w.y - g.mn.y) * g.inv.y, uz = (w.z - g.mn.z) * g.inv.z;
   if (fabs(ux - rint(ux)) <= e * g.inv.x + 1e-9 || fabs(uy - rint(uy)) <= e * g.inv.y + 1e-9 ||
       fabs(uz - rint(uz)) <= e * g.inv.z + 1e-9)
@@ -744,105 +817,55 @@ LD int window_state(const StepArgs& a, double3 x, float3 ra, float n1ra, int key
   return in_window(key, g, c, lo, hi) ? 1 : 0;
 }
 
-// phi / h of the 16-bit store at grid point (gx, gy, gz), known to lie inside
-// the grid by at least eg on every axis, minus the bound on its difference from
-// the FP64 value at the FP64 point: > 0 proves phi > 0 there.
-template <int SDFK>
-LD float phi16_lower(const PartnerF& P, float gx, float gy, float gz, float eg) {
-  const int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
-  const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
-  const int sy = P.gs.x, sz = P.gs.x * P.gs.y;
-  const unsigned short* b = P.sdf + (k0 * sz + j0 * sy + i0);
-  const float c0 = decode16<SDFK>(__ldg(b)), c1 = decode16<SDFK>(__ldg(b + 1));
-  const float c2 = decode16<SDFK>(__ldg(b + sy)), c3 = decode16<SDFK>(__ldg(b + sy + 1));
-  const float c4 = decode16<SDFK>(__ldg(b + sz)), c5 = decode16<SDFK>(__ldg(b + sz + 1));
-  const float c6 = decode16<SDFK>(__ldg(b + sz + sy)), c7 = decode16<SDFK>(__ldg(b + sz + sy + 1));
-  const float wx0 = 1.f - fx, wy0 = 1.f - fy, wz0 = 1.f - fz;
-  const float phi = ((c0 * wx0 + c1 * fx) * wy0 + (c2 * wx0 + c3 * fx) * fy) * wz0 +
-                    ((c4 * wx0 + c5 * fx) * wy0 + (c6 * wx0 + c7 * fx) * fy) * fz;
-  const float cmax = fmaxf(fmaxf(fmaxf(fabsf(c0), fabsf(c1)), fmaxf(fabsf(c2), fabsf(c3))),
-                           fmaxf(fmaxf(fabsf(c4), fabsf(c5)), fmaxf(fabsf(c6), fabsf(c7))));
-  const float band = cmax * (quant16<SDFK>() + 4e-6f) + 3.0f * P.lip * eg + 1e-7f;
-  return phi - band;  // NaN for NaN / Inf corners: never > 0
-}
-
-// Grid point of a partner-relative position r (offset ra from the owner's
-// centre) and its error bound eg; 0 = certainly outside the grid (the FP64 test
-// rejects), 1 = certainly inside by eg, 2 = within eg of the grid boundary.
-LD int grid_point_f(const PartnerF& P, float3 r, float n1ra, float& gx, float& gy, float& gz, float& eg) {
-  const float3 l = rotinvf(r, P.q);
-  gx = (l.x - P.o.x) * P.invh;
-  gy = (l.y - P.o.y) * P.invh;
-  gz = (l.z - P.o.z) * P.invh;
-  eg = P.invh * EPS_F * (n1ra + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
-  // the FP64 test rejects g < 0 or g >= size - 1 on any axis
-  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
-  if (gx < -eg || gy < -eg || gz < -eg || gx >= ux + eg || gy >= uy + eg || gz >= uz + eg) return 0;
-  if (gx < eg || gy < eg || gz < eg || gx >= ux - eg || gy >= uy - eg || gz >= uz - eg) return 2;
-  return 1;
-}
-
-// False only when node_hits certainly rejects the node.
+// FP32 screen of one node (offset nd, template units): false only when the
+// FP64 test (node_hits) certainly rejects it.
 template <int KIND, int SDFK>
-LD bool node_may_hit_f(const StepArgs& a, const SelfF& S, const PartnerF& P, float3 ra, float3 r) {
-  const float n1ra = n1f(ra);
-  const float el = EPS_F * (n1ra + P.n1d);
+LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd) {
+  const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
   if (KIND == KIND_PP) {
-    const float R = P.r * (1.0f + 1e-6f) + el;
-    if (dotf(r, r) > R * R) return false;
+    if (l.x * l.x + l.y * l.y + l.z * l.z > F.R2) return false;
   } else {
-    if (window_state<KIND>(a, S.x, ra, n1ra, P.key) == 0) return false;
+    if (window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) == 0) return false;
   }
-  float gx, gy, gz, eg;
-  const int in = grid_point_f(P, r, n1ra, gx, gy, gz, eg);
-  if (in != 1) return in == 2;
-  return !(phi16_lower<SDFK>(P, gx, gy, gz, eg) > 0.f);
+  const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+  // the FP64 test rejects g < 0 or g >= size - 1 on any axis
+  const float lo = fminf(gx, fminf(gy, gz));
+  const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+  if (lo < -F.eg || hi >= F.eg) return false;
+  if (lo < F.eg || hi >= -F.eg) return true;  // within the error of the grid boundary
+  return !(phi16<SDFK>(F, gx, gy, gz) > F.T);  // NaN never rejects
 }
 
-// Second cluster cull, against the partner's grid and SDF. Nodes outside the
-// grid box [0, size - 1] (grid units) are rejected by the FP64 test, so a cluster
-// sphere wholly outside the box is culled. Otherwise phi / h is evaluated at q,
-// the centre projected into the box shrunk by m >= eg: for a node p inside the
-// box, |p - q| <= |p - c| + sqrt(3) m (projection onto a convex set does not
-// expand distances), the segment p-q lies in the box, and along it phi / h
-// changes by at most gmax per grid unit, so phi(q) - gmax (rad + sqrt(3) m) > 0
-// proves phi > 0 at every node of the cluster.
-template <int SDFK>
-LD bool cluster_sdf_may_hit_f(float3 cA, float rad, const PartnerF& P) {
-  const float3 l = rotinvf(cA + P.d, P.q);
-  const float gx = (l.x - P.o.x) * P.invh, gy = (l.y - P.o.y) * P.invh, gz = (l.z - P.o.z) * P.invh;
-  const float eg = P.invh * EPS_F * (n1f(cA) + P.n1d + P.n1o) + EPS_F * (fabsf(gx) + fabsf(gy) + fabsf(gz));
-  const float radh = rad * P.invh * (1.0f + 1e-6f);
-  const float ux = (float)(P.gs.x - 1), uy = (float)(P.gs.y - 1), uz = (float)(P.gs.z - 1);
-  const float dx = fmaxf(fmaxf(-gx, gx - ux), 0.f), dy = fmaxf(fmaxf(-gy, gy - uy), 0.f),
-              dz = fmaxf(fmaxf(-gz, gz - uz), 0.f);
-  const float R = (radh + eg) * (1.0f + 1e-6f);
-  if (dx * dx + dy * dy + dz * dz > R * R) return false;
-  const float m = fmaxf(eg, 1e-3f);  // > 0: q stays below size - 1, so its cell is in the grid
-  if (ux < 4.f * m || uy < 4.f * m || uz < 4.f * m) return true;
-  const float qx = fminf(fmaxf(gx, m), ux - m), qy = fminf(fmaxf(gy, m), uy - m), qz = fminf(fmaxf(gz, m), uz - m);
-  const float reach = P.gmax * (radh + 2.8f * m) + 1e-6f;
-  return !(phi16_lower<SDFK>(P, qx, qy, qz, eg) > reach);
-}
-
-// Conservative cluster cull in FP32 (the bounds of node_may_hit_f applied to the
-// cluster's bounding sphere).
-template <int KIND>
-LD bool cluster_may_hit_f(float3 cA, float rad, const PartnerF& P) {
-  const float3 wc = cA + P.d;
-  const float e = EPS_F * (n1f(cA) + P.n1d);
+// Cluster cull (sphere of radius rad about the cluster centre cn, template
+// units): false only when no node of the cluster can pass node_hits.
+//  - particle partners: the sphere misses the partner's bounding sphere;
+//  - the sphere misses the partner's grid box (nodes outside it fail the SDF test);
+//  - phi / h at q, the centre projected into the box shrunk by m >= eg, exceeds
+//    the cluster's reach: for a node p inside the box, |p - q| <= |p - c| +
+//    sqrt(3) m (projection onto a convex set does not expand distances), the
+//    segment p-q lies in the box, and along it phi / h changes by at most gmax
+//    per grid unit, so phi(q) - gmax (rad + sqrt(3) m) > 0 proves phi > 0 at
+//    every node of the cluster.
+template <int KIND, int SDFK>
+LD bool cluster_may_hit_f(const PairF& F, float4 cn, float scA) {
+  const float3 l = mulf(F.M, cn.x, cn.y, cn.z) + F.dB;
+  const float rad = cn.w * scA * (1.0f + 1e-6f);
   if (KIND == KIND_PP) {
-    const float R = (P.r + rad) * (1.0f + 1e-6f) + e;
-    return dotf(wc, wc) <= R * R;
+    const float R = F.rB * (1.0f + 1e-6f) + rad + F.el;
+    if (l.x * l.x + l.y * l.y + l.z * l.z > R * R * (1.0f + 1e-6f)) return false;
   }
-  const float3 l = rotinvf(wc, P.q);
-  const float3 hi = f3(P.o.x + (P.gs.x - 1) * P.h, P.o.y + (P.gs.y - 1) * P.h, P.o.z + (P.gs.z - 1) * P.h);
-  const float dx = fmaxf(fmaxf(P.o.x - l.x, l.x - hi.x), 0.f);
-  const float dy = fmaxf(fmaxf(P.o.y - l.y, l.y - hi.y), 0.f);
-  const float dz = fmaxf(fmaxf(P.o.z - l.z, l.z - hi.z), 0.f);
-  const float ext = (hi.x - P.o.x) + (hi.y - P.o.y) + (hi.z - P.o.z);
-  const float R = rad * (1.0f + 1e-6f) + e + EPS_F * (ext + P.n1o);
-  return dx * dx + dy * dy + dz * dz <= R * R;
+  const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+  const float radh = rad * F.invh;
+  const float dx = fmaxf(fmaxf(-gx, gx - F.ux), 0.f), dy = fmaxf(fmaxf(-gy, gy - F.uy), 0.f),
+              dz = fmaxf(fmaxf(-gz, gz - F.uz), 0.f);
+  const float Rb = (radh + F.eg) * (1.0f + 1e-6f);
+  if (dx * dx + dy * dy + dz * dz > Rb * Rb) return false;
+  const float m = fmaxf(F.eg, 1e-3f);  // > 0: q stays below size - 1, so its cell is in the grid
+  if (F.ux < 4.f * m || F.uy < 4.f * m || F.uz < 4.f * m) return true;
+  const float qx = fminf(fmaxf(gx, m), F.ux - m), qy = fminf(fmaxf(gy, m), F.uy - m),
+              qz = fminf(fmaxf(gz, m), F.uz - m);
+  const float reach = (F.gmax * (radh + 2.8f * m) + 1e-6f) * F.Tq * (1.0f + 1e-6f);
+  return !(phi16<SDFK>(F, qx, qy, qz) > F.T + reach);
 }
 
 LD SelfCtx self_ctx(const StepArgs& a, int A) {
@@ -861,63 +884,44 @@ LD int partner_shape(const StepArgs& a, int pid) {
   return a.P.shape[KIND == KIND_GHOST ? (pid >> 3) : pid];
 }
 
-// Screens one (A, partner) pair: FP32 cluster cull and node screen. The nodes
-// the screen cannot reject are written, in node order, to the precision-form
-// node buffer and the pair is queued for k_contacts_f; a pair without such
-// nodes gets its empty contact segment here.
+// Screens one (A, partner) pair: cluster cull, then the node screen over the
+// surviving clusters. The nodes the screen cannot reject are written, in node
+// order, to the precision-form node buffer and the pair is queued for
+// k_contacts_f; a pair without such nodes gets its empty contact segment here.
 template <int KIND, int SDFK>
-LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const SelfF& S, int* s_cl,
-                      unsigned* s_mask, unsigned (&cnt)[6]) {
+LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* s_cl, unsigned* s_mask,
+                      unsigned (&cnt)[6]) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
-  PartnerF P;
+  const int shA = a.P.shape[A];
+  const int n0 = a.S.node_off[shA], nn = a.S.node_cnt[shA], cl0 = a.S.cl_off[shA], ncl = a.S.cl_cnt[shA];
+  const float scA = (float)a.P.scale[A];
+  const double3 xA = a.P.pos[A];
+  PairF F;
   {
-    const Partner P64 = load_partner<KIND>(a, pid);
-    P = partner_f<KIND>(a, P64, S, partner_shape<KIND>(a, pid));
+    const Partner P = load_partner<KIND>(a, pid);
+    F = make_pair_f<KIND, SDFK>(a, A, P, partner_shape<KIND>(a, pid), KIND == KIND_GHOST ? (pid >> 3) : pid);
   }
   int nsurv = 0;
-  for (int c0 = 0; c0 < S.ncl; c0 += 32) {
+  for (int c0 = 0; c0 < ncl; c0 += 32) {
     const int c = c0 + lane;
     bool keep = false;
-    if (c < S.ncl) {
-      const double4 sp = a.S.cl_sphere[S.cl0 + c];
-      const float3 cA = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc);
-      keep = cluster_may_hit_f<KIND>(cA, (float)sp.w * S.sc, P);
+    if (c < ncl) {
+      const double4 sp = a.S.cl_sphere[cl0 + c];
+      keep = cluster_may_hit_f<KIND, SDFK>(F, make_float4((float)sp.x, (float)sp.y, (float)sp.z, (float)sp.w), scA);
     }
     const unsigned m = __ballot_sync(FULL, keep);
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
     nsurv += __popc(m);
   }
-  __syncwarp();
-  // second cull on the survivors, compacted in place (writes never pass reads)
-  int nsurv2 = 0;
-  for (int k0 = 0; k0 < nsurv; k0 += 32) {
-    const int k = k0 + lane;
-    bool keep = false;
-    int c = 0;
-    if (k < nsurv) {
-      c = s_cl[k];
-      const double4 sp = a.S.cl_sphere[S.cl0 + c];
-      const float3 cA = rotf(S.q, f3((float)sp.x, (float)sp.y, (float)sp.z) * S.sc);
-      keep = cluster_sdf_may_hit_f<SDFK>(cA, (float)sp.w * S.sc, P);
-    }
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (keep) s_cl[nsurv2 + __popc(m & lanemask_lt())] = c;
-    nsurv2 += __popc(m);
-  }
-  cnt[0] += 1; cnt[1] += S.ncl; cnt[2] += nsurv; cnt[3] += nsurv2;
-  nsurv = nsurv2;
+  cnt[0] += 1; cnt[1] += ncl; cnt[2] += nsurv; cnt[3] += nsurv;
   __syncwarp();
   int total = 0;
   for (int k = 0; k < nsurv; ++k) {
     const int ni = s_cl[k] * 32 + lane;
-    cnt[4] += min(32, S.nn - s_cl[k] * 32);
+    cnt[4] += min(32, nn - s_cl[k] * 32);
     bool may = false;
-    if (ni < S.nn) {
-      const float4 nd = a.S.node_pos_f[S.n0 + ni];
-      const float3 ra = rotf(S.q, f3(nd.x, nd.y, nd.z) * S.sc);
-      may = node_may_hit_f<KIND, SDFK>(a, S, P, ra, ra + P.d);
-    }
+    if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, a.S.node_pos_f[n0 + ni]);
     const unsigned m = __ballot_sync(FULL, may);
     if (lane == 0) s_mask[k] = m;
     total += __popc(m);
@@ -960,17 +964,6 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, const
   }
 }
 
-LD SelfF self_f(const StepArgs& a, int A) {
-  SelfF S;
-  S.x = a.P.pos[A];
-  S.q = toq(a.P.quat[A]);
-  S.sc = (float)a.P.scale[A];
-  const int sh = a.P.shape[A];
-  S.n0 = a.S.node_off[sh]; S.nn = a.S.node_cnt[sh];
-  S.cl0 = a.S.cl_off[sh]; S.ncl = a.S.cl_cnt[sh];
-  return S;
-}
-
 // One warp per listed pair: the flat pair lists of the kinds in KINDS, in
 // particle, wall, image order.
 template <int KINDS, int SDFK>
@@ -987,18 +980,15 @@ __global__ void __launch_bounds__(NP_WARPS * 32, 4) k_screen_f(StepArgs a, int l
     if ((KINDS & 1) && e < n0) {
       const int idx = a.pl.list[0][e];
       const int A = idx / a.pp.cap;
-      screen_pair_f<KIND_PP, SDFK>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, self_f(a, A), s_cl[warp],
-                                   s_mask[warp], cnt);
+      screen_pair_f<KIND_PP, SDFK>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_mask[warp], cnt);
     } else if ((KINDS & 2) && e < n0 + n1) {
       const int idx = a.pl.list[1][e - n0];
       const int A = idx / a.pw.cap;
-      screen_pair_f<KIND_WALL, SDFK>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, self_f(a, A), s_cl[warp],
-                                     s_mask[warp], cnt);
+      screen_pair_f<KIND_WALL, SDFK>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_mask[warp], cnt);
     } else if (KINDS & 4) {
       const int idx = a.pl.list[2][e - n0 - n1];
       const int A = idx / a.pgh.cap;
-      screen_pair_f<KIND_GHOST, SDFK>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, self_f(a, A), s_cl[warp],
-                                      s_mask[warp], cnt);
+      screen_pair_f<KIND_GHOST, SDFK>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_mask[warp], cnt);
     }
   }
   if (a.screen_stats && (threadIdx.x & 31) == 0)
