@@ -152,6 +152,7 @@ struct StepArgs {
   GridP pg;         // particle grid
   GridP wg;         // wall grid
   const int* cell_idx;    // particle grid: sorted particle index
+  float4* cell_pk;        // particle grid, sorted order: FP32 centre and bounding radius
   const int* cell_start;
   const int* cell_end;
   SlotView pp, pw, pgh;          // this step

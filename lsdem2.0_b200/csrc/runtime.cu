@@ -323,6 +323,7 @@ struct lsdem_solver {
   std::vector<int> h_node_off, h_cl_off;
   GridP pg{}, wg{};
   DArr<int> cell_idx, cell_start, cell_end, sorted_key;
+  DArr<float4> cell_pk;
   DArr<int> bk_counts, bk_fill, bk_offs, bk_scan, bk_big, bk_bigc, bk_tmp;
   SlotsDev slots[2][3];      // [history parity][kind]
   ContactsDev con[2];
@@ -718,6 +719,7 @@ void initialize(lsdem_solver* s) {
   set_grid(s->wg, s->dmin, s->dmax, s->W.n() ? 2.0 * rw : 0.0);
   const int n = s->P.n();
   CK(s->cell_idx.alloc(std::max(n, 1)));
+  CK(s->cell_pk.alloc(std::max(n, 1)));
   CK(s->sorted_key.alloc(std::max(n, 1)));
   CK(s->cell_start.alloc(s->pg.ncells));
   CK(s->cell_end.alloc(s->pg.ncells));
@@ -789,6 +791,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.pg = s->pg;
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
+  a.cell_pk = s->cell_pk.p;
   auto sv = [](SlotsDev& d) {
     SlotView v;
     v.cap = d.cap; v.cnt = d.cnt.p; v.id = d.id.p; v.seg_start = d.seg_start.p; v.seg_cnt = d.seg_cnt.p;
@@ -908,12 +911,12 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
   }
   if (hook) hook(user, t);
   { PhaseTimer pt(s, 7); launch_kick(a, st); }
-  // kernels launched by this step: kick/drift/keys, cell sort (9), candidates,
+  // kernels launched by this step: kick/drift/keys, cell sort (9), packing + candidates,
   // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (8),
   // image compaction + candidates, ghost narrowphase; bonds
   // (the precision form adds one contact pass per narrowphase)
   const int nf = s->precision == PREC_FP64 ? 0 : 1;
-  if (a.P.n > 0) s->launches += 13 + nf + (s->nsets > 0 ? 13 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 13 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
 }

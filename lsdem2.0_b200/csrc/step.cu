@@ -152,11 +152,23 @@ LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
   for (int j = 0; j < cnt; ++j) list[base + j] = A * cap + j;
 }
 
+// Centres and bounding radii in cell-sorted order, FP32, for the candidate walk.
+__global__ void k_pack_cells(StepArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.P.n) return;
+  const int B = a.cell_idx[k];
+  const double3 x = a.P.pos[B];
+  a.cell_pk[k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)a.P.radius[B]);
+}
+
 // Candidate partners of each particle A.
 // Particle partners: B > A, visible (in a cell), bounding spheres within
 // reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
-// node's 27-cell window since cells are at least 2 max radius wide).
+// node's 27-cell window since cells are at least 2 max radius wide). The test
+// runs on the FP32 copies with a margin that covers their rounding (relative
+// 1e-5 of the reach plus 1e-6 of the coordinates), so the candidates are a
+// superset of the exact ones; the narrowphase decides every node exactly.
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
 // mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
@@ -169,6 +181,9 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     const int A = a.cell_idx[t];
     const double3 xA = a.P.pos[A];
     const double rA = a.P.radius[A];
+    const float4 pa = a.cell_pk[t];
+    const float3 xf = make_float3(pa.x, pa.y, pa.z);
+    const float rf = pa.w, n1a = fabsf(pa.x) + fabsf(pa.y) + fabsf(pa.z);
     const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
     const int cap = a.pp.cap;
     int* out = a.pp.id + (size_t)A * cap;
@@ -186,11 +201,12 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
           if (st < 0) continue;
           const int en = a.cell_end[h];
           for (int k = st; k < en; ++k) {
+            const float4 pb = a.cell_pk[k];
+            const float dx = pb.x - xf.x, dy = pb.y - xf.y, dz = pb.z - xf.z;
+            const float R = (rf + pb.w) * (1.0f + 1e-5f) + 1e-6f * (n1a + fabsf(pb.x) + fabsf(pb.y) + fabsf(pb.z));
+            if (dx * dx + dy * dy + dz * dz > R * R) continue;
             const int B = a.cell_idx[k];
             if (B <= A) continue;
-            const double3 xB = a.P.pos[B];
-            const double R = (rA + a.P.radius[B]) * (1.0 + 1e-9) + coord_slack(xA, xB);
-            if (len2(xA - xB) > R * R) continue;
             if (n < cap) out[n] = B;
             ++n;
           }
@@ -229,7 +245,9 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
 }
 
 void launch_candidates(const StepArgs& a, cudaStream_t s) {
-  if (a.P.n > 0) k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
+  if (a.P.n <= 0) return;
+  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(a);
+  k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
 }
 
 // ---------------------------------------------------------------------------
