@@ -42,8 +42,11 @@ struct ShapeView {
   const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
   const double* node_box;     // 8 per shape (unscaled): node bounding box lo xyz, hi xyz,
                               //   largest node distance from the body origin, 0
-  // precision form: SDF values / template spacing in 16-bit floats, FP32 nodes
-  const unsigned short* sdf16;  // same offsets as sdf; FP16 or BF16 bits
+  // precision form: SDF values / template spacing in 16-bit floats (FP16 or BF16
+  // bits), cell-major: the 8 corners of cell (i, j, k) in one uint4, corner
+  // dx + 2 dy + 4 dz in 16-bit lane order, cells x-fastest; FP32 nodes
+  const uint4* cell16;
+  const long long* cell_off;    // per shape, into cell16
   const float4* node_pos_f;     // FP32 copy of node_pos
   const float* lip;             // 2 per shape, in spacings: largest |phi| difference of grid
                                 //   neighbours; largest gradient-norm bound of a grid cell

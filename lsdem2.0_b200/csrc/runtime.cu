@@ -311,7 +311,8 @@ struct lsdem_solver {
   DArr<double3> s_node_pos;
   DArr<double4> s_cl;
   DArr<double> s_nbox;  // per shape: node bounding box (lo xyz, hi xyz), largest node distance, 0
-  DArr<unsigned short> s_sdf16;
+  DArr<uint4> s_cell16;        // precision form: 16-bit corners of every grid cell
+  DArr<long long> s_cell_off;  // per shape, into s_cell16
   DArr<float4> s_node_f;
   DArr<float> s_lip;
   // precision form: screened nodes and queued pairs (per-step scratch)
@@ -655,19 +656,34 @@ void initialize(lsdem_solver* s) {
   }
   if (s->precision != PREC_FP64) {
     // precision form: phi / h of each template in 16 bits, FP32 node copy
-    std::vector<unsigned short> sdf16(sdf.size());
-    size_t k = 0;
-    for (const ShapeHost& sh : s->shapes)
-      for (double v : sh.sdf) {
+    // cell-major 16-bit store: the 8 corners of cell (i, j, k) in 16 bytes, corner
+    // c = dx + 2 dy + 4 dz at 16-bit lane c, cells x-fastest
+    std::vector<uint4> cells;
+    std::vector<long long> cell_off;
+    for (const ShapeHost& sh : s->shapes) {
+      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
+      cell_off.push_back((long long)cells.size());
+      auto enc = [&](double v) -> unsigned {
         const float u = (float)(v / sh.h);
+        unsigned short r;
         if (s->precision == PREC_FP32_BF16) {
           const __nv_bfloat16 b = __float2bfloat16_rn(u);
-          std::memcpy(&sdf16[k++], &b, 2);
+          std::memcpy(&r, &b, 2);
         } else {
           const __half hh = __float2half_rn(u);
-          std::memcpy(&sdf16[k++], &hh, 2);
+          std::memcpy(&r, &hh, 2);
         }
-      }
+        return r;
+      };
+      auto at = [&](int x, int y, int z) { return sh.sdf[(size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z)]; };
+      for (int z = 0; z + 1 < nz; ++z)
+        for (int y = 0; y + 1 < ny; ++y)
+          for (int x = 0; x + 1 < nx; ++x) {
+            unsigned c[8];
+            for (int q = 0; q < 8; ++q) c[q] = enc(at(x + (q & 1), y + ((q >> 1) & 1), z + (q >> 2)));
+            cells.push_back(make_uint4(c[0] | c[1] << 16, c[2] | c[3] << 16, c[4] | c[5] << 16, c[6] | c[7] << 16));
+          }
+    }
     std::vector<float4> nf(node_pos.size());
     for (size_t i = 0; i < node_pos.size(); ++i)
       nf[i] = make_float4((float)node_pos[i].x, (float)node_pos[i].y, (float)node_pos[i].z, 0.f);
@@ -697,7 +713,8 @@ void initialize(lsdem_solver* s) {
       lip.push_back((float)(m / sh.h * (1.0 + 1e-6)));
       lip.push_back((float)(g / sh.h * (1.0 + 1e-6)));
     }
-    CK(s->s_sdf16.upload(sdf16.data(), sdf16.size(), st));
+    CK(s->s_cell16.upload(cells.data(), cells.size(), st));
+    CK(s->s_cell_off.upload(cell_off.data(), cell_off.size(), st));
     CK(s->s_node_f.upload(nf.data(), nf.size(), st));
     CK(s->s_lip.upload(lip.data(), lip.size(), st));
   }
@@ -785,7 +802,8 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
   a.S.cl_sphere = s->s_cl.p;
   a.S.node_box = s->s_nbox.p;
-  a.S.sdf16 = s->s_sdf16.p;
+  a.S.cell16 = s->s_cell16.p;
+  a.S.cell_off = s->s_cell_off.p;
   a.S.node_pos_f = s->s_node_f.p;
   a.S.lip = s->s_lip.p;
   a.pg = s->pg;

@@ -694,11 +694,6 @@ LD double3 tod(float3 v) { return d3(v.x, v.y, v.z); }
 
 static constexpr float EPS_F = 1.6e-5f;
 
-template <int SDFK>
-LD float decode16(unsigned short b) {
-  if (SDFK == PREC_FP32_BF16) return __uint_as_float(((unsigned)b) << 16);
-  return __half2float(__ushort_as_half(b));
-}
 // relative bound of the 16-bit store and FP32 interpolation error (with margin)
 template <int SDFK>
 LD constexpr float quant16() { return SDFK == PREC_FP32_BF16 ? 3.95e-3f + 1e-6f : 4.95e-4f + 1e-6f; }
@@ -717,8 +712,8 @@ struct PairF {
   float T;           // rejection threshold of phi / h
   float Tq;          // 1 / (1 - Q')
   float gmax;        // gradient-norm bound of phi / h per grid unit
-  int sy, sz;
-  const unsigned short* sdf;
+  int sy, sz;        // cell strides
+  const uint4* cells;
   int key;           // walls and images: the partner's cell key
   float RA[9];       // walls and images: R_A scale_A (world offsets of the nodes)
   float n1w;         // walls and images: error bound of the world node offset
@@ -782,9 +777,9 @@ LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int
   F.Tq = 1.0f / (1.0f - Qp);
   F.T = (3.0f * L * Qp + 3.0f * L * eg + 1e-7f) * F.Tq * (1.0f + 1e-5f);
   F.gmax = a.S.lip[2 * pshape + 1];
-  F.sy = P.gs.x;
-  F.sz = P.gs.x * P.gs.y;
-  F.sdf = a.S.sdf16 + (P.sdf - a.S.sdf);
+  F.sy = P.gs.x - 1;
+  F.sz = (P.gs.x - 1) * (P.gs.y - 1);
+  F.cells = a.S.cell16 + a.S.cell_off[pshape];
   F.key = P.key;
   if (KIND != KIND_PP) {
     for (int k = 0; k < 9; ++k) F.RA[k] = ra[k] * scA;
@@ -799,21 +794,21 @@ LD float3 mulf(const float* M, float x, float y, float z) {
 }
 
 // Interpolated phi / h of the 16-bit store at grid point g, which must lie in
-// [0, size - 1) on every axis.
+// [0, size - 1) on every axis: one 16-byte load of the cell's corners.
+template <int SDFK>
+LD float2 unpack16(unsigned w) {
+  if (SDFK == PREC_FP32_BF16) return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
 template <int SDFK>
 LD float phi16(const PairF& F, float gx, float gy, float gz) {
   const int i0 = __float2int_rd(gx), j0 = __float2int_rd(gy), k0 = __float2int_rd(gz);
   const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
-  const unsigned short* b = F.sdf + (k0 * F.sz + j0 * F.sy + i0);
-  const unsigned short* by = b + F.sy;
-  const unsigned short* bz = b + F.sz;
-  const unsigned short* byz = bz + F.sy;
-  const float c0 = decode16<SDFK>(__ldg(b)), c1 = decode16<SDFK>(__ldg(b + 1));
-  const float c2 = decode16<SDFK>(__ldg(by)), c3 = decode16<SDFK>(__ldg(by + 1));
-  const float c4 = decode16<SDFK>(__ldg(bz)), c5 = decode16<SDFK>(__ldg(bz + 1));
-  const float c6 = decode16<SDFK>(__ldg(byz)), c7 = decode16<SDFK>(__ldg(byz + 1));
-  const float x0 = fmaf(fx, c1 - c0, c0), x1 = fmaf(fx, c3 - c2, c2);
-  const float x2 = fmaf(fx, c5 - c4, c4), x3 = fmaf(fx, c7 - c6, c6);
+  const uint4 w = __ldg(F.cells + (k0 * F.sz + j0 * F.sy + i0));
+  const float2 c01 = unpack16<SDFK>(w.x), c23 = unpack16<SDFK>(w.y);
+  const float2 c45 = unpack16<SDFK>(w.z), c67 = unpack16<SDFK>(w.w);
+  const float x0 = fmaf(fx, c01.y - c01.x, c01.x), x1 = fmaf(fx, c23.y - c23.x, c23.x);
+  const float x2 = fmaf(fx, c45.y - c45.x, c45.x), x3 = fmaf(fx, c67.y - c67.x, c67.x);
   const float y0 = fmaf(fy, x1 - x0, x0), y1 = fmaf(fy, x3 - x2, x2);
   return fmaf(fz, y1 - y0, y0);
 }
@@ -984,8 +979,10 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
 
 // One warp per listed pair: the flat pair lists of the kinds in KINDS, in
 // particle, wall, image order.
+// Particle-only screens fit 64 registers (8 blocks per SM); walls and images
+// need the window test's FP64 registers.
 template <int KINDS, int SDFK>
-__global__ void __launch_bounds__(NP_WARPS * 32, 4) k_screen_f(StepArgs a, int li) {
+__global__ void __launch_bounds__(NP_WARPS * 32, KINDS == 1 ? 8 : 5) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
   const int warp = threadIdx.x >> 5;
