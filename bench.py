@@ -76,6 +76,10 @@ B_PAIR = 236
 B_CONTACT = 56
 B_PARTICLE_SCREEN = 72
 B_PAIR_SCREEN = 120
+# DRAM bytes (read + write) per k_screen_f launch, mean of the particle-pair and image
+# launches, from one ncu capture of the default workload in the FP32/BF16 form
+# (profiles/k_screen_f_polydisperse100k_dram.md); other workloads and forms report null.
+SCREEN_TRAFFIC_DEFAULT = (25.87e6 + 0.74e6 + 10.85e6) / 2
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
 
@@ -258,9 +262,15 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+L2_FLUSH_BYTES = 256 << 20  # > the 126 MB L2
+
+
 def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
-    """W warm-up steps, then exactly K timed steps (CUDA events on the solver's stream =
-    torch's current stream, the legacy default stream); max over ranks."""
+    """W warm-up steps, then exactly K timed steps, each bracketed by CUDA events on the
+    solver's stream with a 256 MB scratch write before it (outside the events) so that no
+    step starts from data the previous one left in L2; the state backup of each batch of
+    steps is timed with the batch's first step. Max over ranks. A second run of K steps
+    timed as a whole, L2 not flushed, is reported beside it (`warm_l2`)."""
     sv = load(lsdem, sc, args.workload, local, prec)
     dt = float(sc["dt"])
     if clocks is not None:
@@ -268,19 +278,28 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
     sv.step(dt, max(3, args.warmup))
     launches0 = sv.num(8)
     reruns0 = sv.num(7)
+    sv.set_step_timing(True, L2_FLUSH_BYTES)
     barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if clocks is not None:
         clocks.mark(True)
-    ev0.record()
     sv.step(dt, args.steps)
-    ev1.record()
     torch.cuda.synchronize()
     if clocks is not None:
         clocks.mark(False)
         clocks.__exit__()
-    ms = ev0.elapsed_time(ev1)
-    res = {"ms": ms, "launches": sv.num(8) - launches0, "reruns": sv.num(7) - reruns0, "stats": sv.step_stats()}
+    step_ms, step_calls = sv.profile()["step"]
+    assert step_calls == args.steps, (step_calls, args.steps)
+    sv.set_step_timing(False)
+    res = {"ms": step_ms, "launches": sv.num(8) - launches0, "reruns": sv.num(7) - reruns0,
+           "stats": sv.step_stats()}
+    # the same number of steps timed as one region, L2 not flushed
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    sv.step(dt, args.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    res["warm_ms"] = ev0.elapsed_time(ev1)
     # per-phase device times (CUDA events between phases) from a separate, shorter run
     res["profile_steps"] = min(args.steps, 20)
     sv.set_profiling(True)
@@ -293,9 +312,10 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
         res["screen"] = {k: v / res["profile_steps"] for k, v in sv.screen_stats().items()}
         sv.set_screen_stats(False)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        res["ms"] = float(t.item())
+        for key in ("ms", "warm_ms"):
+            t = torch.tensor([res[key]], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            res[key] = float(t.item())
     return sv, res
 
 
@@ -382,7 +402,9 @@ def main():
                 continue
             svf, r = time_form(lsdem, torch, sc, args, local, p, dist, barrier, None)
             svf.close()
-            forms[name] = {"value": n * world * args.steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / args.steps}
+            forms[name] = {"value": n * world * args.steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / args.steps,
+                           "warm_l2": {"value": n * world * args.steps / (r["warm_ms"] * 1e-3),
+                                       "ms_per_step": r["warm_ms"] / args.steps}}
         for name, p in FORMS.items():
             if p != 0:
                 err = force_error(lsdem, sc, args.workload, local, p)
@@ -404,22 +426,26 @@ def main():
         else:
             kernel = "k_screen_f"
             bytes_launch = (B_PARTICLE_SCREEN * n * launches_per_step + B_PAIR_SCREEN * pairs) / launches_per_step
+        traffic = (SCREEN_TRAFFIC_DEFAULT if (args.workload == "polydisperse" and args.particles == 100_000
+                                              and args.form == "fp32-bf16") else None)
         achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
         b_step = B_STEP_PARTICLE * n + B_CONTACT * stats["contacts"] + 16 * pairs
         ms_step = head["ms"] / args.steps
-        forms[args.form] = dict(forms.get(args.form, {}), value=value, ms_per_step=ms_step)
+        forms[args.form] = dict(forms.get(args.form, {}), value=value, ms_per_step=ms_step,
+                                warm_l2={"value": n * world * args.steps / (head["warm_ms"] * 1e-3),
+                                         "ms_per_step": head["warm_ms"] / args.steps})
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.form],
             "data": "synthetic (seeded)",
             "config": dict(cfg, form=args.form, parallelism=f"replicas x{world}",
-                           l2=f"not flushed: per-step algorithmic traffic {b_step / 1e6:.0f} MB "
-                              f"({'>' if b_step > 126e6 else '<'} 126 MB L2)",
+                           l2=f"flushed: {L2_FLUSH_BYTES >> 20} MB written before every timed step, outside "
+                              f"its events (per-step algorithmic traffic {b_step / 1e6:.0f} MB)",
                            contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs),
             "forms": forms,
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
             "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_step * 1e-3) / 1e9},
             "phases_ms_per_step": {k: v[0] / head["profile_steps"] for k, v in prof.items()},

@@ -187,11 +187,19 @@ void* lsdem_stream(const lsdem_solver* s);
  * 1 cell sort, 2 candidates, 3 particle/wall narrowphase + forces (precision forms:
  * the FP32 screen), 4 periodic wrap + ghost images + ghost candidates, 5 ghost
  * narrowphase + forces (precision forms: the screen), 6 bonds, 7 second half kick,
- * 8 precision forms: FP64 contact pass of both narrowphases. ms and calls hold
- * LSDEM_NUM_PHASES entries. Enabling resets the totals. */
-#define LSDEM_NUM_PHASES 9
+ * 8 precision forms: FP64 contact pass of both narrowphases, 9 whole steps (step
+ * timing, below). ms and calls hold LSDEM_NUM_PHASES entries. Enabling resets the
+ * totals of phases 0-8. */
+#define LSDEM_NUM_PHASES 10
 int lsdem_set_profiling(lsdem_solver* s, int on);
 int lsdem_get_profile(const lsdem_solver* s, double* ms, long long* calls);
+/* Benchmark support (no counterpart in the reference): when on, every step is
+ * bracketed by CUDA events on the solver stream (profile phase 9; the state backup
+ * of each batch of steps is timed with the batch's first step), and when
+ * l2_flush_bytes > 0 a scratch buffer of that size is written before each step,
+ * outside the events, so that no step starts with data left in L2 by the one
+ * before. Resets the phase-9 totals. */
+int lsdem_set_step_timing(lsdem_solver* s, int on, long long l2_flush_bytes);
 /* Work counts of the last step: candidate pairs (particle, wall, ghost) and contacts. */
 int lsdem_step_stats(lsdem_solver* s, long long* out4);
 /* Precision forms: counters of the FP32 screen summed over all steps run while

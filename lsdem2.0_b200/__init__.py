@@ -95,6 +95,7 @@ _SIGS = {
     "lsdem_get_profile": (C.c_int, [P, DP, LP]),
     "lsdem_step_stats": (C.c_int, [P, LP]),
     "lsdem_set_screen_stats": (C.c_int, [P, C.c_int]),
+    "lsdem_set_step_timing": (C.c_int, [P, C.c_int, C.c_longlong]),
     "lsdem_get_screen_stats": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
@@ -375,7 +376,11 @@ class Solver:
         return {"ids": ids, "bonded": bonded, "state": state}
 
     PHASES = ("kick_drift_keys", "cell_sort", "candidates", "narrowphase", "periodic", "ghost_narrowphase", "bonds",
-              "kick", "contact_pass")
+              "kick", "contact_pass", "step")
+
+    def set_step_timing(self, on=True, l2_flush_bytes=0):
+        """Per-step CUDA events (profile()["step"]), optionally with an L2 flush before each step."""
+        self._chk(lib.lsdem_set_step_timing(self.h, 1 if on else 0, int(l2_flush_bytes)), "set_step_timing")
 
     def set_profiling(self, on=True):
         self._chk(lib.lsdem_set_profiling(self.h, 1 if on else 0), "set_profiling")

@@ -358,6 +358,11 @@ struct lsdem_solver {
   double time = 0.0;
   // optional per-phase device timing (CUDA events on the solver stream)
   bool profiling = false;
+  // step timing (benchmarks): CUDA events around every step (phase 9), and an
+  // optional write of a scratch buffer larger than L2 before each step, outside
+  // the events
+  bool step_timing = false;
+  DArr<unsigned char> flush_buf;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
   std::vector<cudaEvent_t> event_pool;
   double prof_ms[LSDEM_NUM_PHASES] = {};
@@ -1033,6 +1038,14 @@ void grow(lsdem_solver* s) {
   }
 }
 
+// Step timing: L2 flush (when a buffer is set) and the step's start event.
+cudaEvent_t step_start(lsdem_solver* s) {
+  if (s->flush_buf.n) CK(cudaMemsetAsync(s->flush_buf.p, (int)(s->steps & 0xff), s->flush_buf.n, s->stream));
+  cudaEvent_t e = pool_event(s);
+  CK(cudaEventRecord(e, s->stream));
+  return e;
+}
+
 int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
   if (!s->ready) throw Fail{LSDEM_ERR_STATE, "lsdem_step before lsdem_initialize"};
   if (!(dt > 0.)) throw Fail{LSDEM_ERR_ARG, "Invalid timeStep"};
@@ -1041,6 +1054,8 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
   while (done < nsteps) {
     const long long B = std::min<long long>(std::max(1, std::min(s->cur_batch, s->batch)), nsteps - done);
     const int hp0 = s->hp;
+    // the batch's state backup is timed with its first step
+    cudaEvent_t first = s->step_timing ? step_start(s) : nullptr;
     backup(s);
     Status stat{};
     for (int attempt = 0;; ++attempt) {
@@ -1048,7 +1063,14 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
       double t = s->time;
       for (long long k = 0; k < B; ++k) {
         const bool rec = s->record && (done + k == nsteps - 1);
+        cudaEvent_t ea = nullptr;
+        if (s->step_timing) ea = (k == 0 && attempt == 0) ? first : step_start(s);
         step_once(s, dt, rec, hook, user, t);
+        if (ea) {
+          cudaEvent_t eb = pool_event(s);
+          CK(cudaEventRecord(eb, st));
+          s->prof_pending.push_back({9, {ea, eb}});
+        }
         t += dt;
       }
       CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(Status), cudaMemcpyDeviceToHost, st));
@@ -1646,8 +1668,24 @@ void* lsdem_stream(const lsdem_solver* s) { return s ? (void*)s->stream : nullpt
 int lsdem_set_profiling(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   s->profiling = on != 0;
-  for (int k = 0; k < LSDEM_NUM_PHASES; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
+  for (int k = 0; k < 9; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
   return LSDEM_OK;
+}
+
+int lsdem_set_step_timing(lsdem_solver* s, int on, long long l2_flush_bytes) {
+  if (!s || l2_flush_bytes < 0) return LSDEM_ERR_ARG;
+  return guard(s, [&] {
+    CK(cudaStreamSynchronize(s->stream));
+    s->step_timing = on != 0;
+    s->prof_ms[9] = 0.;
+    s->prof_calls[9] = 0;
+    if (on && l2_flush_bytes > 0) {
+      if (s->flush_buf.n != (size_t)l2_flush_bytes) CK(s->flush_buf.alloc((size_t)l2_flush_bytes));
+    } else {
+      s->flush_buf.release();
+    }
+    return LSDEM_OK;
+  });
 }
 
 int lsdem_get_profile(const lsdem_solver* s, double* ms, long long* calls) {
