@@ -172,6 +172,11 @@ class LSSolver {
   }
   void removePeriodicBoundary() { periodic_ = 0; lsdem_set_periodic(h_, 0); }
 
+  // Extension: arithmetic form of the narrowphase (LSDEM_PREC_FP64, the reference's,
+  // by default; LSDEM_PREC_FP32_FP16 / LSDEM_PREC_FP32_BF16: certified FP32 screening on
+  // 16-bit SDF templates with FP64 contacts). Takes effect at the next solve().
+  void setPrecision(const int mode) { report(lsdem_set_precision(h_, mode), "[Solver] "); }
+
   // Runs the step loop for maximumTime (numStep = floor(T/dt) + 1, numStep + 1 steps,
   // an output every numStep / numFrame steps), as LSSolver::solve (LSSolver.h:478-505, 994-1022).
   void solve(const double3 minDomain, const double3 maxDomain, const double3 gravity, const double timeStep,
