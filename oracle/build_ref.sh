@@ -28,3 +28,14 @@ nvcc -std=c++17 -O3 -DNDEBUG -Xcompiler -fPIC -shared \
   -I"$K" -I"$K/CUDAKernelFunction" \
   "${SRCS[@]}" -o "$OUT/libfundem_ref.so"
 echo "built $OUT/libfundem_ref.so"
+
+# The config-0 benchmark app (tests/apps/c0_bench.cpp, written against the
+# LSSolver API only) built against the reference solver itself: its
+# kernel/LSSolver.h and the same kernel sources, Release flags, sm_100a. The
+# same app source is built against this repository's drop-in LSSolver by
+# tests/test_fundem_same_gpu.py.
+nvcc -std=c++17 -O3 -DNDEBUG \
+  -gencode arch=compute_100a,code=sm_100a \
+  -I"$REF/FunDEM" -I"$K" -I"$K/CUDAKernelFunction" \
+  "$HERE/../tests/apps/c0_bench.cpp" "${SRCS[@]:0:5}" -o "$OUT/c0_bench_fundem"
+echo "built $OUT/c0_bench_fundem"

@@ -1,0 +1,95 @@
+"""Config 0 on the reference solver's own CUDA build and on this solver, same GPU, same app.
+
+tests/apps/c0_bench.cpp is written against the LSSolver API only. oracle/build_ref.sh builds
+it against the reference (FunDEM/kernel/LSSolver.h and its kernel sources, Release flags,
+sm_100a) into oracle/_ref/c0_bench_fundem; this test builds the same source against the
+drop-in include/kernel/LSSolver.h (FP64 form, the reference's arithmetic). Both run the
+config-0 scene (2,000 identical ellipsoids, 32^3 grids, 1,000 nodes, floor wall) from one
+scene file; each reports the device time of a fixed window of steps, measured with CUDA
+events recorded from the external-force hook (called by both solvers every step between
+the forces and the second half kick), and the particle velocities at the window's end.
+
+Checked: the velocities agree to FP64 round-off (same algorithm, same inputs). The two
+timings are printed (they are reported, not asserted).
+"""
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+FUNDEM = ROOT / "oracle" / "_ref" / "c0_bench_fundem"
+OURS = ROOT / "lsdem2.0_b200" / "_build" / "c0_bench_b200"
+APP = ROOT / "tests" / "apps" / "c0_bench.cpp"
+
+
+def build_ours() -> None:
+    if OURS.exists() and OURS.stat().st_mtime >= max(APP.stat().st_mtime,
+                                                     (ROOT / "include" / "kernel" / "LSSolver.h").stat().st_mtime):
+        return
+    cmd = ["nvcc", "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-I", str(ROOT / "include"), "-I", str(ROOT / "include" / "kernel"), str(APP),
+           "-L", str(ROOT / "lsdem2.0_b200"), "-llsdem_b200", "-Xlinker", "-rpath", "-Xlinker",
+           str(ROOT / "lsdem2.0_b200"), "-o", str(OURS)]
+    OURS.parent.mkdir(exist_ok=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+def write_scene(path, sc, nsteps, k0, k1):
+    s, f = sc["shape"], sc["floor"]
+    n = len(sc["pos"])
+    d = lambda a: np.ascontiguousarray(a, np.float64).tobytes()
+    i32 = lambda *v: struct.pack(f"<{len(v)}i", *v)
+    cx, cy = 0.5 * (sc["min"][0] + sc["max"][0]), 0.5 * (sc["min"][1] + sc["max"][1])
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+    with open(path, "wb") as fh:
+        fh.write(b"LSDEMC0\0")
+        fh.write(i32(len(s["nodes"]), *[int(v) for v in s["size"]], n))
+        fh.write(d([s["spacing"]]) + d(s["origin"]) + d(s["nodes"]) + d(s["sdf"]))
+        fh.write(d(sc["pos"]) + d(sc["quat"]) + d(sc["vel"]))
+        fh.write(d([sc["kn"], sc["ks"], sc["mu"], sc["e"], sc["density"]]))
+        fh.write(i32(*[int(v) for v in f["size"]]) + d([f["spacing"]]) + d(f["origin"]) + d(f["sdf"]))
+        fh.write(d([cx, cy, sc["min"][2]]) + d([1.0, 0.0, 0.0, 0.0]) + d([sc["mu"], sc["e"]]))
+        fh.write(i32(len(f["verts"]), len(tris)) + d(f["verts"]) + tris.tobytes())
+        fh.write(d([sc["dt"]]) + d(sc["min"]) + d(sc["max"]) + d(sc["gravity"]))
+        fh.write(i32(nsteps, k0, k1))
+
+
+def run(binary, scene, outdir, result):
+    r = subprocess.run([str(binary), str(scene), str(outdir), str(result)], capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    raw = result.read_bytes()
+    steps, window, nvel = struct.unpack("<3i", raw[:12])
+    ms = struct.unpack("<d", raw[12:20])[0]
+    vel = np.frombuffer(raw[20:20 + 24 * nvel], np.float64).reshape(nvel, 3)
+    return steps, window, ms, vel
+
+
+@pytest.mark.skipif(not FUNDEM.exists(), reason="oracle/_ref/c0_bench_fundem not built (needs the reference tree)")
+@pytest.mark.skipif(shutil.which("nvcc") is None and not OURS.exists(), reason="nvcc not available")
+def test_config0_same_gpu(lsdem, tmp_path):
+    from lsdem_b200 import scenes
+    build_ours()
+    sc = scenes.ellipsoid_falling()
+    nsteps, k0, k1 = 2000, 200, 1900
+    scene = tmp_path / "c0.bin"
+    write_scene(scene, sc, nsteps, k0, k1)
+    res = {}
+    for name, binary in (("fundem", FUNDEM), ("b200", OURS)):
+        out = tmp_path / name
+        out.mkdir()
+        res[name] = run(binary, scene, out, tmp_path / f"{name}.res")
+    (s0, w0, ms0, v0), (s1, w1, ms1, v1) = res["fundem"], res["b200"]
+    assert s0 >= k1 and s1 >= k1 and w0 == w1 == k1 - k0
+    assert v0.shape == v1.shape == (len(sc["pos"]), 3)
+    vmax = np.abs(v0).max()
+    assert np.abs(v1 - v0).max() <= 1e-9 * vmax, np.abs(v1 - v0).max() / vmax
+    print(f"config 0, {len(sc['pos'])} ellipsoids, steps {k0}..{k1}: reference build {ms0 / w0:.4f} ms/step, "
+          f"this solver (FP64) {ms1 / w1:.4f} ms/step, ratio {ms0 / ms1:.2f}x")
