@@ -39,9 +39,10 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 
-FORMS = {"fp32-bf16": 2, "fp32-fp16": 1, "fp64": 0}
+FORMS = {"fp32-bf16": 2, "fp32-fp16": 1, "fp64": 0, "fp32-bf16-learned": 2}
 DTYPE = {"fp32-bf16": "f32 screen on bf16 SDF, f64 contacts", "fp32-fp16": "f32 screen on fp16 SDF, f64 contacts",
-         "fp64": "f64"}
+         "fp64": "f64", "fp32-bf16-learned": "bf16 network + f32 screen on bf16 SDF, f64 contacts"}
+LEARN = {"iterations": 4000, "batch": 4096, "samples": 1 << 17, "lr": 3e-3}
 
 
 def _package():
@@ -164,7 +165,7 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000, devic
                 "initial_state": f"random sequential addition, deep overlaps re-placed ({iters} passes)"}
 
 
-def load(lsdem, sc, workload, device, prec):
+def load(lsdem, sc, workload, device, prec, learned=False, info=None):
     from lsdem_b200 import scenes
     sv = lsdem.Solver(device=device)
     if workload == "small":
@@ -173,10 +174,19 @@ def load(lsdem, sc, workload, device, prec):
         scenes.load_polydisperse(sv, sc)
     sv.set_precision(prec)
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
+    if learned:
+        t0 = time.perf_counter()
+        loss, err = sv.train_learned_sdf(**LEARN)
+        sv.set_learned_sdf(True)
+        if info is not None:
+            info["training"] = dict(LEARN, seconds=round(time.perf_counter() - t0, 3), loss=loss.tolist(),
+                                    err_over_R=[sv.learned_sdf(k)[1]["err"] / sv.learned_sdf(k)[1]["R"]
+                                                for k in range(len(loss))],
+                                    threshold_h=[sv.learned_sdf(k)[1]["threshold_h"] for k in range(len(loss))])
     return sv
 
 
-def force_error(lsdem, sc, workload, device, prec, warm=20):
+def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
     """Force / torque error of an FP32 form against the FP64 path, from the same state: both
     run `warm` FP64 steps, then one step each; forces are captured in the external hook."""
     import torch
@@ -186,7 +196,7 @@ def force_error(lsdem, sc, workload, device, prec, warm=20):
     st = sv.state()
     sv.close()
     for p in (0, prec):
-        sv = load(lsdem, sc, workload, device, p)
+        sv = load(lsdem, sc, workload, device, p, learned=learned and p != 0)
         sv.set_state(pos=st["pos"], vel=st["vel"], angvel=st["angvel"], quat=st["quat"])
         box = {}
         sv.step(sc["dt"], 1, hook=lambda t, sv=sv: box.update(sv.state()))
@@ -265,13 +275,14 @@ def run_reference(args, rank, world):
 L2_FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 
 
-def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
+def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learned=False):
     """W warm-up steps, then exactly K timed steps, each bracketed by CUDA events on the
     solver's stream with a 256 MB scratch write before it (outside the events) so that no
     step starts from data the previous one left in L2; the state backup of each batch of
     steps is timed with the batch's first step. Max over ranks. A second run of K steps
     timed as a whole, L2 not flushed, is reported beside it (`warm_l2`)."""
-    sv = load(lsdem, sc, args.workload, local, prec)
+    info = {}
+    sv = load(lsdem, sc, args.workload, local, prec, learned=learned, info=info)
     dt = float(sc["dt"])
     if clocks is not None:
         clocks.__enter__()  # the sampler starts up during the warm-up
@@ -291,7 +302,7 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks):
     assert step_calls == args.steps, (step_calls, args.steps)
     sv.set_step_timing(False)
     res = {"ms": step_ms, "launches": sv.num(8) - launches0, "reruns": sv.num(7) - reruns0,
-           "stats": sv.step_stats()}
+           "stats": sv.step_stats(), **info}
     # the same number of steps timed as one region, L2 not flushed
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -365,7 +376,7 @@ def main():
 
     prec = FORMS[args.form]
     clk = Clocks(local)
-    sv, head = time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clk)
+    sv, head = time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clk, learned="learned" in args.form)
     n = sv.n_particles
     value = n * world * args.steps / (head["ms"] * 1e-3)
 
@@ -400,14 +411,17 @@ def main():
         for name, p in FORMS.items():
             if name == args.form:
                 continue
-            svf, r = time_form(lsdem, torch, sc, args, local, p, dist, barrier, None)
+            svf, r = time_form(lsdem, torch, sc, args, local, p, dist, barrier, None, learned="learned" in name)
             svf.close()
             forms[name] = {"value": n * world * args.steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / args.steps,
                            "warm_l2": {"value": n * world * args.steps / (r["warm_ms"] * 1e-3),
                                        "ms_per_step": r["warm_ms"] / args.steps}}
+            if "training" in r:
+                forms[name]["training"] = r["training"]
+                forms[name]["screen_per_step"] = r.get("screen")
         for name, p in FORMS.items():
             if p != 0:
-                err = force_error(lsdem, sc, args.workload, local, p)
+                err = force_error(lsdem, sc, args.workload, local, p, learned="learned" in name)
                 forms.setdefault(name, {})["error_vs_fp64"] = err
 
     if rank == 0:

@@ -204,10 +204,43 @@ int lsdem_set_step_timing(lsdem_solver* s, int on, long long l2_flush_bytes);
 int lsdem_step_stats(lsdem_solver* s, long long* out4);
 /* Precision forms: counters of the FP32 screen summed over all steps run while
  * enabled (no counterpart in the reference): pairs screened, clusters tested,
- * clusters kept by the bounding cull, clusters kept by the SDF cull, node tests,
- * nodes queued for the FP64 test. Enabling resets them; off by default. */
+ * clusters kept by the culls, 16-bit grid lookups of nodes, node tests, nodes
+ * queued for the FP64 test, network evaluations of nodes (learned SDF), 0.
+ * Enabling resets them; off by default. */
 int lsdem_set_screen_stats(lsdem_solver* s, int on);
-int lsdem_get_screen_stats(lsdem_solver* s, long long* out6);
+int lsdem_get_screen_stats(lsdem_solver* s, long long* out8);
+
+/* Learned per-shape SDF (no counterpart in the reference). After lsdem_initialize,
+ * trains one 3-64-64-1 SiLU network per shape template on the GPU (own forward,
+ * backward and Adam kernels; FP32 master weights) on `samples` points of the
+ * template's grid box (half uniform, half near the surface) with FP64 grid targets,
+ * `iterations` Adam steps of `batch` points (a multiple of 128) at learning rate lr
+ * (cosine schedule), then measures each network's largest error against the grid
+ * over all grid nodes and `samples` further points, with the BF16 tensor-core
+ * inference code of the narrowphase. loss_out[shape]: mean squared error of
+ * phi / R of the last batch (R: half the largest grid extent); err_out[shape]: the
+ * measured bound (template units). Either may be NULL. */
+int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samples, double lr,
+                            unsigned long long seed, double* loss_out, double* err_out);
+/* Precision forms: when on, the screen rejects a node by the network where
+ * phi_net exceeds the trust band delta (2 % of the shape size) plus 1.25 x the
+ * measured one-sided error max(phi_net - phi_grid) over the validation points with
+ * phi_grid <= delta; every other node goes on to the grid screen and the FP64 test. */
+int lsdem_set_learned_sdf(lsdem_solver* s, int on);
+/* FP32 weights of a shape's network (LSDEM_MLP_PARAMS floats: W1[64][3], b1[64],
+ * W2[64][64], b2[64], w3[64], b3, padding) and norm[8] = centre xyz, R, measured
+ * error max |phi_net - phi_grid|, network threshold in template spacings, one-sided
+ * error inside the trust band, trust band (template units). */
+#define LSDEM_MLP_PARAMS 4484
+int lsdem_get_learned_sdf(lsdem_solver* s, int shape, float* params, float* norm);
+/* The network of `shape` at n template-frame points (double xyz), through the
+ * narrowphase's inference code: phi in template units. */
+int lsdem_mlp_eval(lsdem_solver* s, int shape, int n, const double* pts, float* phi);
+/* Gradient check support: loss (mean squared error) and its gradient with respect
+ * to the LSDEM_MLP_PARAMS weights over n points (n a multiple of 128; pts: x, y, z,
+ * target per point), computed by the training kernel on `device`; y (optional):
+ * the FP32 forward output per point. */
+int lsdem_mlp_gradient(int device, int n, const float* params, const float* pts, float* loss, float* grad, float* y);
 
 /* Scene set-up helper: random sequential addition of spheres (in the given
  * order) in [lo, hi), periodic or not (the reference's sphere-packing helper,

@@ -47,6 +47,7 @@ P = C.c_void_p
 DP = C.POINTER(C.c_double)
 IP = C.POINTER(C.c_int)
 LP = C.POINTER(C.c_longlong)
+FP = C.POINTER(C.c_float)
 HOOK = C.CFUNCTYPE(None, C.c_void_p, C.c_double)
 
 _SIGS = {
@@ -96,6 +97,11 @@ _SIGS = {
     "lsdem_step_stats": (C.c_int, [P, LP]),
     "lsdem_set_screen_stats": (C.c_int, [P, C.c_int]),
     "lsdem_set_step_timing": (C.c_int, [P, C.c_int, C.c_longlong]),
+    "lsdem_train_learned_sdf": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, DP, DP]),
+    "lsdem_set_learned_sdf": (C.c_int, [P, C.c_int]),
+    "lsdem_get_learned_sdf": (C.c_int, [P, C.c_int, FP, FP]),
+    "lsdem_mlp_eval": (C.c_int, [P, C.c_int, C.c_int, DP, FP]),
+    "lsdem_mlp_gradient": (C.c_int, [C.c_int, C.c_int, FP, FP, FP, FP, FP]),
     "lsdem_get_screen_stats": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
@@ -128,6 +134,24 @@ def _dp(a):  # pointer into a writable float64 array
 
 def _ip(a):
     return None if a is None else a.ctypes.data_as(IP)
+
+
+MLP_PARAMS = 4484
+
+
+def mlp_gradient(params, pts, device=0):
+    """Loss (mean squared error), its gradient and the FP32 forward output of one network
+    over points (n x 4: x, y, z, target; n a multiple of 128), from the training kernel."""
+    params = np.ascontiguousarray(params, np.float32)
+    pts = np.ascontiguousarray(pts, np.float32)
+    loss = np.zeros(1, np.float32)
+    grad = np.zeros(MLP_PARAMS, np.float32)
+    y = np.zeros(len(pts), np.float32)
+    rc = lib.lsdem_mlp_gradient(int(device), len(pts), params.ctypes.data_as(FP), pts.ctypes.data_as(FP),
+                                loss.ctypes.data_as(FP), grad.ctypes.data_as(FP), y.ctypes.data_as(FP))
+    if rc:
+        raise LSDEMError(rc, "mlp_gradient")
+    return float(loss[0]), grad, y
 
 
 def pack_rsa(radius, lo, hi, periodic=False, seed=12345, max_tries=1000, keep=None, pos=None):
@@ -396,14 +420,40 @@ class Solver:
         self._chk(lib.lsdem_step_stats(self.h, o.ctypes.data_as(LP)), "step_stats")
         return {"pairs_particle": int(o[0]), "pairs_wall": int(o[1]), "pairs_ghost": int(o[2]), "contacts": int(o[3])}
 
-    SCREEN_COUNTERS = ("pairs", "clusters", "clusters_bounding_cull", "clusters_sdf_cull", "node_tests",
-                       "nodes_queued")
+    # ---- learned per-shape SDF ---------------------------------------------------
+    def train_learned_sdf(self, iterations=3000, batch=4096, samples=1 << 18, lr=3e-3, seed=12345):
+        """Trains one network per shape template; returns (loss, err) per shape (err in template units)."""
+        ns = self.num(4)
+        loss, err = np.zeros(ns), np.zeros(ns)
+        self._chk(lib.lsdem_train_learned_sdf(self.h, int(iterations), int(batch), int(samples), float(lr), int(seed),
+                                              _dp(loss), _dp(err)), "train_learned_sdf")
+        return loss, err
+
+    def set_learned_sdf(self, on=True):
+        self._chk(lib.lsdem_set_learned_sdf(self.h, 1 if on else 0), "set_learned_sdf")
+
+    def learned_sdf(self, shape):
+        params = np.zeros(MLP_PARAMS, np.float32)
+        norm = np.zeros(8, np.float32)
+        self._chk(lib.lsdem_get_learned_sdf(self.h, int(shape), params.ctypes.data_as(FP), norm.ctypes.data_as(FP)),
+                  "get_learned_sdf")
+        return params, {"centre": norm[:3].astype(np.float64), "R": float(norm[3]), "err": float(norm[4]),
+                        "threshold_h": float(norm[5]), "err_in": float(norm[6]), "delta": float(norm[7])}
+
+    def mlp_eval(self, shape, pts):
+        pts = np.ascontiguousarray(pts, np.float64)
+        phi = np.zeros(len(pts), np.float32)
+        self._chk(lib.lsdem_mlp_eval(self.h, int(shape), len(pts), _dp(pts), phi.ctypes.data_as(FP)), "mlp_eval")
+        return phi
+
+    SCREEN_COUNTERS = ("pairs", "clusters", "clusters_kept", "grid_lookups", "node_tests", "nodes_queued",
+                       "net_evals", "unused")
 
     def set_screen_stats(self, on=True):
         self._chk(lib.lsdem_set_screen_stats(self.h, 1 if on else 0), "set_screen_stats")
 
     def screen_stats(self):
-        o = np.zeros(6, np.int64)
+        o = np.zeros(8, np.int64)
         self._chk(lib.lsdem_get_screen_stats(self.h, o.ctypes.data_as(LP)), "get_screen_stats")
         return dict(zip(self.SCREEN_COUNTERS, (int(v) for v in o)))
 

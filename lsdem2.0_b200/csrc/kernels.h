@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "common.cuh"
+#include "mlp.cuh"
 
 namespace lsdem {
 
@@ -170,10 +171,37 @@ struct StepArgs {
   double rmax;      // largest particle bounding radius
   MaybeView mb;
   PairLists pl;
-  // precision form, optional: screen counters (pairs, clusters tested, after the
-  // bounding cull, after the SDF cull, node tests, nodes queued for FP64)
+  // precision form, optional: screen counters (pairs, clusters tested, clusters
+  // kept, 16-bit grid lookups of nodes, node tests, nodes queued for FP64,
+  // network evaluations of nodes)
   unsigned long long* screen_stats;
+  // precision forms, optional: learned per-shape SDF in front of the grid screen
+  const MlpInfer* mlp_inf;   // per shape (nullptr: off)
+  const MlpNorm* mlp_norm;   // per shape
+  const float* mlp_band;     // per shape: trust band + error bound, in template spacings
 };
+
+// Template data for the learned-SDF kernels (mlp.cu).
+struct MlpShapeData {
+  const MlpNorm* norm;
+  const int3* gsize;
+  const double3* origin;   // template grid origin
+  const double* h;         // template grid spacing
+  const double* sdf;
+  const long long* sdf_off;
+  const int* node_off;
+  const int* node_cnt;
+  const double3* node_pos;
+};
+void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long seed, float4* samples, cudaStream_t st);
+cudaError_t mlp_train_step(float* params, const float4* samples, int nshapes, int S, int B, long long it,
+                           float* partial, float* loss, float* m1, float* m2, float lr, int step, cudaStream_t st);
+void mlp_pack(const float* params, int nshapes, MlpInfer* out, cudaStream_t st);
+void mlp_validate(const MlpShapeData& D, int nshapes, const MlpInfer* inf, int S2, unsigned long long seed,
+                  const float* delta, unsigned* err_bits, cudaStream_t st);
+cudaError_t mlp_grad_once(const float* params, const float4* pts, int n, float* partial, float* loss, cudaStream_t st);
+void mlp_forward(const float* params, const float4* pts, int n, float* y, cudaStream_t st);
+void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, cudaStream_t st);
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);
 void launch_candidates(const StepArgs& a, cudaStream_t s);

@@ -319,6 +319,17 @@ struct lsdem_solver {
   DArr<int> mb_node, mb_ctr;
   DArr<int> plist[3], pl_ctr;
   DArr<unsigned long long> scr_stats;  // screen counters (allocated while enabled)
+  // learned per-shape SDF (precision forms)
+  DArr<float> mlp_params, mlp_m1, mlp_m2, mlp_partial, mlp_loss, mlp_band;
+  DArr<float4> mlp_samples;
+  DArr<MlpInfer> mlp_inf;
+  DArr<MlpNorm> mlp_norm;
+  DArr<double3> mlp_origin;
+  DArr<double> mlp_h;
+  DArr<unsigned> mlp_err;
+  std::vector<MlpNorm> h_mlp_norm;
+  std::vector<float> h_mlp_band;
+  bool mlp_trained = false, mlp_on = false;
   DArr<int4> mb_pair;
   long long mb_cap = 0, mb_pcap = 0;
   std::vector<int> h_node_off, h_cl_off;
@@ -851,6 +862,10 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   for (int k = 0; k < 3; ++k) a.pl.list[k] = s->plist[k].p;
   a.pl.ctr = s->precision == PREC_FP64 ? nullptr : s->pl_ctr.p;
   a.screen_stats = s->scr_stats.p;
+  const bool learned = s->mlp_on && s->mlp_trained && s->precision != PREC_FP64;
+  a.mlp_inf = learned ? s->mlp_inf.p : nullptr;
+  a.mlp_norm = s->mlp_norm.p;
+  a.mlp_band = s->mlp_band.p;
   return a;
 }
 
@@ -1313,6 +1328,195 @@ int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3,
                        initial_length, youngs, poisson, tensile, cohesion, mu);
 }
 
+// ---------------------------------------------------------------------------
+// Learned per-shape SDF
+
+MlpShapeData mlp_shape_data(lsdem_solver* s) {
+  MlpShapeData D;
+  D.norm = s->mlp_norm.p; D.gsize = s->s_gsize.p; D.origin = s->mlp_origin.p; D.h = s->mlp_h.p;
+  D.sdf = s->s_sdf.p; D.sdf_off = s->s_sdf_off.p; D.node_off = s->s_node_off.p; D.node_cnt = s->s_node_cnt.p;
+  D.node_pos = s->s_node_pos.p;
+  return D;
+}
+
+int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samples, double lr,
+                            unsigned long long seed, double* loss_out, double* err_out) {
+  if (!s || iterations < 1 || batch < 128 || batch % 128 != 0 || samples < batch || !(lr > 0.)) return LSDEM_ERR_ARG;
+  if (!s->ready) return fail(s, LSDEM_ERR_STATE, "lsdem_train_learned_sdf before lsdem_initialize");
+  return guard(s, [&] {
+    cudaStream_t st = s->stream;
+    const int ns = (int)s->shapes.size();
+    if (ns == 0) return LSDEM_OK;
+    // normalisation: centre and half the largest extent of each template's grid box
+    s->h_mlp_norm.assign(ns, MlpNorm{});
+    std::vector<double3> org(ns);
+    std::vector<double> hh(ns);
+    for (int k = 0; k < ns; ++k) {
+      const ShapeHost& sh = s->shapes[k];
+      double ext = 0.;
+      for (int a = 0; a < 3; ++a) ext = std::max(ext, (sh.size[a] - 1) * sh.h);
+      MlpNorm& nm = s->h_mlp_norm[k];
+      nm.cx = (float)(sh.origin[0] + 0.5 * (sh.size[0] - 1) * sh.h);
+      nm.cy = (float)(sh.origin[1] + 0.5 * (sh.size[1] - 1) * sh.h);
+      nm.cz = (float)(sh.origin[2] + 0.5 * (sh.size[2] - 1) * sh.h);
+      nm.R = (float)(0.5 * ext);
+      org[k] = make_double3(sh.origin[0], sh.origin[1], sh.origin[2]);
+      hh[k] = sh.h;
+    }
+    CK(s->mlp_norm.upload(s->h_mlp_norm.data(), ns, st));
+    CK(s->mlp_origin.upload(org.data(), ns, st));
+    CK(s->mlp_h.upload(hh.data(), ns, st));
+    // initial weights: Glorot-uniform, zero biases
+    std::vector<float> p0((size_t)ns * MLP_NP, 0.f);
+    uint64_t r = seed * 0x9e3779b97f4a7c15ull + 1;
+    auto uni = [&](double a) {
+      r ^= r << 13; r ^= r >> 7; r ^= r << 17;
+      return (float)(a * (2.0 * (double)(r >> 11) / 9007199254740992.0 - 1.0));
+    };
+    for (int k = 0; k < ns; ++k) {
+      float* P = &p0[(size_t)k * MLP_NP];
+      for (int i = 0; i < 192; ++i) P[MLP_W1 + i] = uni(std::sqrt(6.0 / (3 + 64)));
+      for (int i = 0; i < 4096; ++i) P[MLP_W2 + i] = uni(std::sqrt(6.0 / (64 + 64)));
+      for (int i = 0; i < 64; ++i) P[MLP_W3 + i] = uni(std::sqrt(6.0 / (64 + 1)));
+    }
+    CK(s->mlp_params.upload(p0.data(), p0.size(), st));
+    CK(s->mlp_m1.alloc(p0.size())); CK(s->mlp_m1.zero(st));
+    CK(s->mlp_m2.alloc(p0.size())); CK(s->mlp_m2.zero(st));
+    const int nblk = batch / 128;
+    CK(s->mlp_partial.alloc((size_t)ns * nblk * MLP_NP));
+    CK(s->mlp_loss.alloc((size_t)ns * nblk));
+    CK(s->mlp_samples.alloc((size_t)ns * samples));
+    const MlpShapeData D = mlp_shape_data(s);
+    mlp_samples(D, ns, samples, seed, s->mlp_samples.p, st);
+    CK(cudaGetLastError());
+    // Adam with a cosine learning-rate schedule down to 1 % of lr
+    for (int it = 0; it < iterations; ++it) {
+      const double c = 0.5 * (1.0 + std::cos(M_PI * it / (double)iterations));
+      const float lr_t = (float)(lr * (0.01 + 0.99 * c));
+      CK(mlp_train_step(s->mlp_params.p, s->mlp_samples.p, ns, samples, batch, it, s->mlp_partial.p, s->mlp_loss.p,
+                        s->mlp_m1.p, s->mlp_m2.p, lr_t, it + 1, st));
+    }
+    // loss of the last batch (mean squared error of phi / R, FP32 master weights)
+    std::vector<float> lb = dl(s->mlp_loss, (size_t)ns * nblk, st);
+    CK(s->mlp_inf.alloc(ns));
+    mlp_pack(s->mlp_params.p, ns, s->mlp_inf.p, st);
+    // trust band of each shape: 2 % of its size (twice its largest node distance)
+    std::vector<float> delta(ns);
+    for (int k = 0; k < ns; ++k) {
+      const ShapeHost& sh = s->shapes[k];
+      double rmax = 0.;
+      for (size_t i = 0; i + 2 < sh.nodes.size(); i += 3)
+        rmax = std::max(rmax, std::sqrt(sh.nodes[i] * sh.nodes[i] + sh.nodes[i + 1] * sh.nodes[i + 1] +
+                                        sh.nodes[i + 2] * sh.nodes[i + 2]));
+      delta[k] = (float)(0.02 * 2.0 * rmax);
+    }
+    DArr<float> ddelta;
+    CK(ddelta.upload(delta.data(), ns, st));
+    CK(s->mlp_err.alloc(2 * (size_t)ns)); CK(s->mlp_err.zero(st));
+    mlp_validate(D, ns, s->mlp_inf.p, samples, seed ^ 0x5eedf00dull, ddelta.p, s->mlp_err.p, st);
+    std::vector<unsigned> eb = dl(s->mlp_err, 2 * (size_t)ns, st);
+    CK(cudaStreamSynchronize(st));
+    s->h_mlp_band.assign(ns, 0.f);
+    for (int k = 0; k < ns; ++k) {
+      float e, ein;
+      std::memcpy(&e, &eb[2 * k], 4);
+      std::memcpy(&ein, &eb[2 * k + 1], 4);
+      s->h_mlp_norm[k].err = e;
+      s->h_mlp_norm[k].err_in = ein;
+      s->h_mlp_norm[k].delta = delta[k];
+      // network threshold in template spacings: the trust band plus 1.25 x the
+      // one-sided error there, so that phi_net above it means phi_grid > delta
+      const ShapeHost& sh = s->shapes[k];
+      s->h_mlp_band[k] = (float)((1.25 * ein + delta[k]) / sh.h);
+      double l = 0.;
+      for (int b = 0; b < nblk; ++b) l += lb[(size_t)k * nblk + b];
+      if (loss_out) loss_out[k] = l / batch;
+      if (err_out) err_out[k] = e;
+    }
+    CK(s->mlp_norm.upload(s->h_mlp_norm.data(), ns, st));
+    CK(s->mlp_band.upload(s->h_mlp_band.data(), ns, st));
+    CK(cudaStreamSynchronize(st));
+    s->mlp_trained = true;
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_set_learned_sdf(lsdem_solver* s, int on) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (on && !s->mlp_trained) return fail(s, LSDEM_ERR_STATE, "lsdem_set_learned_sdf before lsdem_train_learned_sdf");
+  s->mlp_on = on != 0;
+  return LSDEM_OK;
+}
+
+int lsdem_get_learned_sdf(lsdem_solver* s, int shape, float* params, float* norm) {
+  if (!s || shape < 0) return LSDEM_ERR_ARG;
+  if (!s->mlp_trained || shape >= (int)s->h_mlp_norm.size()) return fail(s, LSDEM_ERR_STATE, "no trained network");
+  return guard(s, [&] {
+    if (params)
+      CK(cudaMemcpy(params, s->mlp_params.p + (size_t)shape * MLP_NP, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost));
+    if (norm) {
+      const MlpNorm& n = s->h_mlp_norm[shape];
+      const float v[8] = {n.cx, n.cy, n.cz, n.R, n.err, s->h_mlp_band[shape], n.err_in, n.delta};
+      std::memcpy(norm, v, sizeof(v));
+    }
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_mlp_eval(lsdem_solver* s, int shape, int n, const double* pts, float* phi) {
+  if (!s || shape < 0 || n < 0 || (n && (!pts || !phi))) return LSDEM_ERR_ARG;
+  if (!s->mlp_trained || shape >= (int)s->h_mlp_norm.size()) return fail(s, LSDEM_ERR_STATE, "no trained network");
+  return guard(s, [&] {
+    DArr<double3> dp;
+    DArr<float> dphi;
+    CK(dp.upload((const double3*)pts, (size_t)n, s->stream));
+    CK(dphi.alloc((size_t)std::max(n, 1)));
+    mlp_infer(s->mlp_inf.p + shape, s->h_mlp_norm[shape], dp.p, n, dphi.p, s->stream);
+    CK(cudaGetLastError());
+    if (n) CK(cudaMemcpyAsync(phi, dphi.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_mlp_gradient(int device, int n, const float* params, const float* pts, float* loss, float* grad,
+                       float* y) {
+  if (n <= 0 || n % 128 != 0 || !params || !pts) return LSDEM_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return LSDEM_ERR_NODEVICE;
+  try {
+    DArr<float> dpar, dpart, dloss, dy;
+    DArr<float4> dpts;
+    CK(dpar.upload(params, MLP_NP, nullptr));
+    CK(dpts.upload((const float4*)pts, (size_t)n, nullptr));
+    const int nblk = n / 128;
+    CK(dpart.alloc((size_t)nblk * MLP_NP));
+    CK(dloss.alloc((size_t)nblk));
+    CK(mlp_grad_once(dpar.p, dpts.p, n, dpart.p, dloss.p, nullptr));
+    std::vector<float> part = dl(dpart, (size_t)nblk * MLP_NP, nullptr);
+    std::vector<float> lb = dl(dloss, (size_t)nblk, nullptr);
+    if (y) {
+      CK(dy.alloc((size_t)n));
+      mlp_forward(dpar.p, dpts.p, n, dy.p, nullptr);
+      CK(cudaMemcpy(y, dy.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
+    CK(cudaDeviceSynchronize());
+    if (grad)
+      for (int k = 0; k < MLP_NP; ++k) {
+        double g = 0.;
+        for (int b = 0; b < nblk; ++b) g += part[(size_t)b * MLP_NP + k];
+        grad[k] = k <= MLP_B3 ? (float)g : 0.f;
+      }
+    if (loss) {
+      double l = 0.;
+      for (float v : lb) l += v;
+      *loss = (float)(l / n);
+    }
+    return LSDEM_OK;
+  } catch (const Fail& e) {
+    return e.code;
+  }
+}
+
 int lsdem_set_precision(lsdem_solver* s, int mode) {
   if (!s || mode < PREC_FP64 || mode > PREC_FP32_BF16) return LSDEM_ERR_ARG;
   s->precision = mode;
@@ -1718,7 +1922,7 @@ int lsdem_set_screen_stats(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   return guard(s, [&] {
     if (on) {
-      CK(s->scr_stats.alloc(6));
+      CK(s->scr_stats.alloc(8));
       CK(s->scr_stats.zero(s->stream));
     } else {
       CK(cudaStreamSynchronize(s->stream));
@@ -1728,14 +1932,14 @@ int lsdem_set_screen_stats(lsdem_solver* s, int on) {
   });
 }
 
-int lsdem_get_screen_stats(lsdem_solver* s, long long* out6) {
-  if (!s || !out6) return LSDEM_ERR_ARG;
+int lsdem_get_screen_stats(lsdem_solver* s, long long* out8) {
+  if (!s || !out8) return LSDEM_ERR_ARG;
   return guard(s, [&] {
-    for (int k = 0; k < 6; ++k) out6[k] = 0;
+    for (int k = 0; k < 8; ++k) out8[k] = 0;
     if (!s->scr_stats.p) return LSDEM_OK;
-    auto c = dl(s->scr_stats, 6, s->stream);
+    auto c = dl(s->scr_stats, 8, s->stream);
     CK(cudaStreamSynchronize(s->stream));
-    for (int k = 0; k < 6; ++k) out6[k] = (long long)c[k];
+    for (int k = 0; k < 8; ++k) out8[k] = (long long)c[k];
     return LSDEM_OK;
   });
 }

@@ -717,6 +717,10 @@ struct PairF {
   int key;           // walls and images: the partner's cell key
   float RA[9];       // walls and images: R_A scale_A (world offsets of the nodes)
   float n1w;         // walls and images: error bound of the world node offset
+  // learned SDF: u = l * ms - mc (network input), phi / h = y * mtoh, threshold Tn
+  float ms, mtoh, Tn;
+  float3 mc;
+  int pshape;
 };
 
 // Rotation matrix columns of q (the images of the unit axes under rotate()).
@@ -785,6 +789,16 @@ LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int
     for (int k = 0; k < 9; ++k) F.RA[k] = ra[k] * scA;
     F.n1w = EPS_F * N1;
   }
+  F.pshape = pshape;
+  if (a.mlp_inf) {
+    // partner frame (length) -> template units (/ scale) -> network input
+    const MlpNorm nm = a.mlp_norm[pshape];
+    const double ht = 1.0 / (P.invh * P.sc);  // template spacing
+    F.ms = (float)(1.0 / (P.sc * nm.R));
+    F.mc = f3(nm.cx / nm.R, nm.cy / nm.R, nm.cz / nm.R);
+    F.mtoh = (float)(nm.R / ht);
+    F.Tn = a.mlp_band[pshape];
+  }
   return F;
 }
 
@@ -833,7 +847,7 @@ LD int window_state(const StepArgs& a, double3 x, float3 ra, float e0, int key) 
 // FP32 screen of one node (offset nd, template units): false only when the
 // FP64 test (node_hits) certainly rejects it.
 template <int KIND, int SDFK>
-LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd) {
+LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd, bool& looked) {
   const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
   if (KIND == KIND_PP) {
     if (l.x * l.x + l.y * l.y + l.z * l.z > F.R2) return false;
@@ -846,6 +860,7 @@ LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd)
   const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
   if (lo < -F.eg || hi >= F.eg) return false;
   if (lo < F.eg || hi >= -F.eg) return true;  // within the error of the grid boundary
+  looked = true;
   return !(phi16<SDFK>(F, gx, gy, gz) > F.T);  // NaN never rejects
 }
 
@@ -901,9 +916,9 @@ LD int partner_shape(const StepArgs& a, int pid) {
 // surviving clusters. The nodes the screen cannot reject are written, in node
 // order, to the precision-form node buffer and the pair is queued for
 // k_contacts_f; a pair without such nodes gets its empty contact segment here.
-template <int KIND, int SDFK>
+template <int KIND, int SDFK, bool LRN>
 LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* s_cl, unsigned* s_mask,
-                      unsigned (&cnt)[6]) {
+                      unsigned (&cnt)[7], __nv_bfloat16* sw2, int& staged) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
   const int shA = a.P.shape[A];
@@ -927,17 +942,56 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
     nsurv += __popc(m);
   }
-  cnt[0] += 1; cnt[1] += ncl; cnt[2] += nsurv; cnt[3] += nsurv;
+  cnt[0] += 1; cnt[1] += ncl; cnt[2] += nsurv;
   __syncwarp();
   int total = 0;
-  for (int k = 0; k < nsurv; ++k) {
-    const int ni = s_cl[k] * 32 + lane;
-    cnt[4] += min(32, nn - s_cl[k] * 32);
-    bool may = false;
-    if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, a.S.node_pos_f[n0 + ni]);
-    const unsigned m = __ballot_sync(FULL, may);
-    if (lane == 0) s_mask[k] = m;
-    total += __popc(m);
+  if (LRN) {
+    if (nsurv > 0 && staged != F.pshape) {  // this warp's copy of the partner network's W2
+      mlp_stage_w2(a.mlp_inf[F.pshape], sw2);
+      staged = F.pshape;
+    }
+    const MlpInfer& M = a.mlp_inf[F.pshape];
+    unsigned w1b[8];
+    if (nsurv > 0)
+      for (int nt = 0; nt < 8; ++nt) w1b[nt] = M.w1b[nt * 32 + lane];
+    for (int k = 0; k < nsurv; ++k) {
+      const int ni = s_cl[k] * 32 + lane;
+      cnt[4] += min(32, nn - s_cl[k] * 32);
+      const float4 nd = a.S.node_pos_f[n0 + min(ni, nn - 1)];
+      const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
+      bool adm;
+      if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
+      else adm = window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) != 0;
+      const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+      const float lo = fminf(gx, fminf(gy, gz));
+      const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+      const bool need = ni < nn && adm && !(lo < -F.eg || hi >= F.eg);
+      const bool edge = lo < F.eg || hi >= -F.eg;
+      bool may = false;
+      if (__any_sync(FULL, need)) {
+        // the network for the chunk (tensor cores); nodes it cannot reject go to the grid screen
+        const float y = mlp_eval_warp(M, w1b, sw2, fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y),
+                                      fmaf(l.z, F.ms, -F.mc.z));
+        const bool keep = need && !(y * F.mtoh > F.Tn);
+        cnt[6] += __popc(__ballot_sync(FULL, need));
+        cnt[3] += __popc(__ballot_sync(FULL, keep && !edge));
+        may = keep && (edge || !(phi16<SDFK>(F, gx, gy, gz) > F.T));
+      }
+      const unsigned m = __ballot_sync(FULL, may);
+      if (lane == 0) s_mask[k] = m;
+      total += __popc(m);
+    }
+  } else {
+    for (int k = 0; k < nsurv; ++k) {
+      const int ni = s_cl[k] * 32 + lane;
+      cnt[4] += min(32, nn - s_cl[k] * 32);
+      bool may = false, looked = false;
+      if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, a.S.node_pos_f[n0 + ni], looked);
+      cnt[3] += __popc(__ballot_sync(FULL, looked));
+      const unsigned m = __ballot_sync(FULL, may);
+      if (lane == 0) s_mask[k] = m;
+      total += __popc(m);
+    }
   }
   cnt[5] += total;
   __syncwarp();
@@ -980,34 +1034,40 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
 // One warp per listed pair: the flat pair lists of the kinds in KINDS, in
 // particle, wall, image order.
 // Particle-only screens fit 64 registers (8 blocks per SM); walls and images
-// need the window test's FP64 registers.
-template <int KINDS, int SDFK>
-__global__ void __launch_bounds__(NP_WARPS * 32, KINDS == 1 ? 8 : 5) k_screen_f(StepArgs a, int li) {
+// need the window test's FP64 registers, the learned screen the network's.
+template <int KINDS, int SDFK, bool LRN>
+__global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5)) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  __shared__ __align__(16) __nv_bfloat16 s_w2[LRN ? NP_WARPS : 1][LRN ? 64 * 72 : 8];
   const int warp = threadIdx.x >> 5;
+  int staged = -1;
+  __nv_bfloat16* sw2 = s_w2[LRN ? warp : 0];
   const int n0 = (KINDS & 1) ? min(a.pl.ctr[0], a.P.n * a.pp.cap) : 0;
   const int n1 = (KINDS & 2) && a.pw.cap > 0 ? min(a.pl.ctr[1], a.P.n * a.pw.cap) : 0;
   const int n2 = (KINDS & 4) ? min(a.pl.ctr[2], a.P.n * a.pgh.cap) : 0;
   const int tot = n0 + n1 + n2;
-  unsigned cnt[6] = {0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
+  unsigned cnt[7] = {0, 0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
   for (int e = blockIdx.x * NP_WARPS + warp; e < tot; e += gridDim.x * NP_WARPS) {
     if ((KINDS & 1) && e < n0) {
       const int idx = a.pl.list[0][e];
       const int A = idx / a.pp.cap;
-      screen_pair_f<KIND_PP, SDFK>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_mask[warp], cnt);
+      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_mask[warp], cnt,
+                                        sw2, staged);
     } else if ((KINDS & 2) && e < n0 + n1) {
       const int idx = a.pl.list[1][e - n0];
       const int A = idx / a.pw.cap;
-      screen_pair_f<KIND_WALL, SDFK>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_mask[warp], cnt);
+      screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_mask[warp], cnt,
+                                          sw2, staged);
     } else if (KINDS & 4) {
       const int idx = a.pl.list[2][e - n0 - n1];
       const int A = idx / a.pgh.cap;
-      screen_pair_f<KIND_GHOST, SDFK>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_mask[warp], cnt);
+      screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_mask[warp],
+                                           cnt, sw2, staged);
     }
   }
   if (a.screen_stats && (threadIdx.x & 31) == 0)
-    for (int k = 0; k < 6; ++k)
+    for (int k = 0; k < 7; ++k)
       if (cnt[k]) atomicAdd(&a.screen_stats[k], (unsigned long long)cnt[k]);
 }
 
@@ -1067,6 +1127,21 @@ static int num_sms() {
   return g_num_sms;
 }
 
+template <bool LRN>
+void launch_screen(const StepArgs& a, int kinds, int li, dim3 g, dim3 b, cudaStream_t s) {
+  if (a.precision == PREC_FP32_FP16) {
+    if (kinds == 3) k_screen_f<3, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 1) k_screen_f<1, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 4) k_screen_f<4, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
+    else k_screen_f<7, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
+  } else {
+    if (kinds == 3) k_screen_f<3, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 1) k_screen_f<1, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
+    else if (kinds == 4) k_screen_f<4, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
+    else k_screen_f<7, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
+  }
+}
+
 void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   if (a.P.n <= 0) return;
   int want = (a.P.n + NP_WARPS - 1) / NP_WARPS;
@@ -1083,17 +1158,8 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   // precision form: the screen over the flat pair lists (launch_contact_pass
   // follows it); the grid is sized for the device, the list length is on it
   const int li = kinds == 4 ? 1 : 0;
-  if (a.precision == PREC_FP32_FP16) {
-    if (kinds == 3) k_screen_f<3, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 1) k_screen_f<1, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 4) k_screen_f<4, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
-    else k_screen_f<7, PREC_FP32_FP16><<<g, b, 0, s>>>(a, li);
-  } else {
-    if (kinds == 3) k_screen_f<3, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 1) k_screen_f<1, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 4) k_screen_f<4, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
-    else k_screen_f<7, PREC_FP32_BF16><<<g, b, 0, s>>>(a, li);
-  }
+  if (a.mlp_inf) launch_screen<true>(a, kinds, li, g, b, s);
+  else launch_screen<false>(a, kinds, li, g, b, s);
 }
 
 void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s) {
