@@ -275,6 +275,16 @@ def run_reference(args, rank, world):
 L2_FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 
 
+def max_over_ranks(dist, value, device):
+    """Largest value over the ranks of the process group (identity without one)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learned=False):
     """W warm-up steps, then exactly K timed steps, each bracketed by CUDA events on the
     solver's stream with a 256 MB scratch write before it (outside the events) so that no
@@ -322,11 +332,8 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learne
     if prec != 0:
         res["screen"] = {k: v / res["profile_steps"] for k, v in sv.screen_stats().items()}
         sv.set_screen_stats(False)
-    if dist is not None:
-        for key in ("ms", "warm_ms"):
-            t = torch.tensor([res[key]], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            res[key] = float(t.item())
+    for key in ("ms", "warm_ms"):
+        res[key] = max_over_ranks(dist, res[key], "cuda")
     return sv, res
 
 
@@ -398,11 +405,7 @@ def main():
         assert lsdem.lib.lsdem_get_state(sv.h, dp(h["pos"]), dp(h["vel"]), dp(h["angvel"]), dp(h["quat"]),
                                          dp(h["force"]), dp(h["torque"])) == 0
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(dist, time.perf_counter() - t0, "cuda")
     e2e = n * world * args.e2e_steps / e2e_s
     sv.close()
 
