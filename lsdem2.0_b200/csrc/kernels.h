@@ -157,6 +157,8 @@ struct StepArgs {
   GridP wg;         // wall grid
   const int* cell_idx;    // particle grid: sorted particle index
   float4* cell_pk;        // particle grid, sorted order: FP32 centre and bounding radius
+  const int* cell_off;    // particle grid: sorted position of the first body of cell k at [k + 1]
+                          //   (bucket offsets of the cell sort, ncells + 3 entries)
   const int* cell_start;
   const int* cell_end;
   SlotView pp, pw, pgh;          // this step

@@ -826,6 +826,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
   a.cell_pk = s->cell_pk.p;
+  a.cell_off = s->bk_offs.p;
   auto sv = [](SlotsDev& d) {
     SlotView v;
     v.cap = d.cap; v.cnt = d.cnt.p; v.id = d.id.p; v.seg_start = d.seg_start.p; v.seg_cnt = d.seg_cnt.p;

@@ -141,27 +141,29 @@ __global__ void k_bucket_scatter(const int* __restrict__ key, int n, int ncells,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int b = bucket_of(key[i], ncells);
-  if (b == 0 || b == ncells + 1) return;  // placed in index order by k_special_buckets
+  // a special bucket longer than a warp can rank is placed in index order by k_special_buckets
+  if ((b == 0 || b == ncells + 1) && offs[b + 1] - offs[b] > 64) return;
   int p = offs[b] + atomicAdd(&fill[b], 1);
   sorted_idx[p] = i;
 }
 
 // Bodies outside every cell (bucket 0: key -1; last bucket: key past the last
-// cell) can be numerous, e.g. bodies that left a non-periodic domain, so they
-// are placed directly in ascending index order by one block walking the bodies
-// in tiles: two block-wide scans of the membership flags give each member its
-// rank. Exits at once when both buckets are empty.
+// cell) can be numerous, e.g. bodies that left a non-periodic domain. A special
+// bucket of up to 64 members is scattered and ranked like any other; a longer
+// one is placed directly in ascending index order by one block walking the
+// bodies in tiles: two block-wide scans of the membership flags give each
+// member its rank. Exits at once when neither bucket is longer than 64.
 __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells, const int* __restrict__ offs,
                                   int* __restrict__ sorted_idx) {
   __shared__ int sw[32];
   const int L = ncells + 1;
   const int n0 = offs[1] - offs[0], nL = offs[L + 1] - offs[L];
-  if (n0 == 0 && nL == 0) return;
+  if (n0 <= 64 && nL <= 64) return;
   int base0 = offs[0], baseL = offs[L];
   for (int t0 = 0; t0 < n; t0 += blockDim.x) {
     const int i = t0 + threadIdx.x;
     const int b = i < n ? bucket_of(key[i], ncells) : -1;
-    const int f0 = b == 0, fL = b == L;
+    const int f0 = b == 0 && n0 > 64, fL = b == L && nL > 64;
     int tot0, totL;
     const int r0 = block_exclusive_scan<int>(f0, sw, &tot0);
     const int rL = block_exclusive_scan<int>(fL, sw, &totL);
@@ -172,11 +174,8 @@ __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells
   }
 }
 
-// One thread per bucket: restore ascending particle order inside the bucket
-// (insertion sort for small buckets, deferred to k_bucket_big otherwise) and
-// write the cell range [start, end) of cell b - 1, -1 when empty
-// (findStartAndEnd, buildHashStartEnd.cu:47-67).
-// Cell ranges of every bucket, and the stable order inside each bucket (the
+// Cell ranges [start, end) of every cell (-1 when empty; findStartAndEnd,
+// buildHashStartEnd.cu:47-67) and the stable order inside each bucket, and the stable order inside each bucket (the
 // scatter leaves members in arbitrary order): one warp per bucket, members of
 // buckets up to 64 long are ranked by particle index in registers; longer
 // buckets go to k_bucket_big.
@@ -190,7 +189,8 @@ __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int nce
       start[b - 1] = L > 0 ? s : -1;
       end[b - 1] = L > 0 ? e : -1;
     }
-    if (L <= 1 || b == 0 || b == ncells + 1) continue;  // special buckets are already in index order
+    if (L <= 1) continue;
+    if ((b == 0 || b == ncells + 1) && L > 64) continue;  // placed in index order by k_special_buckets
     if (L > 64) {
       if (lane == 0) big_list[atomicAdd(big_count, 1)] = b;
       continue;

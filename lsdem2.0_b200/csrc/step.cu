@@ -187,29 +187,25 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
     const int cap = a.pp.cap;
     int* out = a.pp.id + (size_t)A * cap;
+    // the (up to) 3 cells of a row along x are contiguous in the sorted order
+    const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < a.pg.size.x - 1 ? c.x + 1 : a.pg.size.x - 1;
     for (int dz = -1; dz <= 1; ++dz) {
       const int z = c.z + dz;
       if (z < 0 || z >= a.pg.size.z) continue;
       for (int dy = -1; dy <= 1; ++dy) {
         const int y = c.y + dy;
         if (y < 0 || y >= a.pg.size.y) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int x = c.x + dx;
-          if (x < 0 || x >= a.pg.size.x) continue;
-          const int h = lin3(make_int3(x, y, z), a.pg.size);
-          const int st = a.cell_start[h];
-          if (st < 0) continue;
-          const int en = a.cell_end[h];
-          for (int k = st; k < en; ++k) {
-            const float4 pb = a.cell_pk[k];
-            const float dx = pb.x - xf.x, dy = pb.y - xf.y, dz = pb.z - xf.z;
-            const float R = (rf + pb.w) * (1.0f + 1e-5f) + 1e-6f * (n1a + fabsf(pb.x) + fabsf(pb.y) + fabsf(pb.z));
-            if (dx * dx + dy * dy + dz * dz > R * R) continue;
-            const int B = a.cell_idx[k];
-            if (B <= A) continue;
-            if (n < cap) out[n] = B;
-            ++n;
-          }
+        const int h0 = lin3(make_int3(x0, y, z), a.pg.size);
+        const int st = a.cell_off[h0 + 1], en = a.cell_off[h0 + (x1 - x0) + 2];
+        for (int k = st; k < en; ++k) {
+          const float4 pb = a.cell_pk[k];
+          const float dx = pb.x - xf.x, dy = pb.y - xf.y, dz = pb.z - xf.z;
+          const float R = (rf + pb.w) * (1.0f + 1e-5f) + 1e-6f * (n1a + fabsf(pb.x) + fabsf(pb.y) + fabsf(pb.z));
+          if (dx * dx + dy * dy + dz * dz > R * R) continue;
+          const int B = a.cell_idx[k];
+          if (B <= A) continue;
+          if (n < cap) out[n] = B;
+          ++n;
         }
       }
     }
