@@ -937,7 +937,7 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
       launch_periodic(a, s->periodic, st);
       launch_clamped_keys(a, s->key2.p, st);
       bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
-      launch_ghost_candidates(a, s->g2_idx.p, s->g2_start.p, s->g2_end.p, s->key2.p, st);
+      launch_ghost_candidates(a, s->g2_idx.p, w.offs, st);
     }
     { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
     if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
@@ -952,10 +952,10 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
   { PhaseTimer pt(s, 7); launch_kick(a, st); }
   // kernels launched by this step: kick/drift/keys, cell sort (9), packing + candidates,
   // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (8),
-  // image compaction + candidates, ghost narrowphase; bonds
+  // image compaction + packing + candidates, ghost narrowphase; bonds
   // (the precision form adds one contact pass per narrowphase)
   const int nf = s->precision == PREC_FP64 ? 0 : 1;
-  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 13 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 14 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
 }

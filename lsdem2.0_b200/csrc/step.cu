@@ -152,11 +152,12 @@ LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
   for (int j = 0; j < cnt; ++j) list[base + j] = A * cap + j;
 }
 
-// Centres and bounding radii in cell-sorted order, FP32, for the candidate walk.
-__global__ void k_pack_cells(StepArgs a) {
+// Centres and bounding radii in a sorted order (idx), FP32, for the candidate
+// walks (the particle grid's, then the image search's).
+__global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.P.n) return;
-  const int B = a.cell_idx[k];
+  const int B = idx[k];
   const double3 x = a.P.pos[B];
   a.cell_pk[k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)a.P.radius[B]);
 }
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
 
 void launch_candidates(const StepArgs& a, cudaStream_t s) {
   if (a.P.n <= 0) return;
-  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(a);
+  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, a.cell_idx);
   k_candidates<<<(a.P.n + 127) / 128, 128, 0, s>>>(a);
 }
 
@@ -1260,8 +1261,7 @@ LD int axis_hi(double p, double mn, double inv, int size, double r, int c) {
 // only reach G's cell window when A's clamped cell is within 2 cells of G's
 // cell, and only when A's bounding sphere reaches G's SDF grid box. The lanes
 // walk the occupants of those cells.
-__global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, const int* __restrict__ g2_start,
-                                   const int* __restrict__ g2_end) {
+__global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, const int* __restrict__ g2_off) {
   const int lane = threadIdx.x & 31;
   const int nvis = *a.G.count;
   const int n = a.P.n;
@@ -1287,21 +1287,24 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
     const int x0 = axis_lo(xg.x, g.mn.x, g.inv.x, g.size.x, reach, cx), x1 = axis_hi(xg.x, g.mn.x, g.inv.x, g.size.x, reach, cx);
     const int y0 = axis_lo(xg.y, g.mn.y, g.inv.y, g.size.y, reach, cy), y1 = axis_hi(xg.y, g.mn.y, g.inv.y, g.size.y, reach, cy);
     const int z0 = axis_lo(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz), z1 = axis_hi(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz);
+    const float3 xgf = make_float3((float)xg.x, (float)xg.y, (float)xg.z);
+    const float Rgf = (float)Rg, n1g = fabsf(xgf.x) + fabsf(xgf.y) + fabsf(xgf.z);
     for (int z = z0; z <= z1; ++z) {
       for (int y = y0; y <= y1; ++y) {
-        for (int x = x0; x <= x1; ++x) {
-          const int h = lin3(make_int3(x, y, z), g.size);
-          const int st = g2_start[h];
-          if (st < 0) continue;
-          const int en = g2_end[h];
+        // the cells x0..x1 of a row are contiguous in the sorted order
+        const int h0 = lin3(make_int3(x0, y, z), g.size);
+        const int st = g2_off[h0 + 1], en = g2_off[h0 + (x1 - x0) + 2];
+        {
           for (int k0 = st; k0 < en; k0 += 32) {
             const int k = k0 + lane;
             int slot = -1, A = 0;
             if (k < en) {
-              A = g2_idx[k];
-              const double3 xA = a.P.pos[A];
-              const double R = (a.P.radius[A] + Rg) * (1.0 + 1e-9) + coord_slack(xA, xg);
-              if (!(len2(xA - xg) > R * R)) {
+              // superset test on the FP32 copies (margin covers their rounding)
+              const float4 pa = a.cell_pk[k];
+              const float dx = pa.x - xgf.x, dy = pa.y - xgf.y, dz = pa.z - xgf.z;
+              const float R = (pa.w + Rgf) * (1.0f + 1e-5f) + 1e-6f * (n1g + fabsf(pa.x) + fabsf(pa.y) + fabsf(pa.z));
+              if (!(dx * dx + dy * dy + dz * dz > R * R)) {
+                A = g2_idx[k];
                 slot = atomicAdd(&a.pgh.cnt[A], 1);
                 if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
                 else atomicOr(&a.status->flags, OVF_GHOST);
@@ -1325,13 +1328,13 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
   if (lane == 0 && need > 0) atomicMax(&a.status->need_ghost, need);
 }
 
-void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_start, const int* g2_end,
-                             const int* /*g2_key*/, cudaStream_t s) {
+void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_off, cudaStream_t s) {
   long long n = (long long)a.G.nsets * a.P.n;
   if (n <= 0) return;
   k_ghost_compact<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, g2_idx);  // the candidate walk's copy is spent
   int blocks = num_sms() * 16;
-  k_ghost_candidates<<<blocks, 128, 0, s>>>(a, g2_idx, g2_start, g2_end);
+  k_ghost_candidates<<<blocks, 128, 0, s>>>(a, g2_idx, g2_off);
 }
 
 // ---------------------------------------------------------------------------
