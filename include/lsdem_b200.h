@@ -205,7 +205,8 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4);
 /* Precision forms: counters of the FP32 screen summed over all steps run while
  * enabled (no counterpart in the reference): pairs screened, clusters tested,
  * clusters kept by the culls, 16-bit grid lookups of nodes, node tests, nodes
- * queued for the FP64 test, network evaluations of nodes (learned SDF), 0.
+ * queued for the FP64 test, network evaluations of nodes (learned SDF), 8-node
+ * sub-clusters kept.
  * Enabling resets them; off by default. */
 int lsdem_set_screen_stats(lsdem_solver* s, int on);
 int lsdem_get_screen_stats(lsdem_solver* s, long long* out8);

@@ -447,7 +447,7 @@ class Solver:
         return phi
 
     SCREEN_COUNTERS = ("pairs", "clusters", "clusters_kept", "grid_lookups", "node_tests", "nodes_queued",
-                       "net_evals", "unused")
+                       "net_evals", "subclusters_kept")
 
     def set_screen_stats(self, on=True):
         self._chk(lib.lsdem_set_screen_stats(self.h, 1 if on else 0), "set_screen_stats")

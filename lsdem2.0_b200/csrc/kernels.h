@@ -41,6 +41,8 @@ struct ShapeView {
   const double3* node_pos;    // node store, cluster order, unscaled
   const int* node_orig;       // original node index within the shape
   const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
+  const float4* sub_sphere;   // 4 per cluster (same shape offsets x 4): spheres of 8 nodes,
+                              //   unscaled; radius < 0 for a sub-cluster past the last node
   const double* node_box;     // 8 per shape (unscaled): node bounding box lo xyz, hi xyz,
                               //   largest node distance from the body origin, 0
   // precision form: SDF values / template spacing in 16-bit floats (FP16 or BF16
@@ -175,7 +177,7 @@ struct StepArgs {
   PairLists pl;
   // precision form, optional: screen counters (pairs, clusters tested, clusters
   // kept, 16-bit grid lookups of nodes, node tests, nodes queued for FP64,
-  // network evaluations of nodes)
+  // network evaluations of nodes, sub-clusters kept)
   unsigned long long* screen_stats;
   // precision forms, optional: learned per-shape SDF in front of the grid screen
   const MlpInfer* mlp_inf;   // per shape (nullptr: off)

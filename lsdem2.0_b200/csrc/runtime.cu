@@ -197,6 +197,7 @@ struct ShapeHost {
   double h;
   std::vector<int> perm;      // cluster position -> caller index
   std::vector<double> cl;     // 4 per cluster
+  std::vector<double> sub;    // 4 per sub-cluster of 8 nodes (4 sub-clusters per cluster)
   uint64_t hash;
 };
 
@@ -246,6 +247,24 @@ void build_clusters(ShapeHost& s) {
     }
     s.cl[4 * c] = m[0]; s.cl[4 * c + 1] = m[1]; s.cl[4 * c + 2] = m[2];
     s.cl[4 * c + 3] = r * (1.0 + 1e-12) + 1e-300;
+  }
+  // sub-clusters: 8 consecutive nodes each, 4 per cluster (a missing one has radius -1)
+  s.sub.assign(16 * (size_t)ncl, 0.0);
+  for (int q = 0; q < 4 * ncl; ++q) {
+    const int b = q * 8, e = std::min(M, b + 8);
+    if (b >= M) { s.sub[4 * q + 3] = -1.0; continue; }
+    double m[3] = {0, 0, 0};
+    for (int k = b; k < e; ++k)
+      for (int a = 0; a < 3; ++a) m[a] += s.nodes[3 * s.perm[k] + a];
+    for (int a = 0; a < 3; ++a) m[a] /= (e - b);
+    double r = 0;
+    for (int k = b; k < e; ++k) {
+      const double* p = &s.nodes[3 * s.perm[k]];
+      r = std::max(r, std::sqrt((p[0] - m[0]) * (p[0] - m[0]) + (p[1] - m[1]) * (p[1] - m[1]) +
+                                (p[2] - m[2]) * (p[2] - m[2])));
+    }
+    s.sub[4 * q] = m[0]; s.sub[4 * q + 1] = m[1]; s.sub[4 * q + 2] = m[2];
+    s.sub[4 * q + 3] = r * (1.0 + 1e-12) + 1e-300;
   }
 }
 
@@ -310,6 +329,7 @@ struct lsdem_solver {
   DArr<int> s_node_off, s_node_cnt, s_cl_off, s_cl_cnt, s_node_orig;
   DArr<double3> s_node_pos;
   DArr<double4> s_cl;
+  DArr<float4> s_sub;   // sub-cluster spheres, 4 per cluster (FP32, radius rounded up)
   DArr<double> s_nbox;  // per shape: node bounding box (lo xyz, hi xyz), largest node distance, 0
   DArr<uint4> s_cell16;        // precision form: 16-bit corners of every grid cell
   DArr<long long> s_cell_off;  // per shape, into s_cell16
@@ -655,6 +675,16 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
   {
+    std::vector<float4> sub;
+    for (const ShapeHost& sh : s->shapes)
+      for (size_t q = 0; q < sh.sub.size() / 4; ++q) {
+        const double r = sh.sub[4 * q + 3];
+        sub.push_back(make_float4((float)sh.sub[4 * q], (float)sh.sub[4 * q + 1], (float)sh.sub[4 * q + 2],
+                                  r < 0 ? -1.f : (float)(r * (1.0 + 1e-6)) + 1e-30f));
+      }
+    CK(s->s_sub.upload(sub.data(), sub.size(), st));
+  }
+  {
     std::vector<double> nbox;
     for (const ShapeHost& sh : s->shapes) {
       double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, r2 = 0.;
@@ -818,6 +848,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
   a.S.cl_sphere = s->s_cl.p;
   a.S.node_box = s->s_nbox.p;
+  a.S.sub_sphere = s->s_sub.p;
   a.S.cell16 = s->s_cell16.p;
   a.S.cell_off = s->s_cell_off.p;
   a.S.node_pos_f = s->s_node_f.p;

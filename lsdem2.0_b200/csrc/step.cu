@@ -914,8 +914,9 @@ LD int partner_shape(const StepArgs& a, int pid) {
 // order, to the precision-form node buffer and the pair is queued for
 // k_contacts_f; a pair without such nodes gets its empty contact segment here.
 template <int KIND, int SDFK, bool LRN>
-LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* s_cl, unsigned* s_mask,
-                      unsigned (&cnt)[7], __nv_bfloat16* sw2, int& staged) {
+LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* s_cl, unsigned short* s_sub,
+                      unsigned* s_mask,
+                      unsigned (&cnt)[8], __nv_bfloat16* sw2, int& staged) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
   const int shA = a.P.shape[A];
@@ -939,21 +940,46 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
     nsurv += __popc(m);
   }
-  cnt[0] += 1; cnt[1] += ncl; cnt[2] += nsurv;
   __syncwarp();
+  // second level: sub-clusters of 8 nodes of the surviving clusters, compacted in
+  // ascending order; chunk k of the node loop is sub-clusters 4k .. 4k + 3
+  int nsub = 0;
+  for (int j0 = 0; j0 < 4 * nsurv; j0 += 32) {
+    const int j = j0 + lane;
+    bool keep = false;
+    int sid = 0;
+    if (j < 4 * nsurv) {
+      sid = s_cl[j >> 2] * 4 + (j & 3);
+      const float4 sp = a.S.sub_sphere[4 * cl0 + sid];
+      keep = sp.w >= 0.f && cluster_may_hit_f<KIND, SDFK>(F, sp, scA);
+    }
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) s_sub[nsub + __popc(m & lanemask_lt())] = (unsigned short)sid;
+    nsub += __popc(m);
+  }
+  const int nch = (nsub + 3) >> 2;
+  cnt[0] += 1; cnt[1] += ncl; cnt[2] += nsurv; cnt[7] += nsub;
+  __syncwarp();
+  // this lane's node in chunk k (nn when none)
+  auto node_of = [&](int k) {
+    const int j = 4 * k + (lane >> 3);
+    if (j >= nsub) return nn;
+    const int ni = s_sub[j] * 8 + (lane & 7);
+    return ni < nn ? ni : nn;
+  };
   int total = 0;
   if (LRN) {
-    if (nsurv > 0 && staged != F.pshape) {  // this warp's copy of the partner network's W2
+    if (nch > 0 && staged != F.pshape) {  // this warp's copy of the partner network's W2
       mlp_stage_w2(a.mlp_inf[F.pshape], sw2);
       staged = F.pshape;
     }
     const MlpInfer& M = a.mlp_inf[F.pshape];
     unsigned w1b[8];
-    if (nsurv > 0)
+    if (nch > 0)
       for (int nt = 0; nt < 8; ++nt) w1b[nt] = M.w1b[nt * 32 + lane];
-    for (int k = 0; k < nsurv; ++k) {
-      const int ni = s_cl[k] * 32 + lane;
-      cnt[4] += min(32, nn - s_cl[k] * 32);
+    for (int k = 0; k < nch; ++k) {
+      const int ni = node_of(k);
+      cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
       const float4 nd = a.S.node_pos_f[n0 + min(ni, nn - 1)];
       const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
       bool adm;
@@ -979,9 +1005,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
       total += __popc(m);
     }
   } else {
-    for (int k = 0; k < nsurv; ++k) {
-      const int ni = s_cl[k] * 32 + lane;
-      cnt[4] += min(32, nn - s_cl[k] * 32);
+    for (int k = 0; k < nch; ++k) {
+      const int ni = node_of(k);
+      cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
       bool may = false, looked = false;
       if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, a.S.node_pos_f[n0 + ni], looked);
       cnt[3] += __popc(__ballot_sync(FULL, looked));
@@ -1021,9 +1047,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   ok = __shfl_sync(FULL, ok, 0);
   if (!ok) return;
   int off = 0;
-  for (int k = 0; k < nsurv; ++k) {
+  for (int k = 0; k < nch; ++k) {
     const unsigned m = s_mask[k];
-    if ((m >> lane) & 1u) a.mb.node[start + off + __popc(m & lanemask_lt())] = s_cl[k] * 32 + lane;
+    if ((m >> lane) & 1u) a.mb.node[start + off + __popc(m & lanemask_lt())] = node_of(k);
     off += __popc(m);
   }
 }
@@ -1035,36 +1061,37 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
 template <int KINDS, int SDFK, bool LRN>
 __global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5)) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
+  __shared__ unsigned short s_sub[NP_WARPS][4 * MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
-  __shared__ __align__(16) __nv_bfloat16 s_w2[LRN ? NP_WARPS : 1][LRN ? 64 * 72 : 8];
+  extern __shared__ __align__(16) unsigned char s_dyn[];  // learned screen: W2 of each warp
   const int warp = threadIdx.x >> 5;
   int staged = -1;
-  __nv_bfloat16* sw2 = s_w2[LRN ? warp : 0];
+  __nv_bfloat16* sw2 = reinterpret_cast<__nv_bfloat16*>(s_dyn) + (LRN ? warp * 64 * 72 : 0);
   const int n0 = (KINDS & 1) ? min(a.pl.ctr[0], a.P.n * a.pp.cap) : 0;
   const int n1 = (KINDS & 2) && a.pw.cap > 0 ? min(a.pl.ctr[1], a.P.n * a.pw.cap) : 0;
   const int n2 = (KINDS & 4) ? min(a.pl.ctr[2], a.P.n * a.pgh.cap) : 0;
   const int tot = n0 + n1 + n2;
-  unsigned cnt[7] = {0, 0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
+  unsigned cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
   for (int e = blockIdx.x * NP_WARPS + warp; e < tot; e += gridDim.x * NP_WARPS) {
     if ((KINDS & 1) && e < n0) {
       const int idx = a.pl.list[0][e];
       const int A = idx / a.pp.cap;
-      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_mask[warp], cnt,
-                                        sw2, staged);
+      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_sub[warp], s_mask[warp],
+                                        cnt, sw2, staged);
     } else if ((KINDS & 2) && e < n0 + n1) {
       const int idx = a.pl.list[1][e - n0];
       const int A = idx / a.pw.cap;
-      screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_mask[warp], cnt,
-                                          sw2, staged);
+      screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_sub[warp], s_mask[warp],
+                                          cnt, sw2, staged);
     } else if (KINDS & 4) {
       const int idx = a.pl.list[2][e - n0 - n1];
       const int A = idx / a.pgh.cap;
-      screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_mask[warp],
-                                           cnt, sw2, staged);
+      screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_sub[warp],
+                                           s_mask[warp], cnt, sw2, staged);
     }
   }
   if (a.screen_stats && (threadIdx.x & 31) == 0)
-    for (int k = 0; k < 7; ++k)
+    for (int k = 0; k < 8; ++k)
       if (cnt[k]) atomicAdd(&a.screen_stats[k], (unsigned long long)cnt[k]);
 }
 
@@ -1124,18 +1151,31 @@ static int num_sms() {
   return g_num_sms;
 }
 
+template <int KINDS, int SDFK, bool LRN>
+void launch_screen_k(const StepArgs& a, int li, dim3 g, dim3 b, cudaStream_t s) {
+  const int dyn = LRN ? NP_WARPS * 64 * 72 * (int)sizeof(__nv_bfloat16) : 0;
+  if (LRN) {
+    static bool attr = false;  // per kernel instance
+    if (!attr) {
+      cudaFuncSetAttribute(k_screen_f<KINDS, SDFK, LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      attr = true;
+    }
+  }
+  k_screen_f<KINDS, SDFK, LRN><<<g, b, dyn, s>>>(a, li);
+}
+
 template <bool LRN>
 void launch_screen(const StepArgs& a, int kinds, int li, dim3 g, dim3 b, cudaStream_t s) {
   if (a.precision == PREC_FP32_FP16) {
-    if (kinds == 3) k_screen_f<3, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 1) k_screen_f<1, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 4) k_screen_f<4, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
-    else k_screen_f<7, PREC_FP32_FP16, LRN><<<g, b, 0, s>>>(a, li);
+    if (kinds == 3) launch_screen_k<3, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    else if (kinds == 1) launch_screen_k<1, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    else if (kinds == 4) launch_screen_k<4, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    else launch_screen_k<7, PREC_FP32_FP16, LRN>(a, li, g, b, s);
   } else {
-    if (kinds == 3) k_screen_f<3, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 1) k_screen_f<1, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
-    else if (kinds == 4) k_screen_f<4, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
-    else k_screen_f<7, PREC_FP32_BF16, LRN><<<g, b, 0, s>>>(a, li);
+    if (kinds == 3) launch_screen_k<3, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    else if (kinds == 1) launch_screen_k<1, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    else if (kinds == 4) launch_screen_k<4, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    else launch_screen_k<7, PREC_FP32_BF16, LRN>(a, li, g, b, s);
   }
 }
 
