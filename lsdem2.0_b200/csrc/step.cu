@@ -197,13 +197,14 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
         const int y = c.y + dy;
         if (y < 0 || y >= a.pg.size.y) continue;
         const int h0 = lin3(make_int3(x0, y, z), a.pg.size);
-        const int st = a.cell_off[h0 + 1], en = a.cell_off[h0 + (x1 - x0) + 2];
+        const int st = __ldg(a.cell_off + h0 + 1), en = __ldg(a.cell_off + h0 + (x1 - x0) + 2);
+#pragma unroll 4
         for (int k = st; k < en; ++k) {
-          const float4 pb = a.cell_pk[k];
+          const float4 pb = __ldg(a.cell_pk + k);  // read-only: loads may run ahead of the slot stores
           const float dx = pb.x - xf.x, dy = pb.y - xf.y, dz = pb.z - xf.z;
           const float R = (rf + pb.w) * (1.0f + 1e-5f) + 1e-6f * (n1a + fabsf(pb.x) + fabsf(pb.y) + fabsf(pb.z));
           if (dx * dx + dy * dy + dz * dz > R * R) continue;
-          const int B = a.cell_idx[k];
+          const int B = __ldg(a.cell_idx + k);
           if (B <= A) continue;
           if (n < cap) out[n] = B;
           ++n;
@@ -734,7 +735,7 @@ LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int
   // walls from their quaternion)
   float ra[9], rb[9];
   {
-    const float4 r0 = a.P.rotm[3 * A], r1 = a.P.rotm[3 * A + 1], r2 = a.P.rotm[3 * A + 2];
+    const float4 r0 = __ldg(a.P.rotm + 3 * A), r1 = __ldg(a.P.rotm + 3 * A + 1), r2 = __ldg(a.P.rotm + 3 * A + 2);
     ra[0] = r0.x; ra[1] = r0.y; ra[2] = r0.z; ra[3] = r1.x; ra[4] = r1.y; ra[5] = r1.z;
     ra[6] = r2.x; ra[7] = r2.y; ra[8] = r2.z;
   }
@@ -745,7 +746,7 @@ LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int
       rb[j] = (float)cb[j].x; rb[3 + j] = (float)cb[j].y; rb[6 + j] = (float)cb[j].z;
     }
   } else {
-    const float4 r0 = a.P.rotm[3 * pidx], r1 = a.P.rotm[3 * pidx + 1], r2 = a.P.rotm[3 * pidx + 2];
+    const float4 r0 = __ldg(a.P.rotm + 3 * pidx), r1 = __ldg(a.P.rotm + 3 * pidx + 1), r2 = __ldg(a.P.rotm + 3 * pidx + 2);
     rb[0] = r0.x; rb[1] = r0.y; rb[2] = r0.z; rb[3] = r1.x; rb[4] = r1.y; rb[5] = r1.z;
     rb[6] = r2.x; rb[7] = r2.y; rb[8] = r2.z;
   }
@@ -933,8 +934,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     const int c = c0 + lane;
     bool keep = false;
     if (c < ncl) {
-      const double4 sp = a.S.cl_sphere[cl0 + c];
-      keep = cluster_may_hit_f<KIND, SDFK>(F, make_float4((float)sp.x, (float)sp.y, (float)sp.z, (float)sp.w), scA);
+      const double2* sp = reinterpret_cast<const double2*>(a.S.cl_sphere + cl0 + c);
+      const double2 s0 = __ldg(sp), s1 = __ldg(sp + 1);
+      keep = cluster_may_hit_f<KIND, SDFK>(F, make_float4((float)s0.x, (float)s0.y, (float)s1.x, (float)s1.y), scA);
     }
     const unsigned m = __ballot_sync(FULL, keep);
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
@@ -950,7 +952,7 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     int sid = 0;
     if (j < 4 * nsurv) {
       sid = s_cl[j >> 2] * 4 + (j & 3);
-      const float4 sp = a.S.sub_sphere[4 * cl0 + sid];
+      const float4 sp = __ldg(a.S.sub_sphere + 4 * cl0 + sid);
       keep = sp.w >= 0.f && cluster_may_hit_f<KIND, SDFK>(F, sp, scA);
     }
     const unsigned m = __ballot_sync(FULL, keep);
@@ -980,7 +982,7 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     for (int k = 0; k < nch; ++k) {
       const int ni = node_of(k);
       cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
-      const float4 nd = a.S.node_pos_f[n0 + min(ni, nn - 1)];
+      const float4 nd = __ldg(a.S.node_pos_f + n0 + min(ni, nn - 1));
       const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
       bool adm;
       if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
@@ -1009,7 +1011,7 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
       const int ni = node_of(k);
       cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
       bool may = false, looked = false;
-      if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, a.S.node_pos_f[n0 + ni], looked);
+      if (ni < nn) may = node_may_hit_f<KIND, SDFK>(a, xA, F, __ldg(a.S.node_pos_f + n0 + ni), looked);
       cnt[3] += __popc(__ballot_sync(FULL, looked));
       const unsigned m = __ballot_sync(FULL, may);
       if (lane == 0) s_mask[k] = m;
@@ -1074,9 +1076,9 @@ __global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5))
   unsigned cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // warp-uniform screen counters
   for (int e = blockIdx.x * NP_WARPS + warp; e < tot; e += gridDim.x * NP_WARPS) {
     if ((KINDS & 1) && e < n0) {
-      const int idx = a.pl.list[0][e];
+      const int idx = __ldg(a.pl.list[0] + e);
       const int A = idx / a.pp.cap;
-      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, a.pp.id[idx], li, s_cl[warp], s_sub[warp], s_mask[warp],
+      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, __ldg(a.pp.id + idx), li, s_cl[warp], s_sub[warp], s_mask[warp],
                                         cnt, sw2, staged);
     } else if ((KINDS & 2) && e < n0 + n1) {
       const int idx = a.pl.list[1][e - n0];
@@ -1084,9 +1086,9 @@ __global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5))
       screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_sub[warp], s_mask[warp],
                                           cnt, sw2, staged);
     } else if (KINDS & 4) {
-      const int idx = a.pl.list[2][e - n0 - n1];
+      const int idx = __ldg(a.pl.list[2] + e - n0 - n1);
       const int A = idx / a.pgh.cap;
-      screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, a.pgh.id[idx], li, s_cl[warp], s_sub[warp],
+      screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, __ldg(a.pgh.id + idx), li, s_cl[warp], s_sub[warp],
                                            s_mask[warp], cnt, sw2, staged);
     }
   }
@@ -1340,11 +1342,11 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
             int slot = -1, A = 0;
             if (k < en) {
               // superset test on the FP32 copies (margin covers their rounding)
-              const float4 pa = a.cell_pk[k];
+              const float4 pa = __ldg(a.cell_pk + k);
               const float dx = pa.x - xgf.x, dy = pa.y - xgf.y, dz = pa.z - xgf.z;
               const float R = (pa.w + Rgf) * (1.0f + 1e-5f) + 1e-6f * (n1g + fabsf(pa.x) + fabsf(pa.y) + fabsf(pa.z));
               if (!(dx * dx + dy * dy + dz * dz > R * R)) {
-                A = g2_idx[k];
+                A = __ldg(g2_idx + k);
                 slot = atomicAdd(&a.pgh.cnt[A], 1);
                 if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
                 else atomicOr(&a.status->flags, OVF_GHOST);
