@@ -173,6 +173,12 @@ int lsdem_get_contacts(lsdem_solver* s, int kind, long long cap, long long* node
 /* Bond state: master/slave ids, bonded flag, Un, Us, Ub, Ut, max normal and
  * shear stress, bond point (addBondedForceTorqueKernel outputs). */
 int lsdem_get_bonds(lsdem_solver* s, int* ids2, int* bonded, double* state9);
+/* The constants of every bond as added (no counterpart in the reference, whose
+ * VBondedInteraction keeps them in its host mirrors, VBondedInteraction.h:74-195):
+ * B[4] stiffness coefficients, geo[5] radius, initial length, tensile strength,
+ * cohesion, friction coefficient, frames[24] master n1, n2, n3, local point, slave
+ * n1, n2, n3, local point. Any pointer may be NULL. */
+int lsdem_get_bond_params(lsdem_solver* s, double* B4, double* geo5, double* frames24);
 
 /* Device pointers (double3 arrays in particle order, AoS) for external-force
  * kernels: what LSParticle::force()/torque()/velocity()/angularVelocity()

@@ -97,6 +97,7 @@ _SIGS = {
     "lsdem_step_stats": (C.c_int, [P, LP]),
     "lsdem_set_screen_stats": (C.c_int, [P, C.c_int]),
     "lsdem_set_step_timing": (C.c_int, [P, C.c_int, C.c_longlong]),
+    "lsdem_get_bond_params": (C.c_int, [P, DP, DP, DP]),
     "lsdem_train_learned_sdf": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, DP, DP]),
     "lsdem_set_learned_sdf": (C.c_int, [P, C.c_int]),
     "lsdem_get_learned_sdf": (C.c_int, [P, C.c_int, FP, FP]),
@@ -389,6 +390,12 @@ class Solver:
                                          _ip(o["image"]), _dp(o["spring"]), _dp(g.get("point")), _dp(g.get("normal")),
                                          _dp(g.get("overlap")), _dp(g.get("en_n")), _dp(g.get("en_s"))),
                   "get_contacts")
+        return o
+
+    def bond_params(self):
+        nb = self.num(2)
+        o = {"B": np.zeros((nb, 4)), "geo": np.zeros((nb, 5)), "frames": np.zeros((nb, 24))}
+        self._chk(lib.lsdem_get_bond_params(self.h, _dp(o["B"]), _dp(o["geo"]), _dp(o["frames"])), "get_bond_params")
         return o
 
     def bonds(self):

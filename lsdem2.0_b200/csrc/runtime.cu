@@ -1886,6 +1886,15 @@ int lsdem_get_bonds(lsdem_solver* s, int* ids2, int* bonded, double* state9) {
   });
 }
 
+int lsdem_get_bond_params(lsdem_solver* s, double* B4, double* geo5, double* frames24) {
+  if (!s) return LSDEM_ERR_ARG;
+  const size_t nb = s->bonds.bonded.size();
+  if (B4 && nb) std::memcpy(B4, s->bonds.B.data(), sizeof(double) * 4 * nb);
+  if (geo5 && nb) std::memcpy(geo5, s->bonds.geo.data(), sizeof(double) * 5 * nb);
+  if (frames24 && nb) std::memcpy(frames24, s->bonds.frames.data(), sizeof(double) * 24 * nb);
+  return LSDEM_OK;
+}
+
 int lsdem_device_pointers(lsdem_solver* s, void** force, void** torque, void** vel, void** angvel, void** pos,
                           void** quat) {
   if (!s || !s->ready) return LSDEM_ERR_STATE;

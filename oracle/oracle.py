@@ -424,4 +424,9 @@ def model_from_solver(sv, with_walls=True):
         ws = sv.wall_state()
         walls = {"shape": wp["shape"], "pos": ws["pos"], "vel": ws["vel"], "angvel": ws["angvel"], "quat": ws["quat"],
                  "radius": wp["radius"], "mu": wp["mu"], "e": wp["e"], "origin": wp["origin"], "invh": wp["invh"]}
-    return {"shapes": shapes, "particles": particles, "walls": walls}
+    bonds = None
+    if sv.num(2):
+        b, bp = sv.bonds(), sv.bond_params()
+        bonds = {"ids": b["ids"], "B": bp["B"], "geo": bp["geo"], "frames": bp["frames"], "bonded": b["bonded"],
+                 "state": b["state"]}
+    return {"shapes": shapes, "particles": particles, "walls": walls, "bonds": bonds}
