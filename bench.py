@@ -1,7 +1,7 @@
 """Benchmark of the level-set DEM time step (particle-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload polydisperse|small] [--form fp32-bf16|fp32-fp16|fp64]
+                    [--workload polydisperse|small|bonded|drum|scale] [--form fp32-bf16|fp32-fp16|fp64]
 
 Workload (default "polydisperse", the precision-form configuration, which fits one
 GPU): 100,000 particles from 4 templates (ellipsoid 1:0.8:0.6, superquadric
@@ -17,6 +17,14 @@ are evaluated in FP64 (positions, integration, spring history stay FP64). The
 same run times the FP16-template form and the plain FP64 form (the reference's
 arithmetic, bit-exact pair lists) and states each precision form's force error
 against the FP64 path from the same state.
+
+Other workloads (--workload; each a stated configuration of the method, synthetic and seeded):
+"small" 2,000 ellipsoids (5, 4, 3 mm) falling on a floor, 32^3 grids, 1,000 nodes, dt 1e-6 s;
+"bonded" 50,000 aligned ellipsoids (2, 1.6, 1.2 mm) on a jittered HCP lattice with ~286,000
+V-bonds, floor and a top wall moving down at 0.1 m/s, dt 2e-7 s; "drum" 500,000 particles from
+64 superquadrics (64^3 grids, 1,500 nodes) in a drum of radius 0.15 m and length 0.1 m turning
+at 30 rpm (all shapes scaled by one factor so that they fit the drum); "scale" 2,000,000
+particles from 16 superquadrics (1,500 nodes) periodic in x and y with walls in z.
 
 One step = one full time step (half kick, drift, cell sort, candidates,
 narrowphase + contact forces, periodic images, half kick) of the whole scene.
@@ -145,6 +153,35 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000, devic
         sc = scenes.ellipsoid_falling(seed=scenes.seed_for(0) + rank)
         return sc, {"workload": "ellipsoids-2000-floor", "particles": 2000, "nodes_per_particle": 1000,
                     "sdf_grid": "32^3", "box_m": [0.2, 0.2, 0.4], "dt_s": 1e-6}
+    if workload == "bonded":
+        sc = scenes.bonded_hcp(lsdem, seed=scenes.seed_for(2) + rank)
+        return sc, {"workload": "bonded-hcp-50k-ellipsoids", "particles": len(sc["pos"]),
+                    "bonds": len(sc["bonds"]["master"]), "nodes_per_particle": 1000, "sdf_grid": "32^3",
+                    "lattice": "HCP mapped to aligned ellipsoids (2, 1.6, 1.2 mm), 5% gap, 2% jitter",
+                    "walls": "floor + top wall at -0.1 m/s", "dt_s": sc["dt"]}
+    if workload in ("drum", "scale"):
+        t0 = time.perf_counter()
+        if workload == "drum":
+            sc = scenes.drum(lsdem, n=particles if particles != 100_000 else 500_000,
+                             seed=scenes.seed_for(3) + rank, device=device)
+        else:
+            sc = scenes.settling_box(lsdem, n=particles if particles != 100_000 else 2_000_000,
+                                     seed=scenes.seed_for(4) + rank, device=device)
+        t_gen = time.perf_counter() - t0
+        iters = scenes.resolve_deep_overlaps(lsdem, sc, device=device)
+        n = len(sc["pos"])
+        T = sc["templates"]
+        cfg = {"workload": (f"drum-{n}-superquadrics-64" if workload == "drum" else f"settling-{n}-superquadrics-16"),
+               "particles": n, "templates": len(T), "nodes_per_particle": len(T[0]["nodes"]),
+               "sdf_grid": "x".join(str(int(v)) for v in np.max([t["size"] for t in T], axis=0)) + " (largest)",
+               "sdf_from": "mesh distance of 20480-triangle superquadric meshes, built on the GPU",
+               "setup_s": round(t_gen, 1), "dt_s": sc["dt"],
+               "initial_state": f"random sequential addition, deep overlaps re-placed ({iters} passes)"}
+        if workload == "drum":
+            cfg.update(drum="R 0.15 m, L 0.1 m, 30 rpm about x", size_factor=round(float(sc["size_factor"]), 4))
+        else:
+            cfg.update(box_m=round(float(sc["max"][0]), 4), periodic="xy", walls="z")
+        return sc, cfg
     cache = ROOT / "_build" / "templates_48_2000.npz"
     if cache.exists():
         T = list(np.load(cache, allow_pickle=True)["T"])
@@ -209,9 +246,11 @@ def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
             "force_max": float(np.abs(out[prec]["force"] - F64).max() / np.abs(F64).max())}
 
 
-def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
+def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_seconds=10.0, max_steps=200):
     """FP64 oracle step (the reference algorithm restated on the CPU, all host threads) on a
-    bounded sample: the particles inside a corner sub-box of the same scene."""
+    bounded sample: the particles inside a corner sub-box of the same scene (for the bonded,
+    drum and settling workloads the cluster of particles nearest the median position). At least
+    `steps` steps are timed, and more until `min_seconds` of CPU work (at most `max_steps`)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as ora  # the checker, timed here as the CPU baseline
 
@@ -221,6 +260,15 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
     frac = min(1.0, (target_particles / n) ** (1.0 / 3.0))
     sub_hi = lo + (hi - lo) * frac
     idx = np.nonzero(np.all((pos >= lo) & (pos < sub_hi), axis=1))[0]
+    if workload in ("bonded", "drum", "scale"):
+        # a compact cluster of the particles nearest to the one closest to the median position
+        from scipy.spatial import cKDTree
+        tree = cKDTree(pos)
+        c = pos[tree.query(np.median(pos, axis=0))[1]]
+        idx = np.sort(tree.query(c, k=min(n, target_particles))[1])
+        r = float(np.max([t["bound"] for t in sc["templates"]]) * np.max(sc["scale"]))
+        lo, sub_hi = pos[idx].min(0) - 2 * r, pos[idx].max(0) + 2 * r
+        frac = len(idx) / n
     sv = lsdem.Solver()
     from lsdem_b200 import scenes
     if workload == "small":
@@ -237,6 +285,15 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
         sv.add_particles(np.asarray(ids, np.int32)[sub["shape"]], sub["pos"], sub["quat"], sub["inv_mass"],
                          sub["inv_inertia"], sub["kn"], sub["ks"], sub["mu"], sub["e"], vel=sub["vel"],
                          scale=sub["scale"])
+        b = sc.get("bonds")
+        if b is not None:
+            # the bonds among the sampled particles
+            where = np.full(n, -1)
+            where[idx] = np.arange(len(idx))
+            for k in np.nonzero((where[b["master"]] >= 0) & (where[b["slave"]] >= 0))[0]:
+                sv.add_bond(int(where[b["master"][k]]), int(where[b["slave"][k]]), b["point"][k], b["normal"][k],
+                            b["radius"][k], b["length"][k], b["youngs"], b["poisson"], b["tensile"][k],
+                            b["cohesion"][k], b["mu"])
         dmin, dmax = lo, sub_hi
     model = ora.model_from_solver(sv)
     model.update(domain=(dmin, dmax), gravity=sc["gravity"], periodic=0)
@@ -245,13 +302,18 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2):
     sim = ora.OracleSim(model, nthreads=threads)
     sim.step(sc["dt"])  # untimed first step (history)
     t0 = time.perf_counter()
-    for _ in range(steps):
+    done = 0
+    while done < steps or (time.perf_counter() - t0 < min_seconds and done < max_steps):
         sim.step(sc["dt"])
+        done += 1
     t = time.perf_counter() - t0
+    steps = done
     m = len(idx)
     return {"value": m * steps / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{m} particles of the same scene in a {frac:.3f}-scaled corner sub-box, {steps} steps "
-                      f"of the FP64 oracle (reference per-node 27-cell algorithm)"}
+            "sample": (f"{m} particles of the same scene in a {frac:.3f}-scaled corner sub-box, {steps} steps "
+                       f"of the FP64 oracle (reference per-node 27-cell algorithm)") if workload in ("small", "polydisperse")
+            else (f"{m} particles of the same scene (the cluster nearest its median position, with the bonds among "
+                  f"them), {steps} steps of the FP64 oracle (reference per-node 27-cell algorithm)")}
 
 
 def run_reference(args, rank, world):
@@ -343,7 +405,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="polydisperse", choices=["polydisperse", "small"])
+    ap.add_argument("--workload", default="polydisperse", choices=["polydisperse", "small", "bonded", "drum", "scale"])
     ap.add_argument("--form", default="fp32-bf16", choices=list(FORMS))
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")

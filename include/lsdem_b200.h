@@ -58,6 +58,27 @@ int lsdem_set_flags(lsdem_solver* s, int flags);
 int lsdem_mass_properties(const double* sdf, const int* size3, const double* origin3, double spacing,
                           double density, double* out16);
 
+/* Grid box of a level-set grid built around a triangle mesh with the given
+ * spacing and padding layers: the vertices' bounding box grown by max(1, pad)
+ * spacings, snapped outward to multiples of the spacing
+ * (LevelSetObject::Base::buildGrid, FunDEM/kernel/helper/LevelSetObjectGenerator.h:122-170).
+ * Host only. */
+int lsdem_mesh_grid_box(const double* verts, int n_verts, double spacing, int pad, double* origin3, int* size3);
+
+/* Level-set grid of a closed triangle mesh, computed on `device`: at every grid
+ * node the distance to the nearest triangle, negative inside by the solid-angle
+ * sum, divided by the gradient norm as buildGrid does (-+h/2 where that is
+ * <= 1e-12) — LevelSetObject::Base::buildGrid over
+ * TriangleMeshParticle::evaluateImplicitFunctionValueAndGradient
+ * (LevelSetObjectGenerator.h:122-224, 454-500, 758-802, 888-914).
+ * positive_inside = TriangleMeshParticle::setLevelSetPositiveInside. verts: n_verts
+ * x 3, tris: n_tris x 3 vertex indices, sdf_out: size3[0] x size3[1] x size3[2]
+ * values in the order ix + nx (iy + ny iz), host memory; blocking. LSDEM_ERR_ARG
+ * for a mesh the reference's isValid rejects (no vertices or triangles, an index
+ * out of range or repeated within a triangle). */
+int lsdem_mesh_grid(const double* verts, int n_verts, const int* tris, int n_tris, const double* origin3,
+                    const int* size3, double spacing, int positive_inside, double* sdf_out, int device);
+
 /* Registers a shape template (surface nodes in the body frame + SDF grid with
  * index ix + nx*(iy + ny*iz), phi < 0 inside). Identical templates are shared.
  * Replaces the per-particle copies appended by LSParticle::add (LSParticle.h:115-212). */

@@ -106,6 +106,8 @@ _SIGS = {
     "lsdem_get_screen_stats": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
+    "lsdem_mesh_grid_box": (C.c_int, [DP, C.c_int, C.c_double, C.c_int, DP, IP]),
+    "lsdem_mesh_grid": (C.c_int, [DP, C.c_int, IP, C.c_int, DP, IP, C.c_double, C.c_int, DP, C.c_int]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -177,6 +179,36 @@ def mass_properties(sdf, size, origin, spacing, density):
     if rc:
         raise LSDEMError(rc, "mass_properties")
     return {"mass": out[0], "centroid": out[1:4].copy(), "inertia": out[4:10].copy(), "inv_inertia": out[10:16].copy()}
+
+
+def mesh_grid_box(verts, spacing, pad=2):
+    """Origin and node counts of the grid buildGrid(spacing, pad) puts around a mesh
+    (LevelSetObjectGenerator.h:122-170)."""
+    v = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+    origin = np.zeros(3)
+    size = np.zeros(3, np.int32)
+    rc = lib.lsdem_mesh_grid_box(_d(v), len(v), float(spacing), int(pad), _dp(origin), _ip(size))
+    if rc:
+        raise LSDEMError(rc, "mesh_grid_box")
+    return origin, size
+
+
+def mesh_grid(verts, tris, spacing, pad=2, positive_inside=False, device=0, origin=None, size=None):
+    """Level-set grid of a closed triangle mesh computed on the GPU (buildGrid over the mesh
+    distance with the solid-angle sign, LevelSetObjectGenerator.h:122-224, 454-500, 758-802).
+    Returns (sdf, size, origin) with sdf in the order ix + nx (iy + ny iz)."""
+    v = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    if origin is None or size is None:
+        origin, size = mesh_grid_box(v, spacing, pad)
+    origin = np.ascontiguousarray(origin, np.float64)
+    size = np.ascontiguousarray(size, np.int32)
+    out = np.zeros(int(np.prod(size.astype(np.int64))))
+    rc = lib.lsdem_mesh_grid(_d(v), len(v), _i(t), len(t), _d(origin), _i(size), float(spacing),
+                             1 if positive_inside else 0, _dp(out), int(device))
+    if rc:
+        raise LSDEMError(rc, "mesh_grid")
+    return out, size, origin
 
 
 class Solver:

@@ -22,6 +22,9 @@ LIB = HERE / "liblsdem_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-I", str(ROOT / "include")]
+# Per-file flags: the mesh grid builder rounds every product and sum separately, as the
+# reference's host generator does (no fused multiply-add contraction).
+FILE_FLAGS = {"sdfgen.cu": ["--fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -46,7 +49,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     for s in srcs:
         o = OBJ / (s.stem + ".o")
         if _stale(s, o) or ptxas_info:
-            cmd = [nvcc, *ARCH, *NVFLAGS, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc, *ARCH, *NVFLAGS, *FILE_FLAGS.get(s.name, []), "-c", str(s), "-o", str(o)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)

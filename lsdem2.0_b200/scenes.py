@@ -97,6 +97,136 @@ def make_ellipsoid(axes, n_grid=32, n_nodes=1000, pad=2):
     return {"nodes": nodes, "sdf": sdf, "size": size, "origin": origin, "spacing": h, "bound": float(axes.max())}
 
 
+def superellipsoid_value_gradient(p, axes, ee, en):
+    """Implicit function F = (|x/rx|^(2/ee) + |y/ry|^(2/ee))^(ee/en) + |z/rz|^(2/en) - 1 and its
+    gradient, as the reference's superellipsoid generator evaluates them
+    (FunDEM/kernel/helper/LevelSetObjectGenerator.h:1264-1341: |v|^e by pow, magnitudes floored
+    at 1e-30 in the derivatives, sign(0) = +1)."""
+    p = np.asarray(p, np.float64)
+    rx, ry, rz = (float(a) for a in axes)
+    exy, ez, outer = 2.0 / ee, 2.0 / en, ee / en
+    ax, ay, az = np.abs(p[:, 0] / rx), np.abs(p[:, 1] / ry), np.abs(p[:, 2] / rz)
+    sxy = ax ** exy + ay ** exy
+    F = sxy ** outer + az ** ez - 1.0
+    tiny = 1e-30
+    sgn = lambda v: np.where(v >= 0.0, 1.0, -1.0)
+    o1 = np.maximum(sxy, tiny) ** (outer - 1.0)
+    gx = outer * o1 * exy * np.maximum(ax, tiny) ** (exy - 1.0) * sgn(p[:, 0]) / rx
+    gy = outer * o1 * exy * np.maximum(ay, tiny) ** (exy - 1.0) * sgn(p[:, 1]) / ry
+    gz = ez * np.maximum(az, tiny) ** (ez - 1.0) * sgn(p[:, 2]) / rz
+    return F, np.stack([gx, gy, gz], 1)
+
+
+def make_superellipsoid(axes, ee, en, n_grid=64, n_nodes=1500, pad=2):
+    """Superellipsoid template with the reference generator's grid values: F / |grad F| at each
+    grid node, or -+h/2 where |grad F| <= 1e-12 (LevelSetObjectGenerator.h:185-205). Surface
+    nodes: Fibonacci directions u scaled onto the surface in closed form, t = S(u)^(-en/2) with
+    S(u) = (|ux/rx|^(2/ee) + |uy/ry|^(2/ee))^(ee/en) + |uz/rz|^(2/en), the radial projection the
+    generator applies to its mesh vertices (LevelSetObjectGenerator.h:1013-1044). A single
+    exponent p for all axes is ee = en = 2/p."""
+    axes = np.asarray(axes, np.float64)
+    h, origin = grid_for(axes, n_grid, pad)
+    size = np.array([n_grid] * 3, np.int32)
+    F, g = superellipsoid_value_gradient(grid_points(size, origin, h), axes, ee, en)
+    gn = np.sqrt(g[:, 0] * g[:, 0] + g[:, 1] * g[:, 1] + g[:, 2] * g[:, 2])
+    sdf = np.where(gn > 1e-12, F / np.maximum(gn, 1e-300), np.where(F <= 0.0, -0.5 * h, 0.5 * h))
+    u = fibonacci_directions(n_nodes)
+    exy, ez, outer = 2.0 / ee, 2.0 / en, ee / en
+    S = (np.abs(u[:, 0] / axes[0]) ** exy + np.abs(u[:, 1] / axes[1]) ** exy) ** outer + np.abs(u[:, 2] / axes[2]) ** ez
+    nodes = u * (S ** (-0.5 * en))[:, None]
+    return {"nodes": nodes, "sdf": sdf, "size": size, "origin": origin, "spacing": h,
+            "bound": float(np.max(np.linalg.norm(nodes, axis=1)))}
+
+
+# The 12 vertices (before normalisation) and 20 faces of the regular icosahedron in the
+# numbering of the common icosphere construction, which the reference's superellipsoid
+# generator also uses (LevelSetObjectGenerator.h:1069-1118); the same numbering is kept so
+# that meshes come out vertex for vertex as the reference's.
+_GR = 0.5 * (1.0 + math.sqrt(5.0))
+_ICO_V = [(-1.0, _GR, 0.0), (1.0, _GR, 0.0), (-1.0, -_GR, 0.0), (1.0, -_GR, 0.0),
+          (0.0, -1.0, _GR), (0.0, 1.0, _GR), (0.0, -1.0, -_GR), (0.0, 1.0, -_GR),
+          (_GR, 0.0, -1.0), (_GR, 0.0, 1.0), (-_GR, 0.0, -1.0), (-_GR, 0.0, 1.0)]
+_ICO_F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+          (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+          (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+
+
+def _normalize_rows(v):
+    l2 = v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2]
+    inv = np.where(np.abs(l2) <= 1e-20, 0.0, 1.0 / np.sqrt(np.where(l2 > 0, l2, 1.0)))
+    return v * inv[:, None]
+
+
+def _orient_outward(v, f):
+    a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    centre = (a + b + c) * (1.0 / 3.0)
+    n = np.cross(b - a, c - a)
+    flip = (n * centre).sum(1) < 0.0
+    f[flip] = f[flip][:, [0, 2, 1]]
+    return f
+
+
+def superellipsoid_mesh(axes, ee, en, level=4):
+    """Closed triangle mesh of the superellipsoid (|x/rx|^(2/ee) + |y/ry|^(2/ee))^(ee/en) +
+    |z/rz|^(2/en) = 1 built as the reference's generator builds it
+    (LevelSetObjectGenerator.h:1013-1200): icosahedron on the unit sphere, `level` midpoint
+    subdivisions (each new vertex the normalised midpoint of an edge, created in triangle
+    order), triangles turned to face outward after every stage, then every vertex scaled
+    radially onto the surface by t = S(u)^(-en/2). Returns (vertices (n, 3), triangles (m, 3))."""
+    rx, ry, rz = (float(a) for a in axes)
+    v = _normalize_rows(np.array(_ICO_V, np.float64))
+    f = _orient_outward(v, np.array(_ICO_F, np.int64))
+    verts = [tuple(r) for r in v]
+    for _ in range(max(0, min(int(level), 8))):
+        cache = {}
+        out = np.empty((4 * len(f), 3), np.int64)
+        pend = []
+
+        def mid(i, j):
+            key = (i, j) if i < j else (j, i)
+            k = cache.get(key)
+            if k is None:
+                k = len(verts) + len(pend)
+                cache[key] = k
+                pend.append(key)
+            return k
+        for t, (i0, i1, i2) in enumerate(f.tolist()):
+            i01, i12, i20 = mid(i0, i1), mid(i1, i2), mid(i2, i0)
+            out[4 * t:4 * t + 4] = ((i0, i01, i20), (i1, i12, i01), (i2, i20, i12), (i01, i12, i20))
+        V = np.array(verts, np.float64)
+        pa = np.array(pend, np.int64).reshape(-1, 2)
+        m = _normalize_rows((V[pa[:, 0]] + V[pa[:, 1]]) * 0.5)
+        verts.extend(tuple(r) for r in m)
+        f = _orient_outward(np.array(verts, np.float64), out)
+    V = np.array(verts, np.float64)
+    l2 = V[:, 0] * V[:, 0] + V[:, 1] * V[:, 1] + V[:, 2] * V[:, 2]
+    d = V * (1.0 / np.sqrt(l2))[:, None]
+    exy, ez, outer = 2.0 / ee, 2.0 / en, ee / en
+    S = np.power(np.power(np.abs(d[:, 0] / rx), exy) + np.power(np.abs(d[:, 1] / ry), exy), outer) + \
+        np.power(np.abs(d[:, 2] / rz), ez)
+    V = d * np.power(S, -0.5 * en)[:, None]
+    f = _orient_outward(V, f)
+    return V, f.astype(np.int32)
+
+
+def make_mesh_template(lsdem, verts, tris, spacing, n_nodes_dirs=None, nodes=None, pad=2, device=0):
+    """Template from a closed triangle mesh: the level-set grid computed on the GPU by the
+    reference's buildGrid rule (lsdem.mesh_grid) and the given surface nodes."""
+    sdf, size, origin = lsdem.mesh_grid(verts, tris, spacing, pad=pad, device=device)
+    return {"nodes": np.asarray(nodes, np.float64), "sdf": sdf, "size": size, "origin": origin,
+            "spacing": float(spacing), "verts": np.asarray(verts), "tris": np.asarray(tris),
+            "bound": float(np.max(np.linalg.norm(nodes, axis=1)))}
+
+
+def superellipsoid_nodes(axes, ee, en, n_nodes):
+    """Fibonacci directions scaled radially onto the superellipsoid surface (closed form)."""
+    u = fibonacci_directions(n_nodes)
+    exy, ez, outer = 2.0 / ee, 2.0 / en, ee / en
+    S = (np.abs(u[:, 0] / axes[0]) ** exy + np.abs(u[:, 1] / axes[1]) ** exy) ** outer + \
+        np.abs(u[:, 2] / axes[2]) ** ez
+    return u * (S ** (-0.5 * en))[:, None]
+
+
 def _surface_along_rays(f, u, rmax, iters=60):
     lo = np.zeros(len(u))
     hi = np.full(len(u), rmax)
@@ -399,19 +529,269 @@ def resolve_deep_overlaps(lsdem, sc, threshold=0.02, exclusion=0.8, max_iter=40,
         bad = np.fromiter(bad, np.int64)
         keep = np.ones(n, np.int32)
         keep[bad] = 0
-        # re-placed spheres may come a little closer than the first packing (0.75 x radius)
-        rad = 0.5 * exclusion * sc["scale"]
-        rad = np.where(keep == 0, rad * (0.75 / exclusion), rad)
-        sc["pos"] = lsdem.pack_rsa(rad, sc["min"], sc["max"], periodic=bool(sc["periodic"]),
-                                   seed=int(rng.integers(1 << 62)), max_tries=20000, keep=keep, pos=sc["pos"])
+        if "rsa" in sc:
+            # scenes with their own packing spec: re-placed spheres 10 % smaller than the first packing
+            rsa = dict(sc["rsa"], radius=np.where(keep == 0, 0.9, 1.0) * sc["rsa"]["radius"])
+            sc["pos"] = _rsa(lsdem, rng, rsa, keep=keep, pos=sc["pos"])
+        else:
+            # re-placed spheres may come a little closer than the first packing (0.75 x radius)
+            rad = 0.5 * exclusion * sc["scale"]
+            rad = np.where(keep == 0, rad * (0.75 / exclusion), rad)
+            sc["pos"] = lsdem.pack_rsa(rad, sc["min"], sc["max"], periodic=bool(sc["periodic"]),
+                                       seed=int(rng.integers(1 << 62)), max_tries=20000, keep=keep, pos=sc["pos"])
         sc["quat"][bad] = random_quaternions(rng, len(bad))
     sv.close()
     return it
 
 
 def load_polydisperse(solver, sc):
+    """Adds a multi-template scene (this module's scene dicts) to a Solver: shapes, particles,
+    walls with their prescribed motion, bonds and the periodic axes."""
     ids = [solver.add_shape(t["nodes"], t["sdf"], t["size"], t["origin"], t["spacing"]) for t in sc["templates"]]
     shape = np.asarray(ids, np.int32)[sc["shape"]]
     solver.add_particles(shape, sc["pos"], sc["quat"], sc["inv_mass"], sc["inv_inertia"], sc["kn"], sc["ks"],
-                         sc["mu"], sc["e"], vel=sc["vel"], scale=sc["scale"])
+                         sc["mu"], sc["e"], vel=sc["vel"], angvel=sc.get("angvel"), scale=sc["scale"])
+    for w in sc.get("walls", ()):
+        k = solver.add_wall(w["verts"], w["sdf"], w["size"], w["origin"], w["spacing"], w["pos"], w["quat"], w["mu"],
+                            w["e"])
+        if w.get("vel") is not None:
+            solver.set_wall_velocity(k, w["vel"])
+        if w.get("angvel") is not None:
+            solver.set_wall_angular_velocity(k, w["angvel"])
+    b = sc.get("bonds")
+    if b is not None:
+        for k in range(len(b["master"])):
+            solver.add_bond(int(b["master"][k]), int(b["slave"][k]), b["point"][k], b["normal"][k], b["radius"][k],
+                            b["length"][k], b["youngs"], b["poisson"], b["tensile"][k], b["cohesion"][k], b["mu"])
     solver.set_periodic(sc["periodic"])
+
+
+# ---------------------------------------------------------------------------
+# Bonded, drum and large-scale workloads
+
+
+def _unit_density_templates(lsdem, T):
+    """Mass (= volume at density 1), inverse inertia and the frame moved to the centroid, from
+    each template's grid by the reference's smoothed-Heaviside integration (LSSolver.h:66-135)."""
+    out = []
+    for t in T:
+        mp = lsdem.mass_properties(t["sdf"], t["size"], t["origin"], t["spacing"], 1.0)
+        c = mp["centroid"]
+        out.append({"nodes": t["nodes"] - c, "sdf": t["sdf"], "size": t["size"], "origin": t["origin"] - c,
+                    "spacing": t["spacing"], "mass": mp["mass"], "inv_inertia": mp["inv_inertia"],
+                    "bound": float(np.max(np.linalg.norm(t["nodes"] - c, axis=1)))})
+    return out
+
+
+def _rsa(lsdem, rng, rsa, keep=None, pos=None, max_tries=20000):
+    """Random sequential addition of the spheres of an "rsa" spec (radius per particle, box lo/hi,
+    periodic flag), largest first."""
+    r = np.asarray(rsa["radius"], np.float64)
+    order = np.argsort(-r, kind="stable")
+    out = np.empty((len(r), 3))
+    kp = None if keep is None else np.asarray(keep)[order]
+    p0 = None if pos is None else np.asarray(pos)[order]
+    out[order] = lsdem.pack_rsa(r[order], rsa["lo"], rsa["hi"], periodic=rsa["periodic"],
+                                seed=int(rng.integers(1 << 62)), max_tries=max_tries, keep=kp, pos=p0)
+    return out
+
+
+def _body_arrays(tm, shape, scale, density):
+    m1 = np.array([t["mass"] for t in tm])[shape]
+    iI = np.array([t["inv_inertia"] for t in tm])[shape]
+    return 1.0 / (density * m1 * scale ** 3), iI / (density * scale[:, None] ** 5)
+
+
+def plane_wall(extent, pos, up=True, mu=0.5, e=0.6):
+    """Flat wall at `pos` covering a square of side 2 x extent around it, free side above
+    (up=True) or below (turned by a half turn about x)."""
+    w = make_plane_wall((2 * extent, 2 * extent))
+    return dict(w, pos=np.asarray(pos, np.float64), quat=np.array([1.0, 0, 0, 0]) if up else np.array([0.0, 1, 0, 0]),
+                mu=mu, e=e)
+
+
+def drum_wall(radius, length, h, mu=0.5, e=0.6, pad=2):
+    """Closed rotating-drum wall: the cavity of a cylinder of `radius` and `length` around the
+    local x axis, centred at the local origin; phi is the exact distance to the cavity boundary,
+    positive inside the cavity (the free side) and negative in the wall."""
+    n = [int(math.ceil((0.5 * length) / h)) + pad, int(math.ceil(radius / h)) + pad, int(math.ceil(radius / h)) + pad]
+    size = np.array([2 * n[0] + 1, 2 * n[1] + 1, 2 * n[2] + 1], np.int32)
+    origin = -h * np.array(n, np.float64)
+    p = grid_points(size, origin, h)
+    rho = np.sqrt(p[:, 1] ** 2 + p[:, 2] ** 2)
+    ax = np.abs(p[:, 0])
+    inside = (rho < radius) & (ax < 0.5 * length)
+    out = np.sqrt(np.maximum(rho - radius, 0.0) ** 2 + np.maximum(ax - 0.5 * length, 0.0) ** 2)
+    sdf = np.where(inside, np.minimum(radius - rho, 0.5 * length - ax), -out)
+    a = 2 * math.pi * np.arange(32) / 32
+    ring = np.stack([np.zeros(32), radius * np.cos(a), radius * np.sin(a)], 1)
+    verts = np.concatenate([ring + [-0.5 * length, 0, 0], ring + [0.5 * length, 0, 0]])
+    return {"verts": verts, "sdf": sdf, "size": size, "origin": origin, "spacing": h, "mu": mu, "e": e}
+
+
+def superquadric_templates(lsdem, rng, count, exponents, semi_axes, n_grid, n_nodes, level=5, pad=2, device=0):
+    """`count` superquadrics |x/a|^p + |y/b|^p + |z/c|^p = 1 with p uniform in `exponents` and
+    a, b, c uniform in `semi_axes`. Each grid is the mesh distance of the shape's subdivided
+    icosphere mesh (superellipsoid_mesh, `level` subdivisions: 20 x 4^level triangles), computed
+    on the GPU by the reference's buildGrid rule with a spacing that puts about n_grid nodes
+    along the longest axis; the surface nodes are Fibonacci directions scaled onto the surface."""
+    T = []
+    for _ in range(count):
+        p = float(rng.uniform(*exponents))
+        ax = rng.uniform(*semi_axes, size=3)
+        ee = en = 2.0 / p
+        v, f = superellipsoid_mesh(ax, ee, en, level)
+        h = 2.0 * float(ax.max()) / (n_grid - 1 - 2 * pad)
+        sdf, size, origin = lsdem.mesh_grid(v, f, h, pad=pad, device=device)
+        T.append({"nodes": superellipsoid_nodes(ax, ee, en, n_nodes), "sdf": sdf, "size": size, "origin": origin,
+                  "spacing": h, "exponent": p, "semi_axes": ax})
+    return T
+
+
+def bonded_hcp(lsdem, n=50_000, axes=(2e-3, 1.6e-3, 1.2e-3), n_grid=32, n_nodes=1000, gap=0.05, jitter=0.02,
+               bond_reach=1.1, youngs=1e8, poisson=0.3, strength_median=1e6, strength_sigma=0.3,
+               wall_speed=0.1, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=2e-7, seed=None):
+    """Bonded workload: n identical ellipsoids (semi-axes 2, 1.6, 1.2 mm) on a jittered HCP
+    lattice, bonded to every lattice neighbour, compressed by a top wall at 0.1 m/s.
+
+    The lattice is the reference's hexagonal close packing (SpherePackingGenerator.h:486-555:
+    rows shifted by r, layers by (r, r/sqrt(3))) of unit-diameter spheres at a spacing of
+    (1 + gap), mapped by diag(2a, 2b, 2c): the map sends touching spheres to touching aligned
+    ellipsoids, so the gap is 5 % of the contact distance along every lattice direction. Every
+    centre then moves by a random vector of length up to jitter x spacing (2 %, less than the
+    gap: no initial overlaps). Bonds join lattice neighbours whose centre distance in the unit
+    lattice is within bond_reach (1.1) of the contact distance: bond point at the midpoint,
+    normal from slave to master, length = centre distance (the reference's convention,
+    tutorial3-bondedLSParticleBeam.cpp:78-86), radius = 1 x the radius of the sphere of equal
+    volume (abc)^(1/3); tensile strength and cohesion log-normal (median 1e6 Pa, sigma 0.3),
+    bond friction 0. Floor at z = 0, top wall above the top layer moving down at wall_speed.
+    Contact law as the small workload; gravity -z."""
+    rng = np.random.default_rng(seed_for(2) if seed is None else seed)
+    ax = np.asarray(axes, np.float64)
+    r = 0.5 * (1.0 + gap)
+    m = int(round(n ** (1.0 / 3.0))) + 2
+    dx, dy, dz = 2 * r, math.sqrt(3.0) * r, math.sqrt(8.0 / 3.0) * r
+    pts = []
+    for k in range(2 * m):
+        for j in range(2 * m):
+            for i in range(2 * m):
+                x = i * dx + (r if j % 2 else 0.0) + (r if k % 2 else 0.0)
+                y = j * dy + (r / math.sqrt(3.0) if k % 2 else 0.0)
+                pts.append((x, y, k * dz))
+                if len(pts) >= 8 * m ** 3:
+                    break
+    pts = np.array(pts)
+    # a block of nx x ny x nz sites, as close to a cube in the mapped frame as n allows
+    span = 2 * ax * np.array([dx, dy, dz])
+    per = (n / np.prod(1.0 / span)) ** (1.0 / 3.0) / span
+    nx, ny = max(2, int(round(per[0]))), max(2, int(round(per[1])))
+    nz = int(math.ceil(n / (nx * ny)))
+    ii = np.round((pts[:, 0] - np.where(np.round(pts[:, 1] / dy) % 2 == 1, r, 0.0)) / dx)
+    jj = np.round(pts[:, 1] / dy)
+    kk = np.round(pts[:, 2] / dz)
+    sel = (ii >= 0) & (ii < nx) & (jj >= 0) & (jj < ny) & (kk >= 0) & (kk < nz)
+    u = pts[sel]
+    u = u[np.lexsort((u[:, 0], u[:, 1], u[:, 2]))][:n]
+    d = rng.normal(size=(len(u), 3))
+    d *= (rng.random(len(u)) ** (1.0 / 3.0) / np.linalg.norm(d, axis=1))[:, None]
+    u = u + jitter * 2 * r * d
+    from scipy.spatial import cKDTree
+
+    pairs = cKDTree(u).query_pairs(bond_reach, output_type="ndarray")
+    pos = u * (2 * ax)
+    pos -= pos.min(0)
+    pos += ax + 0.5 * gap * 2 * ax
+    shp = make_ellipsoid(ax, n_grid, n_nodes)
+    tm = _unit_density_templates(lsdem, [shp])
+    nb = len(pos)
+    shape = np.zeros(nb, np.int32)
+    scale = np.ones(nb)
+    inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
+    master, slave = pairs[:, 0], pairs[:, 1]
+    dv = pos[master] - pos[slave]
+    L0 = np.linalg.norm(dv, axis=1)
+    nb_bonds = len(master)
+    lo = np.zeros(3)
+    hi = pos.max(0) + ax + 0.5 * gap * 2 * ax
+    extent = float(max(hi[0], hi[1]))
+    walls = [plane_wall(extent, [0.5 * hi[0], 0.5 * hi[1], 0.0], True, mu, e),
+             dict(plane_wall(extent, [0.5 * hi[0], 0.5 * hi[1], hi[2]], False, mu, e),
+                  vel=np.array([0.0, 0.0, -wall_speed]))]
+    bonds = {"master": master.astype(np.int32), "slave": slave.astype(np.int32), "point": 0.5 * (pos[master] + pos[slave]),
+             "normal": dv / L0[:, None], "length": L0, "radius": np.full(nb_bonds, float(np.prod(ax) ** (1.0 / 3.0))),
+             "youngs": youngs, "poisson": poisson,
+             "tensile": strength_median * np.exp(strength_sigma * rng.standard_normal(nb_bonds)),
+             "cohesion": strength_median * np.exp(strength_sigma * rng.standard_normal(nb_bonds)), "mu": 0.0}
+    margin = 4 * float(ax.max())
+    return {"templates": tm, "shape": shape, "scale": scale, "pos": pos, "quat": np.tile([1.0, 0, 0, 0], (nb, 1)),
+            "vel": np.zeros((nb, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
+            "mu": mu, "e": e, "dt": dt, "min": lo - margin * np.array([1, 1, 0]),
+            "max": hi + margin * np.array([1, 1, 1]), "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 0,
+            "walls": walls, "bonds": bonds}
+
+
+def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-3), n_grid=64, n_nodes=1500,
+         radius=0.15, length=0.1, rpm=30.0, fill_fraction=0.3, wall_spacing=1e-3, kn=1e5, kt_ratio=0.8, mu=0.5,
+         e=0.6, density=2500.0, dt=5e-7, exclusion=0.7, seed=None, device=0, templates=None):
+    """Rotating-drum workload: n particles drawn uniformly from `shapes` seeded superquadrics
+    (exponents uniform 2-8, semi-axes uniform 1-3 mm, 64^3 grids from their meshes, 1500
+    nodes) in a closed drum of radius 0.15 m and length 0.1 m turning at 30 rpm about its
+    horizontal axis (x), gravity -z.
+
+    The stated counts and sizes do not fit the stated drum: 500,000 such bodies hold ~0.024 m^3
+    of solid, 3.4 x the drum's 7.1e-3 m^3. The drum, the count and the shape family are kept
+    and every shape is scaled by one common factor so that the bodies fill the loading box (the
+    part of the drum below z = 0.3 R, |y| <= 0.7 R, 5 mm clear of the end caps) at a solid
+    fraction of `fill_fraction`; the factor is returned as "size_factor". Positions by random
+    sequential addition of spheres of `exclusion` (0.7) x the bounding radius (bounding spheres
+    of these shapes hold ~2.2 x their volume), random orientations, at rest; deep overlaps are
+    removed afterwards by resolve_deep_overlaps."""
+    rng = np.random.default_rng(seed_for(3) if seed is None else seed)
+    T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
+    tm = _unit_density_templates(lsdem, T)
+    shape = rng.integers(0, len(tm), size=n).astype(np.int32)
+    vol = np.array([t["mass"] for t in tm])[shape].sum()
+    lo = np.array([-0.5 * length + 5e-3, -0.7 * radius, -math.sqrt(radius ** 2 - (0.7 * radius) ** 2)])
+    hi = np.array([0.5 * length - 5e-3, 0.7 * radius, 0.3 * radius])
+    box_vol = float(np.prod(hi - lo))
+    s = (fill_fraction * box_vol / vol) ** (1.0 / 3.0)
+    scale = np.full(n, s)
+    bound = np.array([t["bound"] for t in tm])[shape] * s
+    rsa = {"radius": exclusion * bound, "lo": lo + bound.max(), "hi": hi - bound.max(), "periodic": False}
+    pos = _rsa(lsdem, rng, rsa)
+    inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
+    w = drum_wall(radius, length, wall_spacing, mu, e)
+    w.update(pos=np.zeros(3), quat=np.array([1.0, 0, 0, 0]), angvel=np.array([2 * math.pi * rpm / 60.0, 0, 0]))
+    ext = np.array([0.5 * length, radius, radius])
+    return {"templates": tm, "shape": shape, "scale": scale, "pos": pos, "quat": random_quaternions(rng, n),
+            "vel": np.zeros((n, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
+            "mu": mu, "e": e, "dt": dt, "min": -ext, "max": ext, "gravity": np.array([0.0, 0.0, -9.81]),
+            "periodic": 0, "walls": [w], "size_factor": s, "rsa": rsa}
+
+
+def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=(1e-3, 2.5e-3), n_grid=48,
+                 n_nodes=1500, solid_fraction=0.3, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=5e-7,
+                 exclusion=0.7, seed=None, device=0, templates=None):
+    """Large-scale workload: n particles from `shapes` seeded superquadrics (exponents uniform
+    2-6, semi-axes uniform 1-2.5 mm, 1500 nodes, 48^3 grids from their meshes), periodic in x
+    and y, floor and ceiling walls in z, settling under gravity from a random loose packing at
+    solid fraction 0.3 (cube box; random sequential addition of spheres of `exclusion` (0.7) x
+    the bounding radius, periodic in x and y and kept one bounding radius clear of the walls;
+    random orientations, at rest; deep overlaps removed afterwards by resolve_deep_overlaps)."""
+    rng = np.random.default_rng(seed_for(4) if seed is None else seed)
+    T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
+    tm = _unit_density_templates(lsdem, T)
+    shape = rng.integers(0, len(tm), size=n).astype(np.int32)
+    vol = np.array([t["mass"] for t in tm])[shape].sum()
+    L = (vol / solid_fraction) ** (1.0 / 3.0)
+    scale = np.ones(n)
+    bound = np.array([t["bound"] for t in tm])[shape]
+    b = float(bound.max())
+    rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - b]), "periodic": True}
+    pos = _rsa(lsdem, rng, rsa)
+    inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
+    walls = [plane_wall(L, [0.5 * L, 0.5 * L, 0.0], True, mu, e), plane_wall(L, [0.5 * L, 0.5 * L, L], False, mu, e)]
+    return {"templates": tm, "shape": shape, "scale": scale, "pos": pos, "quat": random_quaternions(rng, n),
+            "vel": np.zeros((n, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
+            "mu": mu, "e": e, "dt": dt, "min": np.zeros(3), "max": np.full(3, L),
+            "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 3, "walls": walls, "rsa": rsa}

@@ -39,3 +39,12 @@ nvcc -std=c++17 -O3 -DNDEBUG \
   -I"$REF/FunDEM" -I"$K" -I"$K/CUDAKernelFunction" \
   "$HERE/../tests/apps/c0_bench.cpp" "${SRCS[@]:0:5}" -o "$OUT/c0_bench_fundem"
 echo "built $OUT/c0_bench_fundem"
+
+# Golden-vector driver for the level-set grid builder: the reference's host-only
+# generator header (kernel/helper/LevelSetObjectGenerator.h) driven by
+# oracle/ref_mesh_grid.cpp. Host code; g++ with the CUDA include path for the
+# vector types, no device code.
+g++ -std=c++17 -O3 -DNDEBUG -ffp-contract=off \
+  -I/usr/local/cuda/include -I"$K" -I"$K/CUDAKernelFunction" \
+  "$HERE/ref_mesh_grid.cpp" -o "$OUT/mesh_grid_ref"
+echo "built $OUT/mesh_grid_ref"

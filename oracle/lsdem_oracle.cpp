@@ -597,6 +597,75 @@ ORA_API void ora_mass_props(const double* sdf, int nx, int ny, int nz, const dou
   out[10] = inv.xx; out[11] = inv.yy; out[12] = inv.zz; out[13] = inv.xy; out[14] = inv.xz; out[15] = inv.yz;
 }
 
+// ---------------------------------------------------------------------------
+// Level-set grid of a closed triangle mesh: LevelSetObject::Base::buildGrid
+// (FunDEM/kernel/helper/LevelSetObjectGenerator.h:122-224) over
+// TriangleMeshParticle::evaluateImplicitFunctionValueAndGradient (:888-914).
+// Closest point on a triangle by the Voronoi-region tests of Ericson,
+// "Real-Time Collision Detection" (2005) 5.1.5 (closestPointOnTriangle,
+// :454-500); the nearest triangle by a scan in index order (the reference's BVH
+// finds the same distance); inside by the solid-angle sum of Van Oosterom and
+// Strackee (1983) in triangle order (:758-802).
+static d3 closest_on_triangle(d3 p, d3 a, d3 b, d3 c) {
+  const d3 ab = b - a, ac = c - a, ap = p - a;
+  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0.0 && d2 <= 0.0) return a;
+  const d3 bp = p - b;
+  const double d3v = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3v >= 0.0 && d4 <= d3v) return b;
+  const double vc = d1 * d4 - d3v * d2;
+  if (vc <= 0.0 && d1 >= 0.0 && d3v <= 0.0) return a + (d1 / (d1 - d3v)) * ab;
+  const d3 cp = p - c;
+  const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0 && d5 <= d6) return c;
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return a + (d2 / (d2 - d6)) * ac;
+  const double va = d3v * d6 - d5 * d4;
+  if (va <= 0.0 && (d4 - d3v) >= 0.0 && (d5 - d6) >= 0.0) return b + ((d4 - d3v) / ((d4 - d3v) + (d5 - d6))) * (c - b);
+  const double denom = 1.0 / (va + vb + vc);
+  const double v = vb * denom, w = vc * denom;
+  return a + ab * v + ac * w;
+}
+
+static double solid_angle(d3 p, d3 a, d3 b, d3 c) {
+  const d3 r0 = a - p, r1 = b - p, r2 = c - p;
+  const double l0 = len(r0), l1 = len(r1), l2 = len(r2);
+  if (l0 < 1e-30 || l1 < 1e-30 || l2 < 1e-30) return 0.0;
+  const double num = dot(r0, cross(r1, r2));
+  const double den = l0 * l1 * l2 + dot(r0, r1) * l2 + dot(r1, r2) * l0 + dot(r2, r0) * l1;
+  return 2.0 * std::atan2(num, den);
+}
+
+ORA_API void ora_mesh_grid(const double* verts, const int* tris, int nt, const double* origin, int nx, int ny, int nz,
+                           double h, int positive_inside, double* out) {
+  const long long n = (long long)nx * ny * nz;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long long i = 0; i < n; ++i) {
+    const int ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / ((long long)nx * ny));
+    const d3 p = mk(origin[0] + double(ix) * h, origin[1] + double(iy) * h, origin[2] + double(iz) * h);
+    double best = 1.7976931348623157e308, sum = 0.0;
+    d3 cp = mk(0., 0., 0.);
+    for (int t = 0; t < nt; ++t) {
+      const d3 a = ld3(verts, tris[3 * t]), b = ld3(verts, tris[3 * t + 1]), c = ld3(verts, tris[3 * t + 2]);
+      const d3 x = closest_on_triangle(p, a, b, c);
+      const double dd = len2(p - x);
+      if (dd < best) { best = dd; cp = x; }
+      sum += solid_angle(p, a, b, c);
+    }
+    const double d = len(p - cp);
+    const bool inside = std::fabs(sum / (4.0 * 3.14159265358979323846)) > 0.5;
+    double value = inside ? -d : d;
+    d3 g = mk(0., 0., 0.);
+    if (d > 1e-30) {
+      const d3 u = (p - cp) / d;
+      g = inside ? -u : u;
+    }
+    if (positive_inside) { value = -value; g = -g; }
+    const double gn = len(g);
+    out[i] = gn > 1e-12 ? value / gn : (value <= 0.0 ? -1.0 : 1.0) * 0.5 * h;
+  }
+}
+
 // Host-side helpers used by the orchestration layer.
 ORA_API void ora_rotate(int n, const double* quat, const double* v, double* out) {
   for (int i = 0; i < n; ++i) st3(out, i, rotate(ldq(quat, i), ld3(v, i)));

@@ -101,6 +101,7 @@ lib.ora_bond_force.argtypes = [C.c_int, IP, DP, DP, DP, IP, DP, DP, DP, DP, DP]
 lib.ora_kick.argtypes = [C.c_int, DP, DP, DP, DP, DP, DP, DP, DP, C.c_double]
 lib.ora_drift.argtypes = [C.c_int, DP, DP, DP, DP, C.c_double]
 lib.ora_mass_props.argtypes = [DP, C.c_int, C.c_int, C.c_int, DP, C.c_double, C.c_double, DP]
+lib.ora_mesh_grid.argtypes = [DP, IP, C.c_int, DP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, DP]
 lib.ora_set_threads.argtypes = [C.c_int]
 lib.ora_num_threads.restype = C.c_int
 
@@ -157,6 +158,17 @@ def mass_props(sdf, size, origin, h, density):
     out = np.zeros(16)
     lib.ora_mass_props(_d(f64(sdf)), int(size[0]), int(size[1]), int(size[2]), _d(f64(origin)), float(h),
                        float(density), _d(out))
+    return out
+
+
+def mesh_grid(verts, tris, origin, size, h, positive_inside=False):
+    """Level-set grid of a closed triangle mesh (buildGrid over the mesh distance with the
+    solid-angle sign, LevelSetObjectGenerator.h:122-224, 454-500, 758-802)."""
+    v = f64(verts, (-1, 3))
+    t = i32(np.reshape(tris, (-1, 3)))
+    out = np.zeros(int(np.prod(np.asarray(size, np.int64))))
+    lib.ora_mesh_grid(_d(v), _i(t), len(t), _d(f64(origin)), int(size[0]), int(size[1]), int(size[2]), float(h),
+                      1 if positive_inside else 0, _d(out))
     return out
 
 
