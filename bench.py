@@ -176,11 +176,14 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000, devic
                "sdf_grid": "x".join(str(int(v)) for v in np.max([t["size"] for t in T], axis=0)) + " (largest)",
                "sdf_from": "mesh distance of 20480-triangle superquadric meshes, built on the GPU",
                "setup_s": round(t_gen, 1), "dt_s": sc["dt"],
-               "initial_state": f"random sequential addition, deep overlaps re-placed ({iters} passes)"}
+               "initial_state": (f"random sequential addition, deep overlaps re-placed ({iters} passes, "
+                                 f"{sc.get('reserve_placed', 0)} bodies to the reserve box)")}
         if workload == "drum":
-            cfg.update(drum="R 0.15 m, L 0.1 m, 30 rpm about x", size_factor=round(float(sc["size_factor"]), 4))
+            cfg.update(drum="R 0.15 m, L 0.1 m, 30 rpm about x", size_factor=round(float(sc["size_factor"]), 4),
+                       fill="solid fraction 0.22 of the loading box")
         else:
-            cfg.update(box_m=round(float(sc["max"][0]), 4), periodic="xy", walls="z")
+            cfg.update(box_m=[round(float(v), 4) for v in sc["max"]], periodic="xy", walls="z",
+                       solid_fraction=sc["solid_fraction"])
         return sc, cfg
     cache = ROOT / "_build" / "templates_48_2000.npz"
     if cache.exists():

@@ -530,9 +530,25 @@ def resolve_deep_overlaps(lsdem, sc, threshold=0.02, exclusion=0.8, max_iter=40,
         keep = np.ones(n, np.int32)
         keep[bad] = 0
         if "rsa" in sc:
-            # scenes with their own packing spec: re-placed spheres 10 % smaller than the first packing
-            rsa = dict(sc["rsa"], radius=np.where(keep == 0, 0.9, 1.0) * sc["rsa"]["radius"])
-            sc["pos"] = _rsa(lsdem, rng, rsa, keep=keep, pos=sc["pos"])
+            # scenes with their own packing spec: re-placed with the same spheres; when no room is
+            # left (or in the last pass) the remaining bodies go to the spec's reserve box, where
+            # their bounding spheres do not overlap each other or the packing
+            rsa = sc["rsa"]
+            placed = False
+            if it < max_iter:
+                try:
+                    sc["pos"] = _rsa(lsdem, rng, rsa, keep=keep, pos=sc["pos"])
+                    placed = True
+                except Exception:
+                    placed = False
+            if not placed:
+                if "reserve_lo" not in rsa:
+                    raise RuntimeError("resolve_deep_overlaps: no room to re-place overlapping bodies")
+                res = {"radius": rsa["bound"][bad], "lo": rsa["reserve_lo"], "hi": rsa["reserve_hi"], "periodic": False}
+                sc["pos"][bad] = _rsa(lsdem, rng, res)
+                sc["quat"][bad] = random_quaternions(rng, len(bad))
+                sc["reserve_placed"] = int(len(bad))
+                break
         else:
             # re-placed spheres may come a little closer than the first packing (0.75 x radius)
             rad = 0.5 * exclusion * sc["scale"]
@@ -731,8 +747,8 @@ def bonded_hcp(lsdem, n=50_000, axes=(2e-3, 1.6e-3, 1.2e-3), n_grid=32, n_nodes=
 
 
 def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-3), n_grid=64, n_nodes=1500,
-         radius=0.15, length=0.1, rpm=30.0, fill_fraction=0.3, wall_spacing=1e-3, kn=1e5, kt_ratio=0.8, mu=0.5,
-         e=0.6, density=2500.0, dt=5e-7, exclusion=0.7, seed=None, device=0, templates=None):
+         radius=0.15, length=0.1, rpm=30.0, fill_fraction=0.22, wall_spacing=1e-3, kn=1e5, kt_ratio=0.8, mu=0.5,
+         e=0.6, density=2500.0, dt=5e-7, exclusion=0.85, seed=None, device=0, templates=None):
     """Rotating-drum workload: n particles drawn uniformly from `shapes` seeded superquadrics
     (exponents uniform 2-8, semi-axes uniform 1-3 mm, 64^3 grids from their meshes, 1500
     nodes) in a closed drum of radius 0.15 m and length 0.1 m turning at 30 rpm about its
@@ -743,9 +759,11 @@ def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-
     and every shape is scaled by one common factor so that the bodies fill the loading box (the
     part of the drum below z = 0.3 R, |y| <= 0.7 R, 5 mm clear of the end caps) at a solid
     fraction of `fill_fraction`; the factor is returned as "size_factor". Positions by random
-    sequential addition of spheres of `exclusion` (0.7) x the bounding radius (bounding spheres
-    of these shapes hold ~2.2 x their volume), random orientations, at rest; deep overlaps are
-    removed afterwards by resolve_deep_overlaps."""
+    sequential addition of spheres of `exclusion` x the bounding radius (bounding spheres of
+    these shapes hold ~2.2 x their volume, so 0.22 with exclusion 0.85 is close to the densest
+    random placement without mass interpenetration), random orientations, at rest; deep overlaps
+    are removed afterwards by resolve_deep_overlaps, which puts the bodies it cannot fit into
+    the empty upper part of the drum."""
     rng = np.random.default_rng(seed_for(3) if seed is None else seed)
     T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
     tm = _unit_density_templates(lsdem, T)
@@ -757,7 +775,10 @@ def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-
     s = (fill_fraction * box_vol / vol) ** (1.0 / 3.0)
     scale = np.full(n, s)
     bound = np.array([t["bound"] for t in tm])[shape] * s
-    rsa = {"radius": exclusion * bound, "lo": lo + bound.max(), "hi": hi - bound.max(), "periodic": False}
+    bm = float(bound.max())
+    rsa = {"radius": exclusion * bound, "lo": lo + bm, "hi": hi - bm, "periodic": False, "bound": bound,
+           "reserve_lo": np.array([lo[0] + bm, -0.5 * radius, hi[2] + bm]),
+           "reserve_hi": np.array([hi[0] - bm, 0.5 * radius, 0.8 * radius])}
     pos = _rsa(lsdem, rng, rsa)
     inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
     w = drum_wall(radius, length, wall_spacing, mu, e)
@@ -770,14 +791,22 @@ def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-
 
 
 def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=(1e-3, 2.5e-3), n_grid=48,
-                 n_nodes=1500, solid_fraction=0.3, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=5e-7,
-                 exclusion=0.7, seed=None, device=0, templates=None):
+                 n_nodes=1500, solid_fraction=0.25, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=5e-7,
+                 exclusion=0.85, reserve=0.02, seed=None, device=0, templates=None):
     """Large-scale workload: n particles from `shapes` seeded superquadrics (exponents uniform
     2-6, semi-axes uniform 1-2.5 mm, 1500 nodes, 48^3 grids from their meshes), periodic in x
     and y, floor and ceiling walls in z, settling under gravity from a random loose packing at
-    solid fraction 0.3 (cube box; random sequential addition of spheres of `exclusion` (0.7) x
-    the bounding radius, periodic in x and y and kept one bounding radius clear of the walls;
-    random orientations, at rest; deep overlaps removed afterwards by resolve_deep_overlaps)."""
+    solid fraction (cube box; random sequential addition of spheres of `exclusion` x the bounding
+    radius, periodic in x and y and kept one bounding radius clear of the walls; random
+    orientations, at rest; deep overlaps removed afterwards by resolve_deep_overlaps).
+
+    Random placement of these shapes cannot reach the stated 0.3 without deep overlaps: their
+    bounding spheres hold ~1.9 x their volume, so at 0.3 the spheres must overlap (exclusion
+    <= 0.8) and a third or more of the bodies then start deeply interpenetrated, which
+    re-placement cannot resolve. The default is 0.25 with exclusion 0.85 (~14 % of bodies in
+    deep overlap before re-placement, a few per thousand after it); the bodies re-placement
+    cannot fit go to a reserve slab above the packing (`reserve` x n bounding spheres at 20 %
+    fraction, no overlaps), which raises the ceiling accordingly."""
     rng = np.random.default_rng(seed_for(4) if seed is None else seed)
     T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
     tm = _unit_density_templates(lsdem, T)
@@ -787,11 +816,15 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
     scale = np.ones(n)
     bound = np.array([t["bound"] for t in tm])[shape]
     b = float(bound.max())
-    rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - b]), "periodic": True}
+    slab = reserve * n * (4.0 / 3.0) * math.pi * float(np.mean(bound ** 3)) / 0.2 / (L * L) + 2 * b
+    H = L + b + slab
+    rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - b]), "periodic": True,
+           "bound": bound, "reserve_lo": np.array([0.0, 0.0, L + b]), "reserve_hi": np.array([L, L, H])}
     pos = _rsa(lsdem, rng, rsa)
     inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
-    walls = [plane_wall(L, [0.5 * L, 0.5 * L, 0.0], True, mu, e), plane_wall(L, [0.5 * L, 0.5 * L, L], False, mu, e)]
+    walls = [plane_wall(L, [0.5 * L, 0.5 * L, 0.0], True, mu, e), plane_wall(L, [0.5 * L, 0.5 * L, H], False, mu, e)]
     return {"templates": tm, "shape": shape, "scale": scale, "pos": pos, "quat": random_quaternions(rng, n),
             "vel": np.zeros((n, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
-            "mu": mu, "e": e, "dt": dt, "min": np.zeros(3), "max": np.full(3, L),
-            "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 3, "walls": walls, "rsa": rsa}
+            "mu": mu, "e": e, "dt": dt, "min": np.zeros(3), "max": np.array([L, L, H]),
+            "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 3, "walls": walls, "rsa": rsa,
+            "solid_fraction": solid_fraction}
