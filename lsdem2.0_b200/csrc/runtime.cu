@@ -700,6 +700,35 @@ void initialize(lsdem_solver* s) {
     }
     CK(s->s_nbox.upload(nbox.data(), nbox.size(), st));
   }
+  {
+    // per template, in spacings: the largest difference of neighbouring SDF values
+    // (bound of each partial derivative of the trilinear interpolant per grid
+    // unit) and the largest gradient-norm bound of a cell, sqrt of the sum over
+    // axes of the cell's largest edge difference squared
+    std::vector<float> lip;
+    for (const ShapeHost& sh : s->shapes) {
+      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
+      const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+      auto at = [&](int x, int y, int z) { return sh.sdf[(size_t)x + sy * y + sz * z]; };
+      double m = 0., g = 0.;
+      for (int z = 0; z + 1 < nz; ++z)
+        for (int y = 0; y + 1 < ny; ++y)
+          for (int x = 0; x + 1 < nx; ++x) {
+            double e[3] = {0., 0., 0.};
+            for (int b = 0; b < 4; ++b) {
+              const int u = b & 1, v = b >> 1;
+              e[0] = std::max(e[0], std::fabs(at(x + 1, y + u, z + v) - at(x, y + u, z + v)));
+              e[1] = std::max(e[1], std::fabs(at(x + u, y + 1, z + v) - at(x + u, y, z + v)));
+              e[2] = std::max(e[2], std::fabs(at(x + u, y + v, z + 1) - at(x + u, y + v, z)));
+            }
+            m = std::max(m, std::max(e[0], std::max(e[1], e[2])));
+            g = std::max(g, std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]));
+          }
+      lip.push_back((float)(m / sh.h * (1.0 + 1e-6)));
+      lip.push_back((float)(g / sh.h * (1.0 + 1e-6)));
+    }
+    CK(s->s_lip.upload(lip.data(), lip.size(), st));
+  }
   if (s->precision != PREC_FP64) {
     // precision form: phi / h of each template in 16 bits, FP32 node copy
     // cell-major 16-bit store: the 8 corners of cell (i, j, k) in 16 bytes, corner
@@ -733,36 +762,9 @@ void initialize(lsdem_solver* s) {
     std::vector<float4> nf(node_pos.size());
     for (size_t i = 0; i < node_pos.size(); ++i)
       nf[i] = make_float4((float)node_pos[i].x, (float)node_pos[i].y, (float)node_pos[i].z, 0.f);
-    // per template, in spacings: the largest difference of neighbouring SDF values
-    // (bound of each partial derivative of the trilinear interpolant per grid
-    // unit) and the largest gradient-norm bound of a cell, sqrt of the sum over
-    // axes of the cell's largest edge difference squared
-    std::vector<float> lip;
-    for (const ShapeHost& sh : s->shapes) {
-      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
-      const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-      auto at = [&](int x, int y, int z) { return sh.sdf[(size_t)x + sy * y + sz * z]; };
-      double m = 0., g = 0.;
-      for (int z = 0; z + 1 < nz; ++z)
-        for (int y = 0; y + 1 < ny; ++y)
-          for (int x = 0; x + 1 < nx; ++x) {
-            double e[3] = {0., 0., 0.};
-            for (int b = 0; b < 4; ++b) {
-              const int u = b & 1, v = b >> 1;
-              e[0] = std::max(e[0], std::fabs(at(x + 1, y + u, z + v) - at(x, y + u, z + v)));
-              e[1] = std::max(e[1], std::fabs(at(x + u, y + 1, z + v) - at(x + u, y, z + v)));
-              e[2] = std::max(e[2], std::fabs(at(x + u, y + v, z + 1) - at(x + u, y + v, z)));
-            }
-            m = std::max(m, std::max(e[0], std::max(e[1], e[2])));
-            g = std::max(g, std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]));
-          }
-      lip.push_back((float)(m / sh.h * (1.0 + 1e-6)));
-      lip.push_back((float)(g / sh.h * (1.0 + 1e-6)));
-    }
     CK(s->s_cell16.upload(cells.data(), cells.size(), st));
     CK(s->s_cell_off.upload(cell_off.data(), cell_off.size(), st));
     CK(s->s_node_f.upload(nf.data(), nf.size(), st));
-    CK(s->s_lip.upload(lip.data(), lip.size(), st));
   }
   // node ids (LSBoundaryNode order: particle by particle, caller node order)
   s->P.node_base.resize(s->P.n());

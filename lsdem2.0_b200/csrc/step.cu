@@ -136,6 +136,42 @@ LD void grid_box(const double3 o, double invh, int3 gs, double3& lo, double3& hi
   hi = d3(o.x + (gs.x - 1) / invh, o.y + (gs.y - 1) / invh, o.z + (gs.z - 1) / invh);
 }
 
+// True when no point within `reach` of l (wall frame) that lies in wall w's grid
+// box can have phi <= 0, so that no node of a particle of that bounding radius can
+// pass the wall's SDF test (sdf_eval rejects nodes outside the box, and inside it
+// the interpolated phi is positive). q is l's grid position projected onto the
+// box; for a node position p in the box |p - q| <= |p - l| (projection onto a
+// convex set does not expand distances), the segment p-q stays in the box, and
+// along it phi changes by at most the template's cell gradient-norm bound per
+// grid unit (lip[2 sh + 1] spacings per spacing). phi(q) is the FP64 trilinear
+// value of the grid, as the node test computes it, with a rounding margin.
+LD bool wall_far(const StepArgs& a, int w, double3 l, double reach) {
+  const int sh = a.W.shape[w];
+  const int3 gs = a.S.gsize[sh];
+  const double invh = a.W.invh[w];
+  const double3 o = a.W.origin[w];
+  const double qx = fmin(fmax((l.x - o.x) * invh, 0.0), (double)(gs.x - 1));
+  const double qy = fmin(fmax((l.y - o.y) * invh, 0.0), (double)(gs.y - 1));
+  const double qz = fmin(fmax((l.z - o.z) * invh, 0.0), (double)(gs.z - 1));
+  const int i0 = min((int)qx, gs.x - 2), j0 = min((int)qy, gs.y - 2), k0 = min((int)qz, gs.z - 2);
+  const double fx = qx - i0, fy = qy - j0, fz = qz - k0;
+  const int sy = gs.x, sz = gs.x * gs.y;
+  const double* b = a.S.sdf + a.S.sdf_off[sh] + ((size_t)k0 * sz + (size_t)j0 * sy + i0);
+  const double sc = a.W.scale[w];
+  double cmax = 0.0, acc = 0.0;
+#pragma unroll 1
+  for (int e = 0; e < 4; ++e) {  // the four x-edges of the cell
+    const int dy = e & 1, dz = e >> 1;
+    const double* be = b + dz * sz + dy * sy;
+    const double v0 = __ldg(be), v1 = __ldg(be + 1);
+    cmax = fmax(cmax, fmax(fabs(v0), fabs(v1)));
+    acc += (v0 * (1.0 - fx) + v1 * fx) * (dy ? fy : 1.0 - fy) * (dz ? fz : 1.0 - fz);
+  }
+  const double phi = sc * acc;
+  const double bound = (double)a.S.lip[2 * sh + 1] * reach * (1.0 + 1e-9) + 1e-12 * sc * cmax + 1e-300;
+  return phi > bound;
+}
+
 // Appends this lane's entries A * cap + j, j < cnt, to a flat pair list, with
 // one atomic per warp (all lanes of the warp call it).
 LD void append_pairs(int* list, int* ctr, int A, int cap, int cnt) {
@@ -170,7 +206,8 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
 // runs on the FP32 copies with a margin that covers their rounding (relative
 // 1e-5 of the reach plus 1e-6 of the coordinates), so the candidates are a
 // superset of the exact ones; the narrowphase decides every node exactly.
-// Wall partners: visible walls whose SDF grid box the bounding sphere reaches.
+// Wall partners: visible walls whose SDF grid box the bounding sphere reaches and
+// whose interpolated phi is not provably positive over it (wall_far).
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
 // mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
 // and their occupant loads are broadcasts. Slots are filled in cell-walk then
@@ -222,6 +259,7 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
       grid_box(a.W.origin[w], a.W.invh[w], a.S.gsize[a.W.shape[w]], lo, hi);
       const double reach = rA * (1.0 + 1e-9) + coord_slack(xA, a.W.pos[w]) + 1e-12 * len(hi - lo);
       if (box_dist(l, lo, hi) > reach) continue;
+      if (wall_far(a, w, l, reach)) continue;
       if (nw < capw) a.pw.id[(size_t)A * capw + nw] = w;
       ++nw;
     }

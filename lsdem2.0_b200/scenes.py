@@ -618,12 +618,20 @@ def _body_arrays(tm, shape, scale, density):
     return 1.0 / (density * m1 * scale ** 3), iI / (density * scale[:, None] ** 5)
 
 
-def plane_wall(extent, pos, up=True, mu=0.5, e=0.6):
+def plane_wall(extent, pos, up=True, mu=0.5, e=0.6, h=2e-3):
     """Flat wall at `pos` covering a square of side 2 x extent around it, free side above
-    (up=True) or below (turned by a half turn about x)."""
-    w = make_plane_wall((2 * extent, 2 * extent))
-    return dict(w, pos=np.asarray(pos, np.float64), quat=np.array([1.0, 0, 0, 0]) if up else np.array([0.0, 1, 0, 0]),
-                mu=mu, e=e)
+    (up=True) or below (turned by a half turn about x). phi = z on a grid of spacing `h`
+    (2 mm) five nodes deep (|z| <= 2h): phi is linear, so the grid is exact at any spacing,
+    and a fine spacing keeps the 16-bit copy of phi / h precise in absolute terms (its
+    certified error band is a fixed fraction of a spacing)."""
+    m = int(math.ceil(extent / h))
+    size = np.array([2 * m + 1, 2 * m + 1, 5], np.int32)
+    origin = np.array([-m * h, -m * h, -2 * h])
+    sdf = grid_points(size, origin, h)[:, 2].copy()
+    verts = np.array([[-extent, -extent, 0.0], [extent, -extent, 0.0], [extent, extent, 0.0], [-extent, extent, 0.0]])
+    return {"verts": verts, "sdf": sdf, "size": size, "origin": origin, "spacing": h,
+            "pos": np.asarray(pos, np.float64), "quat": np.array([1.0, 0, 0, 0]) if up else np.array([0.0, 1, 0, 0]),
+            "mu": mu, "e": e}
 
 
 def drum_wall(radius, length, h, mu=0.5, e=0.6, pad=2):
