@@ -205,7 +205,7 @@ def build_scene(lsdem, workload: str, rank: int, particles: int = 100_000, devic
                 "initial_state": f"random sequential addition, deep overlaps re-placed ({iters} passes)"}
 
 
-def load(lsdem, sc, workload, device, prec, learned=False, info=None):
+def load(lsdem, sc, workload, device, prec, learned=False, info=None, record=False):
     from lsdem_b200 import scenes
     sv = lsdem.Solver(device=device)
     if workload == "small":
@@ -213,6 +213,8 @@ def load(lsdem, sc, workload, device, prec, learned=False, info=None):
     else:
         scenes.load_polydisperse(sv, sc)
     sv.set_precision(prec)
+    if record:
+        sv.set_record_contacts(True)
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
     if learned:
         t0 = time.perf_counter()
@@ -226,9 +228,37 @@ def load(lsdem, sc, workload, device, prec, learned=False, info=None):
     return sv
 
 
+def _energies(lsdem, sv):
+    """Kinetic energy (translation + rotation) of the state and elastic energy stored in the
+    contacts (normal + tangential terms of every particle, wall and image contact)."""
+    st = sv.state()
+    pp = sv.particle_params()
+    im = pp["inv_mass"]
+    live = im > 0
+    ke = 0.5 * float(np.sum((st["vel"] ** 2).sum(1)[live] / im[live]))
+    q = st["quat"]
+    w0, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    R = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w0 * z), 2 * (x * z + w0 * y)], 1),
+                  np.stack([2 * (x * y + w0 * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w0 * x)], 1),
+                  np.stack([2 * (x * z - w0 * y), 2 * (y * z + w0 * x), 1 - 2 * (x * x + y * y)], 1)], 1)
+    wb = np.einsum("nji,nj->ni", R, st["angvel"])  # body-frame angular velocity
+    ii = pp["inv_inertia"]
+    inv = np.stack([np.stack([ii[:, 0], ii[:, 3], ii[:, 4]], 1), np.stack([ii[:, 3], ii[:, 1], ii[:, 5]], 1),
+                    np.stack([ii[:, 4], ii[:, 5], ii[:, 2]], 1)], 1)
+    ok = live & (np.abs(np.linalg.det(inv)) > 0)
+    Lb = np.linalg.solve(inv[ok], wb[ok][:, :, None])[:, :, 0]
+    ke += 0.5 * float(np.sum((wb[ok] * Lb).sum(1)))
+    ec = 0.0
+    for kind in (lsdem.CONTACT_PARTICLE, lsdem.CONTACT_WALL, lsdem.CONTACT_GHOST):
+        c = sv.contacts(kind, geometry=True)
+        ec += float(np.sum(c["en_n"]) + np.sum(c["en_s"]))
+    return ke, ec
+
+
 def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
-    """Force / torque error of an FP32 form against the FP64 path, from the same state: both
-    run `warm` FP64 steps, then one step each; forces are captured in the external hook."""
+    """Force / torque / energy error of an FP32 form against the FP64 path, from the same
+    state: both run `warm` FP64 steps, then one step each; forces are captured in the external
+    hook, kinetic and contact energies read after the step."""
     import torch
     out = {}
     sv = load(lsdem, sc, workload, device, 0)
@@ -236,17 +266,21 @@ def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
     st = sv.state()
     sv.close()
     for p in (0, prec):
-        sv = load(lsdem, sc, workload, device, p, learned=learned and p != 0)
+        sv = load(lsdem, sc, workload, device, p, learned=learned and p != 0, record=True)
         sv.set_state(pos=st["pos"], vel=st["vel"], angvel=st["angvel"], quat=st["quat"])
         box = {}
         sv.step(sc["dt"], 1, hook=lambda t, sv=sv: box.update(sv.state()))
         torch.cuda.synchronize()
+        box["energy"] = _energies(lsdem, sv)
         out[p] = box
         sv.close()
     F64, T64 = out[0]["force"], out[0]["torque"]
+    (k64, e64), (kp, ep) = out[0]["energy"], out[prec]["energy"]
     return {"force_l2": float(np.linalg.norm(out[prec]["force"] - F64) / np.linalg.norm(F64)),
             "torque_l2": float(np.linalg.norm(out[prec]["torque"] - T64) / np.linalg.norm(T64)),
-            "force_max": float(np.abs(out[prec]["force"] - F64).max() / np.abs(F64).max())}
+            "force_max": float(np.abs(out[prec]["force"] - F64).max() / np.abs(F64).max()),
+            "kinetic_energy_rel": abs(kp - k64) / k64 if k64 > 0 else None,
+            "contact_energy_rel": abs(ep - e64) / e64 if e64 > 0 else None}
 
 
 def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_seconds=10.0, max_steps=200):

@@ -48,3 +48,11 @@ g++ -std=c++17 -O3 -DNDEBUG -ffp-contract=off \
   -I/usr/local/cuda/include -I"$K" -I"$K/CUDAKernelFunction" \
   "$HERE/ref_mesh_grid.cpp" -o "$OUT/mesh_grid_ref"
 echo "built $OUT/mesh_grid_ref"
+
+# The bonded-workload app (tests/apps/c2_bench.cpp, LSSolver API only) against the
+# reference solver, as the config-0 app above.
+nvcc -std=c++17 -O3 -DNDEBUG \
+  -gencode arch=compute_100a,code=sm_100a \
+  -I"$REF/FunDEM" -I"$K" -I"$K/CUDAKernelFunction" \
+  "$HERE/../tests/apps/c2_bench.cpp" "${SRCS[@]:0:5}" -o "$OUT/c2_bench_fundem"
+echo "built $OUT/c2_bench_fundem"

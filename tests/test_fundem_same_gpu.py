@@ -1,4 +1,4 @@
-"""Config 0 on the reference solver's own CUDA build and on this solver, same GPU, same app.
+"""Configs 0 and 2 on the reference solver's own CUDA build and on this solver, same GPU, same app.
 
 tests/apps/c0_bench.cpp is written against the LSSolver API only. oracle/build_ref.sh builds
 it against the reference (FunDEM/kernel/LSSolver.h and its kernel sources, Release flags,
@@ -11,6 +11,13 @@ the forces and the second half kick), and the particle velocities at the window'
 
 Checked: the velocities agree to FP64 round-off (same algorithm, same inputs). The two
 timings are printed (they are reported, not asserted).
+
+Config 2 (tests/apps/c2_bench.cpp, oracle/_ref/c2_bench_fundem): aligned ellipsoids (2, 1.6,
+1.2 mm, 32^3 grids, 1,000 nodes) on the jittered HCP lattice with a V-bond to every lattice
+neighbour, a floor and a top wall moving down at 0.1 m/s, added through addLSParticle (density),
+addWall, setFixedVelocityToWall and addBondedInteraction, at a reduced count of 8,000
+particles: the reference keeps a full SDF copy per particle in host and device memory (Q14),
+2.1 GB here, 13 GB at the configuration's 50,000.
 """
 import shutil
 import struct
@@ -26,17 +33,20 @@ pytestmark = pytest.mark.gpu
 FUNDEM = ROOT / "oracle" / "_ref" / "c0_bench_fundem"
 OURS = ROOT / "lsdem2.0_b200" / "_build" / "c0_bench_b200"
 APP = ROOT / "tests" / "apps" / "c0_bench.cpp"
+FUNDEM2 = ROOT / "oracle" / "_ref" / "c2_bench_fundem"
+OURS2 = ROOT / "lsdem2.0_b200" / "_build" / "c2_bench_b200"
+APP2 = ROOT / "tests" / "apps" / "c2_bench.cpp"
 
 
-def build_ours() -> None:
-    if OURS.exists() and OURS.stat().st_mtime >= max(APP.stat().st_mtime,
-                                                     (ROOT / "include" / "kernel" / "LSSolver.h").stat().st_mtime):
+def build_ours(app=APP, out=OURS) -> None:
+    if out.exists() and out.stat().st_mtime >= max(app.stat().st_mtime,
+                                                    (ROOT / "include" / "kernel" / "LSSolver.h").stat().st_mtime):
         return
     cmd = ["nvcc", "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
-           "-I", str(ROOT / "include"), "-I", str(ROOT / "include" / "kernel"), str(APP),
+           "-I", str(ROOT / "include"), "-I", str(ROOT / "include" / "kernel"), str(app),
            "-L", str(ROOT / "lsdem2.0_b200"), "-llsdem_b200", "-Xlinker", "-rpath", "-Xlinker",
-           str(ROOT / "lsdem2.0_b200"), "-o", str(OURS)]
-    OURS.parent.mkdir(exist_ok=True)
+           str(ROOT / "lsdem2.0_b200"), "-o", str(out)]
+    out.parent.mkdir(exist_ok=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
 
@@ -93,3 +103,55 @@ def test_config0_same_gpu(lsdem, tmp_path):
     assert np.abs(v1 - v0).max() <= 1e-9 * vmax, np.abs(v1 - v0).max() / vmax
     print(f"config 0, {len(sc['pos'])} ellipsoids, steps {k0}..{k1}: reference build {ms0 / w0:.4f} ms/step, "
           f"this solver (FP64) {ms1 / w1:.4f} ms/step, ratio {ms0 / ms1:.2f}x")
+
+
+def write_scene_c2(path, sc, nsteps, k0, k1):
+    t = sc["templates"][0]
+    n = len(sc["pos"])
+    d = lambda a: np.ascontiguousarray(a, np.float64).tobytes()
+    i32 = lambda *v: struct.pack(f"<{len(v)}i", *v)
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+    b = sc["bonds"]
+    with open(path, "wb") as fh:
+        fh.write(b"LSDEMC2\0")
+        fh.write(i32(len(t["nodes"]), *[int(v) for v in t["size"]]) + d([t["spacing"]]) + d(t["origin"]))
+        fh.write(d(t["nodes"]) + d(t["sdf"]))
+        fh.write(i32(n) + d(sc["pos"]) + d(sc["quat"]) + d(sc["vel"]))
+        fh.write(d([sc["kn"], sc["ks"], sc["mu"], sc["e"], 2500.0]))
+        fh.write(i32(len(sc["walls"])))
+        for w in sc["walls"]:
+            fh.write(i32(*[int(v) for v in w["size"]]) + d([w["spacing"]]) + d(w["origin"]) + d(w["sdf"]))
+            fh.write(d(w["pos"]) + d(w["quat"]) + d([w["mu"], w["e"]]))
+            fh.write(d(w["vel"] if w.get("vel") is not None else np.zeros(3)))
+            fh.write(i32(len(w["verts"]), len(tris)) + d(w["verts"]) + tris.tobytes())
+        nb = len(b["master"])
+        ids = np.stack([b["master"], b["slave"]], 1).astype(np.int32)
+        fh.write(i32(nb) + ids.tobytes() + d(b["point"]) + d(b["normal"]) + d(b["radius"]) + d(b["length"]))
+        fh.write(d(b["tensile"]) + d(b["cohesion"]) + d([b["youngs"], b["poisson"], b["mu"]]))
+        fh.write(d([sc["dt"]]) + d(sc["min"]) + d(sc["max"]) + d(sc["gravity"]))
+        fh.write(i32(nsteps, k0, k1))
+
+
+@pytest.mark.skipif(not FUNDEM2.exists(), reason="oracle/_ref/c2_bench_fundem not built (needs the reference tree)")
+@pytest.mark.skipif(shutil.which("nvcc") is None and not OURS2.exists(), reason="nvcc not available")
+def test_config2_bonded_same_gpu(lsdem, tmp_path):
+    from lsdem_b200 import scenes
+    build_ours(APP2, OURS2)
+    sc = scenes.bonded_hcp(lsdem, n=8000)
+    nsteps, k0, k1 = 120, 20, 120
+    scene = tmp_path / "c2.bin"
+    write_scene_c2(scene, sc, nsteps, k0, k1)
+    res = {}
+    for name, binary in (("fundem", FUNDEM2), ("b200", OURS2)):
+        out = tmp_path / name
+        out.mkdir()
+        res[name] = run(binary, scene, out, tmp_path / f"{name}.res")
+    (s0, w0, ms0, v0), (s1, w1, ms1, v1) = res["fundem"], res["b200"]
+    assert s0 >= k1 and s1 >= k1 and w0 == w1 == k1 - k0
+    assert v0.shape == v1.shape == (len(sc["pos"]), 3)
+    vmax = np.abs(v0).max()
+    err = np.abs(v1 - v0).max() / vmax
+    assert err <= 1e-6, err
+    print(f"config 2 (bonded, {len(sc['pos'])} ellipsoids, {len(sc['bonds']['master'])} bonds), steps {k0}..{k1}: "
+          f"reference build {ms0 / w0:.4f} ms/step, this solver (FP64) {ms1 / w1:.4f} ms/step, "
+          f"ratio {ms0 / ms1:.2f}x, velocity difference {err:.2e} of the largest")
