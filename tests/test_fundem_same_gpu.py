@@ -16,9 +16,11 @@ Config 2 (tests/apps/c2_bench.cpp, oracle/_ref/c2_bench_fundem): aligned ellipso
 1.2 mm, 32^3 grids, 1,000 nodes) on the jittered HCP lattice with a V-bond to every lattice
 neighbour, a floor and a top wall moving down at 0.1 m/s, added through addLSParticle (density),
 addWall, setFixedVelocityToWall and addBondedInteraction, at a reduced count of 8,000
-particles: the reference keeps a full SDF copy per particle in host and device memory (Q14),
-2.1 GB here, 13 GB at the configuration's 50,000.
+particles by default: the reference keeps a full SDF copy per particle in host and device
+memory (Q14), 2.1 GB here, 13 GB at the configuration's 50,000 (LSDEM_C2_PARTICLES=50000 runs
+that size).
 """
+import os
 import shutil
 import struct
 import subprocess
@@ -137,7 +139,7 @@ def write_scene_c2(path, sc, nsteps, k0, k1):
 def test_config2_bonded_same_gpu(lsdem, tmp_path):
     from lsdem_b200 import scenes
     build_ours(APP2, OURS2)
-    sc = scenes.bonded_hcp(lsdem, n=8000)
+    sc = scenes.bonded_hcp(lsdem, n=int(os.environ.get("LSDEM_C2_PARTICLES", "8000")))
     nsteps, k0, k1 = 120, 20, 120
     scene = tmp_path / "c2.bin"
     write_scene_c2(scene, sc, nsteps, k0, k1)
