@@ -4,8 +4,9 @@
 // overrides addExternalForceTorque and launches kernels on
 // getLSParticle().force() etc.) compile against this header unchanged.
 //
-// Output: each frame writes the particle centres with velocity, angular
-// velocity and particle id as a VTU point set under <dir>_phase<k>/LSParticle/.
+// Output: each frame writes the reference's VTU files (surface-node mesh and
+// particle centres, contacts, bonds, walls, wall contacts) under <dir>_phase<k>/,
+// produced on the GPU by lsdem_write_vtu.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -66,18 +67,20 @@ class LSSolver {
                      const double normalStiffness, const double shearStiffness, const double frictionCoefficient,
                      const double restitutionCoefficient, const double density,
                      const std::vector<int3>& boundaryNodeConnectivity = {}) {
-    (void)boundaryNodeConnectivity;
     const int sz[3] = {gridNodeSize.x, gridNodeSize.y, gridNodeSize.z};
     const double o[3] = {gridNodeLocalOrigin.x, gridNodeLocalOrigin.y, gridNodeLocalOrigin.z};
     const double p[3] = {position.x, position.y, position.z};
     const double v[3] = {velocity.x, velocity.y, velocity.z};
     const double w[3] = {angularVelocity.x, angularVelocity.y, angularVelocity.z};
     const double q[4] = {orientation.q0, orientation.q1, orientation.q2, orientation.q3};
-    report(lsdem_add_ls_particle(h_, (const double*)boundaryNodeLocalPosition.data(),
-                                 (int)boundaryNodeLocalPosition.size(), gridNodeSignedDistance.data(), sz, o,
-                                 gridNodeSpacing, p, v, w, q, normalStiffness, shearStiffness, frictionCoefficient,
-                                 restitutionCoefficient, density, nullptr),
-           "[LSParticle] ");
+    int index = -1;
+    if (report(lsdem_add_ls_particle(h_, (const double*)boundaryNodeLocalPosition.data(),
+                                     (int)boundaryNodeLocalPosition.size(), gridNodeSignedDistance.data(), sz, o,
+                                     gridNodeSpacing, p, v, w, q, normalStiffness, shearStiffness, frictionCoefficient,
+                                     restitutionCoefficient, density, &index),
+               "[LSParticle] "))
+      return;
+    setTriangles(0, index, boundaryNodeConnectivity);
   }
 
   // Explicit mass and inertia overload (LSSolver.h:190-223).
@@ -88,7 +91,6 @@ class LSSolver {
                      const double mass, const symMatrix inertiaTensor, const double normalStiffness,
                      const double shearStiffness, const double frictionCoefficient,
                      const double restitutionCoefficient, const std::vector<int3>& boundaryNodeConnectivity = {}) {
-    (void)boundaryNodeConnectivity;
     const int sz[3] = {gridNodeSize.x, gridNodeSize.y, gridNodeSize.z};
     const double o[3] = {gridNodeLocalOrigin.x, gridNodeLocalOrigin.y, gridNodeLocalOrigin.z};
     int shape = -1;
@@ -104,9 +106,12 @@ class LSSolver {
     const double v[3] = {velocity.x, velocity.y, velocity.z};
     const double w[3] = {angularVelocity.x, angularVelocity.y, angularVelocity.z};
     const double q[4] = {orientation.q0, orientation.q1, orientation.q2, orientation.q3};
-    report(lsdem_add_particles(h_, 1, &shape, nullptr, p, v, w, q, &invm, I6, &normalStiffness, &shearStiffness,
-                               &frictionCoefficient, &restitutionCoefficient, nullptr),
-           "[LSParticle] ");
+    int index = -1;
+    if (report(lsdem_add_particles(h_, 1, &shape, nullptr, p, v, w, q, &invm, I6, &normalStiffness, &shearStiffness,
+                                   &frictionCoefficient, &restitutionCoefficient, &index),
+               "[LSParticle] "))
+      return;
+    setTriangles(0, index, boundaryNodeConnectivity);
   }
 
   // Fixed level-set wall (LSSolver.h:245-272).
@@ -115,15 +120,17 @@ class LSSolver {
                const int3 gridNodeSize, const double gridNodeSpacing, const double3 position,
                const quaternion orientation, const double frictionCoefficient,
                const double restitutionCoefficient = 1.) {
-    (void)objTriangleVertexID;
     const int sz[3] = {gridNodeSize.x, gridNodeSize.y, gridNodeSize.z};
     const double o[3] = {gridNodeLocalOrigin.x, gridNodeLocalOrigin.y, gridNodeLocalOrigin.z};
     const double p[3] = {position.x, position.y, position.z};
     const double q[4] = {orientation.q0, orientation.q1, orientation.q2, orientation.q3};
-    report(lsdem_add_wall(h_, (const double*)objVertexLocalPosition.data(), (int)objVertexLocalPosition.size(),
-                          gridNodeSignedDistance.data(), sz, o, gridNodeSpacing, p, q, frictionCoefficient,
-                          restitutionCoefficient, nullptr),
-           "[LSParticle] ");
+    int index = -1;
+    if (report(lsdem_add_wall(h_, (const double*)objVertexLocalPosition.data(), (int)objVertexLocalPosition.size(),
+                              gridNodeSignedDistance.data(), sz, o, gridNodeSpacing, p, q, frictionCoefficient,
+                              restitutionCoefficient, &index),
+               "[LSParticle] "))
+      return;
+    setTriangles(1, index, objTriangleVertexID);
   }
 
   void moveLSParticle(const size_t index, const double3 offSet) {
@@ -204,6 +211,7 @@ class LSSolver {
     if (report(rc, "[Solver] ")) return;
     bindView();
     lsdem_set_record_contacts(h_, 1);
+    clearOutput();
     std::cout << "[Solver] Upload Completed" << std::endl;
     const size_t numStep = size_t(maximumTime / timeStep) + 1;
     size_t frameInterval = numStep;
@@ -262,38 +270,31 @@ class LSSolver {
     dir_ = (d / p).string();
   }
 
+  // Triangles of a body's nodes, kept for the mesh files (LSParticle::add, LSParticle.h:165-172).
+  void setTriangles(int kind, int index, const std::vector<int3>& tris) {
+    if (tris.empty() || index < 0) return;
+    report(lsdem_set_triangles(h_, kind, index, (const int*)tris.data(), (int)tris.size()), "[LSParticle] ");
+  }
+
+  std::string phaseDir() const { return dir_ + "_phase" + std::to_string(phase_); }
+
+  // removeVtuFiles of the four output directories at the start of a phase (LSSolver.h:600-612).
+  void clearOutput() {
+    for (const char* sub : {"LSParticle", "LSParticleInteraction", "Wall", "LSParticle-WallInteraction"}) {
+      const std::filesystem::path d = std::filesystem::path(phaseDir()) / sub;
+      std::error_code ec;
+      if (!std::filesystem::is_directory(d, ec)) continue;
+      for (const auto& e : std::filesystem::directory_iterator(d, ec))
+        if (e.path().extension() == ".vtu") std::filesystem::remove(e.path(), ec);
+    }
+  }
+
+  // One frame: the reference's six VTU files (LSSolver::output, LSSolver.h:637-665), written by
+  // the library from device state (lsdem_write_vtu).
   void output(size_t iFrame, size_t iStep, double time) {
     std::cout << "[Solver] Phase " << phase_ << ": ------ Frame " << iFrame << " at Time " << time << " ------ "
               << std::endl;
-    const size_t n = (size_t)lsdem_num(h_, 0);
-    std::vector<double> pos(3 * n), vel(3 * n), w(3 * n);
-    if (n && lsdem_get_state(h_, pos.data(), vel.data(), w.data(), nullptr, nullptr, nullptr) != LSDEM_OK) return;
-    const std::filesystem::path dir = std::filesystem::path(dir_ + "_phase" + std::to_string(phase_)) / "LSParticle";
-    std::error_code ec;
-    std::filesystem::create_directories(dir, ec);
-    std::ostringstream fn;
-    fn << "LSParticleCenter_" << std::setw(4) << std::setfill('0') << iFrame << ".vtu";
-    std::ofstream f(dir / fn.str());
-    if (!f) return;
-    f << std::setprecision(10);
-    f << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\">\n"
-      << "<UnstructuredGrid>\n<FieldData><DataArray type=\"Float64\" Name=\"TIME\" NumberOfTuples=\"1\" "
-         "format=\"ascii\">"
-      << time << "</DataArray><DataArray type=\"Int64\" Name=\"STEP\" NumberOfTuples=\"1\" format=\"ascii\">" << iStep
-      << "</DataArray></FieldData>\n<Piece NumberOfPoints=\"" << n << "\" NumberOfCells=\"0\">\n<Points>\n"
-      << "<DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
-    for (size_t i = 0; i < 3 * n; ++i) f << pos[i] << (i % 3 == 2 ? "\n" : " ");
-    f << "</DataArray>\n</Points>\n<PointData>\n<DataArray type=\"Int32\" Name=\"particleID\" format=\"ascii\">\n";
-    for (size_t i = 0; i < n; ++i) f << i << "\n";
-    f << "</DataArray>\n<DataArray type=\"Float64\" Name=\"velocity\" NumberOfComponents=\"3\" format=\"ascii\">\n";
-    for (size_t i = 0; i < 3 * n; ++i) f << vel[i] << (i % 3 == 2 ? "\n" : " ");
-    f << "</DataArray>\n<DataArray type=\"Float64\" Name=\"angularVelocity\" NumberOfComponents=\"3\" "
-         "format=\"ascii\">\n";
-    for (size_t i = 0; i < 3 * n; ++i) f << w[i] << (i % 3 == 2 ? "\n" : " ");
-    f << "</DataArray>\n</PointData>\n<Cells><DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\">"
-      << "</DataArray><DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\"></DataArray>"
-      << "<DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\"></DataArray></Cells>\n"
-      << "</Piece>\n</UnstructuredGrid>\n</VTKFile>\n";
+    report(lsdem_write_vtu(h_, phaseDir().c_str(), iFrame, iStep, time), "[Solver] ");
   }
 
   lsdem_solver* h_ = nullptr;

@@ -277,6 +277,34 @@ int lsdem_mlp_gradient(int device, int n, const float* params, const float* pts,
 int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic,
                    unsigned long long seed, int max_tries, const int* keep, double* pos_out);
 
+/* Triangles of a body's nodes (kind 0: particle, its surface nodes in the order
+ * given at insertion; kind 1: wall, its vertices), kept for the mesh files of
+ * lsdem_write_vtu: the boundaryNodeConnectivity / objTriangleVertexID argument of
+ * LSParticle::add (FunDEM/kernel/LSParticle.h:165-172) through addLSParticle and
+ * addWall (LSSolver.h:51-65, 245-254). tris: n_tris x 3 node indices of that body;
+ * n_tris = 0 clears them. Host only. */
+int lsdem_set_triangles(lsdem_solver* s, int kind, int index, const int* tris, int n_tris);
+
+/* One output frame: the VTU files of LSSolver::output (LSSolver.h:637-665) under
+ * the phase directory `dir`, with the reference's file names, layout, array
+ * names and types (inline base64 binary, UInt64 headers):
+ *   dir/LSParticle/LSObjectMesh_NNNN.vtu   surface nodes (world position,
+ *       particleID, velocity) and their triangles (LSParticle.h:311-506);
+ *   dir/LSParticle/Particle_NNNN.vtu       particle centres, velocity, angular
+ *       velocity, orientation, radius (LSParticle.h:508-654);
+ *   dir/LSParticleInteraction/LSInteraction_NNNN.vtu   particle contacts
+ *       (SolidInteraction.h:154-317);
+ *   dir/LSParticleInteraction/VBondedInteraction_NNNN.vtu   bonds, when there are
+ *       any (VBondedInteraction.h:262-448);
+ *   dir/Wall/LSObjectMesh_NNNN.vtu         wall vertices and triangles;
+ *   dir/LSParticle-WallInteraction/LSInteraction_NNNN.vtu  wall contacts.
+ * Arrays are computed and base64-encoded on the device in chunks of 32 MB, the
+ * encoded chunks copied through two pinned buffers while the previous chunk is
+ * written. Contacts need recorded geometry (lsdem_set_record_contacts). Returns
+ * when the files are written; the solver's stream is ordered before the writer. */
+int lsdem_write_vtu(lsdem_solver* s, const char* dir, unsigned long long frame, unsigned long long step,
+                    double time);
+
 /* Broadphase cell sort that allocates no device memory: cell keys of n body
  * centres (pos_dev: device array of n x 3 doubles), their stable sorted order
  * and per-cell [start, end) (-1 when empty) for the grid (min, max, inverse

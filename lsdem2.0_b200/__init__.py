@@ -107,6 +107,8 @@ _SIGS = {
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
     "lsdem_mesh_grid_box": (C.c_int, [DP, C.c_int, C.c_double, C.c_int, DP, IP]),
+    "lsdem_set_triangles": (C.c_int, [P, C.c_int, C.c_int, IP, C.c_int]),
+    "lsdem_write_vtu": (C.c_int, [P, C.c_char_p, C.c_ulonglong, C.c_ulonglong, C.c_double]),
     "lsdem_mesh_grid": (C.c_int, [DP, C.c_int, IP, C.c_int, DP, IP, C.c_double, C.c_int, DP, C.c_int]),
 }
 for _name, (_res, _args) in _SIGS.items():
@@ -300,6 +302,16 @@ class Solver:
 
     def set_periodic(self, axes: int):
         self._chk(lib.lsdem_set_periodic(self.h, int(axes)), "set_periodic")
+
+    def set_triangles(self, kind, index, tris):
+        """Triangles of a body's nodes (kind 0 particle, 1 wall) for the mesh output files."""
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        self._chk(lib.lsdem_set_triangles(self.h, int(kind), int(index), _i(t), len(t)), "set_triangles")
+
+    def write_vtu(self, directory, frame, step, time):
+        """The reference's output files of one frame under `directory` (LSSolver::output)."""
+        self._chk(lib.lsdem_write_vtu(self.h, str(directory).encode(), int(frame), int(step), float(time)),
+                  "write_vtu")
 
     def set_capacity(self, pp=0, wall=0, ghost=0, contacts=0, batch=0):
         self._chk(lib.lsdem_set_capacity(self.h, int(pp), int(wall), int(ghost), int(contacts), int(batch)),

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
+#include <vector>
 #include "common.cuh"
 #include "mlp.cuh"
 
@@ -231,4 +233,41 @@ struct BondView {
 };
 void launch_bonds(const StepArgs& a, const BondView& b, cudaStream_t s);
 
+
+// ---------------------------------------------------------------------------
+// Frame output (csrc/vtu.cu): what the writer needs of one solver's frame.
+struct VtuError { std::string msg; };
+struct VtuContacts { std::vector<double> point, normal, spring, en_n, en_s; };
+struct VtuInput {
+  std::string dir;                 // phase directory; the files go to its four subdirectories
+  unsigned long long frame = 0, step = 0;
+  double time = 0.;
+  cudaStream_t solver_stream = nullptr;
+  long long layout = 0;            // changes whenever bodies, templates or triangles change
+  int n = 0;                       // particles; device state in particle order
+  const double3* pos = nullptr;
+  const double3* vel = nullptr;
+  const double3* angvel = nullptr;
+  const Quat* quat = nullptr;
+  const double* radius = nullptr;  // device
+  const long long* node_base = nullptr;  // host, n + 1, caller node order
+  const int* shape = nullptr;      // host
+  const double* scale = nullptr;   // host
+  std::vector<const std::vector<double>*> tnodes;    // per shape, caller order
+  const int* tri_set = nullptr;    // host, per particle (-1: no triangles)
+  std::vector<const std::vector<int>*> tri_sets;
+  int nw = 0;                      // walls; host state
+  const double* wpos = nullptr;
+  const double* wquat = nullptr;
+  const double* wvel = nullptr;
+  const double* wangvel = nullptr;
+  std::vector<const std::vector<double>*> wall_verts;
+  std::vector<const std::vector<int>*> wall_tris;    // null: no triangles
+  VtuContacts pp, pw;
+  std::vector<int> bond_ids, bond_bonded;
+  std::vector<double> bond_state;
+};
+struct VtuCtx;
+void vtu_write(VtuCtx*& ctx, const VtuInput& in);
+void vtu_free(VtuCtx* ctx);
 }  // namespace lsdem

@@ -318,6 +318,14 @@ struct lsdem_solver {
   std::map<std::pair<int, uint64_t>, double> radius_cache;  // (shape, scale bits) -> radius
   BodyHost P, W;
   BondHost bonds;
+  // frame output: wall vertices (local frame), triangle sets of the bodies' nodes
+  // (LSParticle::add's boundaryNodeConnectivity, LSParticle.h:165-172), the writer
+  std::vector<std::vector<double>> wall_verts;
+  std::vector<std::vector<int>> tri_sets;
+  std::map<std::vector<int>, int> tri_set_of;
+  std::vector<int> P_tris, W_tris;  // per body: triangle set, -1 none
+  long long vtu_layout = 0;
+  VtuCtx* vtu = nullptr;
   int periodic = 0;
   double dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0}, grav[3] = {0, 0, 0};
   // device
@@ -1202,6 +1210,7 @@ int lsdem_create(int device, void* stream, lsdem_solver** out) {
 void lsdem_destroy(lsdem_solver* s) {
   if (!s) return;
   if (s->ready) cudaStreamSynchronize(s->stream);
+  if (s->vtu) vtu_free(s->vtu);
   delete s;
 }
 
@@ -1294,6 +1303,7 @@ int lsdem_add_wall(lsdem_solver* s, const double* verts, int n_verts, const doub
     for (int i = 0; i < n_verts; ++i) r = std::max(r, hlen(v3(verts + 3 * i)));
     if (index) *index = s->W.n();
     push_body(s, s->W, sh, 1.0, pos, nullptr, nullptr, quat, 0., nullptr, 0., 0., mu, e, r);
+    s->wall_verts.emplace_back(verts, verts + 3 * (size_t)std::max(n_verts, 0));
     s->ready = false;
     return LSDEM_OK;
   });
@@ -1594,6 +1604,7 @@ int lsdem_initialize(lsdem_solver* s, const double* min3, const double* max3, co
     s->dmax[a] = max3[a];
     s->grav[a] = gravity3 ? gravity3[a] : 0.;
   }
+  ++s->vtu_layout;
   return guard(s, [&] {
     initialize(s);
     return LSDEM_OK;
@@ -1990,6 +2001,98 @@ int lsdem_get_screen_stats(lsdem_solver* s, long long* out8) {
 // Random sequential addition of spheres (largest first, in the given order)
 // in the box [lo, hi), optionally periodic, using a uniform cell list.
 // Returns LSDEM_ERR_ARG when a sphere cannot be placed in max_tries.
+// ---------------------------------------------------------------------------
+// Frame output
+
+int lsdem_set_triangles(lsdem_solver* s, int kind, int index, const int* tris, int n_tris) {
+  if (!s || (kind != 0 && kind != 1) || n_tris < 0 || (n_tris > 0 && !tris)) return LSDEM_ERR_ARG;
+  const int nb = kind == 0 ? s->P.n() : s->W.n();
+  if (index < 0 || index >= nb) return fail(s, LSDEM_ERR_ARG, "body index out of range");
+  const int nn = kind == 0 ? (int)(s->shapes[s->P.shape[index]].nodes.size() / 3)
+                           : (int)(s->wall_verts[index].size() / 3);
+  for (int k = 0; k < 3 * n_tris; ++k)
+    if (tris[k] < 0 || tris[k] >= nn) return fail(s, LSDEM_ERR_ARG, "triangle vertex index out of range");
+  std::vector<int>& ids = kind == 0 ? s->P_tris : s->W_tris;
+  if ((int)ids.size() < nb) ids.resize(nb, -1);
+  if (n_tris == 0) {
+    ids[index] = -1;
+  } else {
+    std::vector<int> t(tris, tris + 3 * (size_t)n_tris);
+    auto it = s->tri_set_of.find(t);
+    if (it == s->tri_set_of.end()) {
+      it = s->tri_set_of.emplace(t, (int)s->tri_sets.size()).first;
+      s->tri_sets.push_back(std::move(t));
+    }
+    ids[index] = it->second;
+  }
+  ++s->vtu_layout;
+  return LSDEM_OK;
+}
+
+int lsdem_write_vtu(lsdem_solver* s, const char* dir, unsigned long long frame, unsigned long long step, double time) {
+  if (!s || !dir) return LSDEM_ERR_ARG;
+  if (!s->ready) return fail(s, LSDEM_ERR_STATE, "write_vtu before initialize");
+  return guard(s, [&] {
+    VtuInput in;
+    in.dir = dir;
+    in.frame = frame; in.step = step; in.time = time;
+    in.solver_stream = s->stream;
+    in.layout = s->vtu_layout;
+    const int n = s->P.n();
+    in.n = n;
+    in.pos = s->dP.pos.p; in.vel = s->dP.vel.p; in.angvel = s->dP.angvel.p;
+    in.quat = reinterpret_cast<const Quat*>(s->dP.quat.p);
+    in.radius = s->dP.radius.p;
+    std::vector<long long> nbase(n + 1, 0);
+    for (int i = 0; i < n; ++i) nbase[i + 1] = nbase[i] + (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3);
+    in.node_base = nbase.data();
+    in.shape = s->P.shape.data();
+    in.scale = s->P.scale.data();
+    for (const ShapeHost& sh : s->shapes) in.tnodes.push_back(&sh.nodes);
+    std::vector<int> ptris(s->P_tris);
+    ptris.resize(n, -1);
+    in.tri_set = ptris.data();
+    for (const auto& t : s->tri_sets) in.tri_sets.push_back(&t);
+    // walls: current state (few), vertices and triangles
+    const int nw = s->W.n();
+    in.nw = nw;
+    std::vector<double> wp(3 * nw), wv(3 * nw), ww(3 * nw), wq(4 * nw);
+    if (nw) {
+      int rc = lsdem_get_wall_state(s, wp.data(), wv.data(), ww.data(), wq.data());
+      if (rc) throw Fail{rc, "wall state"};
+    }
+    in.wpos = wp.data(); in.wvel = wv.data(); in.wangvel = ww.data(); in.wquat = wq.data();
+    for (int w = 0; w < nw; ++w) {
+      in.wall_verts.push_back(&s->wall_verts[w]);
+      const int k = w < (int)s->W_tris.size() ? s->W_tris[w] : -1;
+      in.wall_tris.push_back(k < 0 ? nullptr : &s->tri_sets[k]);
+    }
+    // contacts of the particle and wall lists, as recorded at the last step
+    for (int kind : {LSDEM_CONTACT_PARTICLE, LSDEM_CONTACT_WALL}) {
+      long long m = 0;
+      lsdem_count_contacts(s, kind, &m);
+      if (m > 0 && !s->con[s->hp].geom) throw Fail{LSDEM_ERR_STATE, "contact geometry not recorded (lsdem_set_record_contacts)"};
+      VtuContacts& c = kind == LSDEM_CONTACT_PARTICLE ? in.pp : in.pw;
+      c.point.resize(3 * m); c.normal.resize(3 * m); c.spring.resize(3 * m); c.en_n.resize(m); c.en_s.resize(m);
+      std::vector<double> ov(m);
+      if (m > 0) {
+        int rc = lsdem_get_contacts(s, kind, m, nullptr, nullptr, nullptr, c.spring.data(), c.point.data(),
+                                    c.normal.data(), ov.data(), c.en_n.data(), c.en_s.data());
+        if (rc) throw Fail{rc, "contacts"};
+      }
+    }
+    const size_t nbd = s->bonds.bonded.size();
+    in.bond_ids.resize(2 * nbd); in.bond_bonded.resize(nbd); in.bond_state.resize(9 * nbd);
+    if (nbd) lsdem_get_bonds(s, in.bond_ids.data(), in.bond_bonded.data(), in.bond_state.data());
+    try {
+      vtu_write(s->vtu, in);
+    } catch (const VtuError& e) {
+      throw Fail{LSDEM_ERR_CUDA, "write_vtu: " + e.msg};
+    }
+    return LSDEM_OK;
+  });
+}
+
 int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* hi, int periodic, unsigned long long seed,
                    int max_tries, const int* keep, double* pos_out) {
   if (n < 0 || !radius || !lo || !hi || !pos_out) return LSDEM_ERR_ARG;

@@ -45,3 +45,34 @@ def history_from_gpu(c, n_nodes_total):
     cnt = np.bincount(node, minlength=n_nodes_total)
     return {"prefix": np.cumsum(cnt).astype(np.int32), "partner": np.asarray(c["partner"], np.int32)[order],
             "spring": np.asarray(c["spring"])[order]}
+
+
+def read_vtu(path):
+    """Arrays of a VTK XML UnstructuredGrid file with inline base64 binary arrays (UInt64 byte-count
+    header) or ascii arrays: {"TIME", "STEP", "points", "connectivity", "offsets", "types", and the
+    PointData arrays by name}."""
+    import base64
+    import xml.etree.ElementTree as ET
+
+    types = {"Float32": np.float32, "Float64": np.float64, "Int32": np.int32, "Int64": np.int64, "UInt8": np.uint8}
+    root = ET.parse(path).getroot()
+    out = {}
+    piece = root.find("UnstructuredGrid/Piece")
+    out["n_points"] = int(piece.get("NumberOfPoints"))
+    out["n_cells"] = int(piece.get("NumberOfCells"))
+    for da in root.iter("DataArray"):
+        dt = types[da.get("type")]
+        nc = int(da.get("NumberOfComponents", "1"))
+        text = (da.text or "").strip()
+        if da.get("format") == "binary":
+            raw = base64.b64decode(text)
+            nbytes = int(np.frombuffer(raw[:8], "<u8")[0])
+            assert len(raw) == 8 + nbytes, (path, da.get("Name"), len(raw), nbytes)
+            a = np.frombuffer(raw[8:8 + nbytes], dt)
+        else:
+            a = np.array(text.split(), dt)
+        if nc > 1:
+            a = a.reshape(-1, nc)
+        name = da.get("Name")
+        out[name if name else "points"] = a
+    return out

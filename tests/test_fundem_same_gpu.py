@@ -9,8 +9,11 @@ scene file; each reports the device time of a fixed window of steps, measured wi
 events recorded from the external-force hook (called by both solvers every step between
 the forces and the second half kick), and the particle velocities at the window's end.
 
-Checked: the velocities agree to FP64 round-off (same algorithm, same inputs). The two
-timings are printed (they are reported, not asserted).
+Checked: the velocities agree to FP64 round-off (same algorithm, same inputs), and the output
+frames the two solvers write (the reference's VTU files: surface-node mesh, particles, contacts,
+bonds, walls, wall contacts) are the same files with the same XML structure and equal arrays
+(float32 values to 1e-5 of the scale, integers exact, contacts as sets). The two timings are
+printed (they are reported, not asserted).
 
 Config 2 (tests/apps/c2_bench.cpp, oracle/_ref/c2_bench_fundem): aligned ellipsoids (2, 1.6,
 1.2 mm, 32^3 grids, 1,000 nodes) on the jittered HCP lattice with a V-bond to every lattice
@@ -73,6 +76,52 @@ def write_scene(path, sc, nsteps, k0, k1):
         fh.write(i32(nsteps, k0, k1))
 
 
+def _structure(path):
+    """Element tags and attributes of a VTU file, array payloads left out."""
+    import xml.etree.ElementTree as ET
+    out = []
+    for el in ET.parse(path).getroot().iter():
+        attrs = dict(el.attrib)
+        if el.tag == "DataArray" and attrs.get("format") == "ascii":
+            attrs["value"] = (el.text or "").strip()
+        out.append((el.tag, tuple(sorted(attrs.items()))))
+    return out
+
+
+def compare_frames(dir_ref, dir_ours, scale):
+    """The last frame's files of both solvers: the same files, the same XML structure, equal
+    arrays (float32 casts of FP64 values that agree to round-off), contacts as sets."""
+    from helpers import read_vtu
+    ref = {p.relative_to(dir_ref): p for p in dir_ref.rglob("*.vtu")}
+    ours = {p.relative_to(dir_ours): p for p in dir_ours.rglob("*.vtu")}
+    assert sorted(ref) == sorted(ours), (sorted(ref), sorted(ours))
+    last = max(int(p.stem.split("_")[-1]) for p in ref)
+    checked = []
+    for rel in sorted(ref):
+        if int(rel.stem.split("_")[-1]) != last:
+            continue
+        assert _structure(ref[rel]) == _structure(ours[rel]), rel
+        a, b = read_vtu(ref[rel]), read_vtu(ours[rel])
+        assert a["n_points"] == b["n_points"] and a["n_cells"] == b["n_cells"], rel
+        if rel.name.startswith("LSInteraction"):
+            oa, ob = np.lexsort(a["points"].T[::-1]), np.lexsort(b["points"].T[::-1])
+        else:
+            oa = ob = slice(None)
+        for k, v in a.items():
+            if k in ("n_points", "n_cells", "connectivity", "offsets", "types") and rel.name.startswith("LSInteraction"):
+                continue
+            va, vb = np.asarray(v), np.asarray(b[k])
+            if va.ndim and len(va) == a["n_points"] and va.size:
+                va, vb = va[oa], vb[ob]
+            if va.dtype.kind == "f":
+                s = scale if k in ("points",) else max(float(np.abs(va).max(initial=0.0)), 1e-30)
+                assert np.abs(va.astype(np.float64) - vb).max(initial=0.0) <= 1e-5 * s, (rel, k)
+            else:
+                assert np.array_equal(va, vb), (rel, k)
+        checked.append(str(rel))
+    return checked
+
+
 def run(binary, scene, outdir, result):
     r = subprocess.run([str(binary), str(scene), str(outdir), str(result)], capture_output=True, text=True,
                        timeout=900)
@@ -103,6 +152,8 @@ def test_config0_same_gpu(lsdem, tmp_path):
     assert v0.shape == v1.shape == (len(sc["pos"]), 3)
     vmax = np.abs(v0).max()
     assert np.abs(v1 - v0).max() <= 1e-9 * vmax, np.abs(v1 - v0).max() / vmax
+    files = compare_frames(tmp_path / "fundem_phase1", tmp_path / "b200_phase1", float(np.abs(sc["max"]).max()))
+    print("frame files equal to the reference build's:", ", ".join(files))
     print(f"config 0, {len(sc['pos'])} ellipsoids, steps {k0}..{k1}: reference build {ms0 / w0:.4f} ms/step, "
           f"this solver (FP64) {ms1 / w1:.4f} ms/step, ratio {ms0 / ms1:.2f}x")
 
@@ -140,7 +191,8 @@ def test_config2_bonded_same_gpu(lsdem, tmp_path):
     from lsdem_b200 import scenes
     build_ours(APP2, OURS2)
     sc = scenes.bonded_hcp(lsdem, n=int(os.environ.get("LSDEM_C2_PARTICLES", "8000")))
-    nsteps, k0, k1 = 120, 20, 120
+    # frames are written at steps 0, 119 and 120: the window (20, 110] times steps only
+    nsteps, k0, k1 = 120, 20, 110
     scene = tmp_path / "c2.bin"
     write_scene_c2(scene, sc, nsteps, k0, k1)
     res = {}
@@ -154,6 +206,8 @@ def test_config2_bonded_same_gpu(lsdem, tmp_path):
     vmax = np.abs(v0).max()
     err = np.abs(v1 - v0).max() / vmax
     assert err <= 1e-6, err
+    files = compare_frames(tmp_path / "fundem_phase1", tmp_path / "b200_phase1", float(np.abs(sc["max"]).max()))
+    print("frame files equal to the reference build's:", ", ".join(files))
     print(f"config 2 (bonded, {len(sc['pos'])} ellipsoids, {len(sc['bonds']['master'])} bonds), steps {k0}..{k1}: "
           f"reference build {ms0 / w0:.4f} ms/step, this solver (FP64) {ms1 / w1:.4f} ms/step, "
           f"ratio {ms0 / ms1:.2f}x, velocity difference {err:.2e} of the largest")
