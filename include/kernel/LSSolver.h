@@ -174,9 +174,7 @@ class LSSolver {
   void addPeriodicBoundaryYD() { periodic_ |= 2; lsdem_set_periodic(h_, periodic_); }
   // Extension: the same image rule along z.
   void addPeriodicBoundaryZD() { periodic_ |= 4; lsdem_set_periodic(h_, periodic_); }
-  void addPeriodicBoundarySector() {
-    std::cerr << "[Solver] sector periodicity is not available in this build" << std::endl;
-  }
+  void addPeriodicBoundarySector() { periodic_ = LSDEM_PERIODIC_SECTOR; lsdem_set_periodic(h_, periodic_); }
   void removePeriodicBoundary() { periodic_ = 0; lsdem_set_periodic(h_, 0); }
 
   // Extension: arithmetic form of the narrowphase (LSDEM_PREC_FP64, the reference's,

@@ -134,7 +134,13 @@ int lsdem_set_precision(lsdem_solver* s, int mode);
 
 /* Periodic axes bit mask (bit 0 x, 1 y, 2 z). x and y follow
  * addPeriodicBoundaryXD/YD (LSSolver.h:426-447); z applies the same rule. 0 removes
- * periodicity (removePeriodicBoundary, LSSolver.h:459-464). */
+ * periodicity (removePeriodicBoundary, LSSolver.h:459-464). LSDEM_PERIODIC_SECTOR
+ * (alone) is the quarter-sector periodicity of addPeriodicBoundarySector
+ * (LSSolver.h:448-452, PeriodicBoundary.h:313-420): about the z axis through the
+ * domain minimum, particles leaving across x = min.x or y = min.y are turned by
+ * -/+90 degrees, images turned by 90, 180 and 270 degrees (contact image codes 8, 16,
+ * 32). Combined with x/y/z bits: LSDEM_ERR_ARG. */
+#define LSDEM_PERIODIC_SECTOR 8
 int lsdem_set_periodic(lsdem_solver* s, int axes);
 
 /* Uploads the model and builds the grids for the domain [min, max)

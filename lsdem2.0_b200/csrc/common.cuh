@@ -68,6 +68,45 @@ LD Quat quat_integrate(Quat q, double3 w, double dt) {
   return Quat{r.q0 * inv, r.q1 * inv, r.q2 * inv, r.q3 * inv};
 }
 
+// Rotation of v by the rotation vector om (axis om / |om|, angle |om|), Rodrigues'
+// formula with a second-order expansion below |om|^2 = 1e-20 and the device's rsqrt
+// and sincos, as the reference's device rotateVector (myVec.h:143-182).
+LD double3 rotate_vector_dev(double3 v, double3 om) {
+  const double theta2 = dot(om, om);
+  const double3 oxv = cross(om, v);
+  const double3 oxoxv = cross(om, oxv);
+  if (is_zero(theta2)) return v + oxv + 0.5 * oxoxv;
+  const double inv = rsqrt(theta2);
+  const double theta = theta2 * inv;
+  double s, c;
+  sincos(theta, &s, &c);
+  const double A = s * inv;
+  const double B = (1.0 - c) * (inv * inv);
+  return v + A * oxv + B * oxoxv;
+}
+
+// q turned by the rotation vector om in the global frame, rot(om) * q, normalised
+// with the device's rsqrt (rotateQuaternion, myQua.h:131-179).
+LD Quat rotate_quaternion_dev(Quat q, double3 om) {
+  const double theta2 = om.x * om.x + om.y * om.y + om.z * om.z;
+  if (is_zero(theta2)) return q;
+  const double theta = sqrt(theta2);
+  const double inv = 1.0 / theta;
+  const double ux = om.x * inv, uy = om.y * inv, uz = om.z * inv;
+  const double half = 0.5 * theta;
+  const double c = cos(half), s = sin(half);
+  const double r0 = c, r1 = s * ux, r2 = s * uy, r3 = s * uz;
+  Quat r;
+  r.q0 = r0 * q.q0 - r1 * q.q1 - r2 * q.q2 - r3 * q.q3;
+  r.q1 = r0 * q.q1 + r1 * q.q0 + r2 * q.q3 - r3 * q.q2;
+  r.q2 = r0 * q.q2 - r1 * q.q3 + r2 * q.q0 + r3 * q.q1;
+  r.q3 = r0 * q.q3 + r1 * q.q2 - r2 * q.q1 + r3 * q.q0;
+  const double l2 = r.q0 * r.q0 + r.q1 * r.q1 + r.q2 * r.q2 + r.q3 * r.q3;
+  if (is_zero(l2)) return r;
+  const double il = rsqrt(l2);
+  return Quat{r.q0 * il, r.q1 * il, r.q2 * il, r.q3 * il};
+}
+
 HD Sym6 rotate_inv_inertia(Quat q, Sym6 I) {
   double q0 = q.q0, q1 = q.q1, q2 = q.q2, q3 = q.q3;
   double q11 = 2 * q1 * q1, q22 = 2 * q2 * q2, q33 = 2 * q3 * q3;

@@ -108,10 +108,14 @@ struct ContactView {
   double* en_s;
 };
 
-// Ghost images of the periodic boundary: up to 7 image sets.
+// Ghost images of the periodic boundary: up to 7 image sets (translations along x,
+// y, z and their combinations), or the 3 rotated sets of sector periodicity.
 struct GhostView {
   int nsets;
-  int mask[7];         // axes of each set (bit 0 x, 1 y, 2 z)
+  int mask[7];         // axes of each set (bit 0 x, 1 y, 2 z); sector sets 8, 16, 32 (90, 180, 270 degrees)
+  int sector;          // sector periodicity: images rotated about the z axis through the domain minimum
+  Quat* gquat;         // sector: nsets * n image orientations
+  double3* gvel;       // sector: nsets * n image velocities
   double3* gpos;       // nsets * n
   int* gkey;           // nsets * n, clamped cell or -1
   int* list;           // nsets * n: visible images (set * n + particle), compacted

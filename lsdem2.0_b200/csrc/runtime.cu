@@ -376,7 +376,8 @@ struct lsdem_solver {
   // periodic
   int nsets = 0;
   int set_mask[7] = {0};
-  DArr<double3> gpos;
+  DArr<double3> gpos, gvel;
+  DArr<Quat> gquat;
   DArr<int> gkey, key2, g2_idx, g2_start, g2_end, glist, gcount;
   // bonds
   DArr<int> b_ids, b_bonded;
@@ -799,10 +800,16 @@ void initialize(lsdem_solver* s) {
   alloc_bucket(s, n, s->pg.ncells);
   // periodic image sets: single axes in x, y, z order, then pairs, then xyz
   s->nsets = 0;
-  const int ax = s->periodic;
+  const int ax = s->periodic & 7;
   const int order[7] = {1, 2, 4, 3, 5, 6, 7};
   for (int k = 0; k < 7; ++k)
     if ((order[k] & ax) == order[k]) s->set_mask[s->nsets++] = order[k];
+  if (s->periodic & 8) {  // sector: images turned by 90, 180 and 270 degrees
+    s->nsets = 3;
+    s->set_mask[0] = 8; s->set_mask[1] = 16; s->set_mask[2] = 32;
+    CK(s->gquat.alloc((size_t)3 * std::max(n, 1)));
+    CK(s->gvel.alloc((size_t)3 * std::max(n, 1)));
+  }
   if (s->nsets > 0) {
     CK(s->gpos.alloc((size_t)s->nsets * std::max(n, 1)));
     CK(s->gkey.alloc((size_t)s->nsets * std::max(n, 1)));
@@ -888,6 +895,9 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.C_old = cv(s->con[old], false);
   a.G.nsets = s->nsets;
   for (int k = 0; k < 7; ++k) a.G.mask[k] = s->set_mask[k];
+  a.G.sector = (s->periodic & 8) ? 1 : 0;
+  a.G.gquat = s->gquat.p;
+  a.G.gvel = s->gvel.p;
   a.G.gpos = s->gpos.p;
   a.G.gkey = s->gkey.p;
   a.G.list = s->glist.p;
@@ -1570,7 +1580,9 @@ int lsdem_set_precision(lsdem_solver* s, int mode) {
 
 int lsdem_set_periodic(lsdem_solver* s, int axes) {
   if (!s) return LSDEM_ERR_ARG;
-  s->periodic = axes & 7;
+  if ((axes & 8) && (axes & 7))
+    return fail(s, LSDEM_ERR_ARG, "sector periodicity cannot be combined with x, y or z periodicity");
+  s->periodic = axes & 15;
   s->ready = false;
   return LSDEM_OK;
 }

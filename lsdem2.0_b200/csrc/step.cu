@@ -349,6 +349,12 @@ LD Partner load_partner(const StepArgs& a, int pid) {
     P.gs = a.S.gsize[sh]; P.sdf = a.S.sdf + a.S.sdf_off[sh]; P.sc = B.scale[i];
     P.real = i;
     P.v = B.vel[i]; P.w = B.angvel[i];
+    if (KIND == KIND_GHOST && a.G.sector) {
+      // rotated image: its own orientation and velocity; the angular velocity stays the
+      // particle's (addGhostLevelSetParticleContactForceTorqueKernel, contactKernel.cu:240-242)
+      P.q = a.G.gquat[(size_t)set * B.n + i];
+      P.v = a.G.gvel[(size_t)set * B.n + i];
+    }
     P.invm = B.invmass[i]; P.kn = B.kn[i]; P.ks = B.ks[i]; P.mu = B.mu[i]; P.res = B.res[i];
   }
   return P;
@@ -777,7 +783,7 @@ LD PairF make_pair_f(const StepArgs& a, int A, const Partner& P, int pshape, int
     ra[0] = r0.x; ra[1] = r0.y; ra[2] = r0.z; ra[3] = r1.x; ra[4] = r1.y; ra[5] = r1.z;
     ra[6] = r2.x; ra[7] = r2.y; ra[8] = r2.z;
   }
-  if (KIND == KIND_WALL) {
+  if (KIND == KIND_WALL || (KIND == KIND_GHOST && a.G.sector)) {
     double3 cb[3];
     rot_cols(P.q, cb);
     for (int j = 0; j < 3; ++j) {
@@ -1275,6 +1281,73 @@ LD int ghost_key(double3 p, const GridP& g) {
   return out ? lin3(c, g.size) : -1;
 }
 
+// Sector periodicity about the z axis through the domain minimum m: a particle
+// left of x = m.x (with y >= m.y) is turned by -90 degrees about that axis, one
+// below y = m.y (with x >= m.x) by +90 degrees: position about m, velocity and
+// orientation (updateVelocityPositionOrientationOutOfSectorKernel, mySpatialGrid.cu:58-85;
+// the angular velocity is left as it is, as there). The particle and wall forces of
+// the step were evaluated before the wrap with the pre-wrap state, so its force and
+// torque turn with it (the reference evaluates them after the wrap, which mixes the
+// frames as for translations). Images: a copy per set, turned by 90 degrees when the
+// particle is in the first cell row along y, by 270 (-90) degrees when in the first
+// cell column along x, and by 180 degrees when in both
+// (calculateSectorGhostVelocityPositionOrientationKernel, mySpatialGrid.cu:154-212).
+LD void sector_wrap_images(const StepArgs& a, int i, double3& p) {
+  const GridP& g = a.pg;
+  const int n = a.P.n;
+  const double hp = 0.5 * 3.14159265358979323846;
+  double3 v = a.P.vel[i];
+  Quat q = a.P.quat[i];
+  bool turned = false;
+  double3 om = d3(0., 0., 0.);
+  if (p.x < g.mn.x && p.y >= g.mn.y) {
+    om = d3(0., 0., -hp);
+    v = rotate_vector_dev(v, om);
+    p = g.mn + rotate_vector_dev(p - g.mn, om);
+    q = rotate_quaternion_dev(q, om);
+    a.P.force[i] = rotate_vector_dev(a.P.force[i], om);
+    a.P.torque[i] = rotate_vector_dev(a.P.torque[i], om);
+    turned = true;
+  }
+  if (p.y < g.mn.y && p.x >= g.mn.x) {
+    om = d3(0., 0., hp);
+    v = rotate_vector_dev(v, om);
+    p = g.mn + rotate_vector_dev(p - g.mn, om);
+    q = rotate_quaternion_dev(q, om);
+    a.P.force[i] = rotate_vector_dev(a.P.force[i], om);
+    a.P.torque[i] = rotate_vector_dev(a.P.torque[i], om);
+    turned = true;
+  }
+  if (turned) {
+    a.P.vel[i] = v;
+    a.P.quat[i] = q;
+    if (a.P.rotm) {
+      const double3 c0 = rotate(q, d3(1., 0., 0.)), c1 = rotate(q, d3(0., 1., 0.)), c2 = rotate(q, d3(0., 0., 1.));
+      a.P.rotm[3 * i] = make_float4((float)c0.x, (float)c1.x, (float)c2.x, 0.f);
+      a.P.rotm[3 * i + 1] = make_float4((float)c0.y, (float)c1.y, (float)c2.y, 0.f);
+      a.P.rotm[3 * i + 2] = make_float4((float)c0.z, (float)c1.z, (float)c2.z, 0.f);
+    }
+  }
+  double3 gp[3] = {p, p, p}, gv[3] = {v, v, v};
+  Quat gq[3] = {q, q, q};
+  const double ang[3] = {hp, 2.0 * hp, -hp};  // sets R90, R180, R270
+  const int3 c = cell_of(p, g);
+  const bool row = c.y == 0, col = c.x == 0;
+  for (int s = 0; s < 3; ++s) {
+    const bool on = s == 0 ? row : (s == 1 ? row && col : col);
+    if (!on) continue;
+    const double3 o = d3(0., 0., ang[s]);
+    gv[s] = rotate_vector_dev(v, o);
+    gp[s] = g.mn + rotate_vector_dev(p - g.mn, o);
+    gq[s] = rotate_quaternion_dev(q, o);
+  }
+  for (int s = 0; s < 3; ++s) {
+    a.G.gpos[(size_t)s * n + i] = gp[s];
+    a.G.gvel[(size_t)s * n + i] = gv[s];
+    a.G.gquat[(size_t)s * n + i] = gq[s];
+  }
+}
+
 __global__ void k_periodic(StepArgs a, int axes) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.P.n) return;
@@ -1289,8 +1362,12 @@ __global__ void k_periodic(StepArgs a, int axes) {
     for (int s = 0; s < a.G.nsets; ++s)
       if (a.G.mask[s] == (1 << ax)) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
   }
-  for (int s = 0; s < a.G.nsets; ++s)
-    if (__popc(a.G.mask[s]) >= 2) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
+  if (a.G.sector) {
+    sector_wrap_images(a, i, p);
+  } else {
+    for (int s = 0; s < a.G.nsets; ++s)
+      if (__popc(a.G.mask[s]) >= 2) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
+  }
   for (int s = 0; s < a.G.nsets; ++s) a.G.gkey[(size_t)s * n + i] = ghost_key(a.G.gpos[(size_t)s * n + i], g);
   a.P.pos[i] = p;
 }

@@ -200,6 +200,92 @@ ORA_API void ora_ghost_positions(int n, const double* pos, const double* mn, con
   }
 }
 
+// Sector periodicity (host arithmetic of the reference's helpers: rotateVector,
+// myVec.h:143-182, and rotateQuaternion, myQua.h:131-179).
+static d3 rotate_vector(d3 v, d3 om) {
+  const double theta2 = dot(om, om);
+  if (is_zero(theta2)) {
+    const d3 oxv = cross(om, v), oxoxv = cross(om, oxv);
+    return v + oxv + 0.5 * oxoxv;
+  }
+  const double inv = 1.0 / std::sqrt(theta2);
+  const double theta = theta2 * inv;
+  const double s = std::sin(theta), c = std::cos(theta);
+  const double A = s * inv, B = (1.0 - c) * (inv * inv);
+  const d3 oxv = cross(om, v), oxoxv = cross(om, oxv);
+  return v + A * oxv + B * oxoxv;
+}
+static qt rotate_quaternion(qt q, d3 om) {
+  const double theta2 = om.x * om.x + om.y * om.y + om.z * om.z;
+  if (is_zero(theta2)) return q;
+  const double theta = std::sqrt(theta2), inv = 1.0 / theta;
+  const double ux = om.x * inv, uy = om.y * inv, uz = om.z * inv;
+  const double half = 0.5 * theta, c = std::cos(half), s = std::sin(half);
+  const double r0 = c, r1 = s * ux, r2 = s * uy, r3 = s * uz;
+  qt r{r0 * q.q0 - r1 * q.q1 - r2 * q.q2 - r3 * q.q3, r0 * q.q1 + r1 * q.q0 + r2 * q.q3 - r3 * q.q2,
+       r0 * q.q2 - r1 * q.q3 + r2 * q.q0 + r3 * q.q1, r0 * q.q3 + r1 * q.q2 - r2 * q.q1 + r3 * q.q0};
+  return normalize(r);
+}
+
+// updateVelocityPositionOrientationOutOfSectorKernel (mySpatialGrid.cu:58-85): a particle
+// left of x = m.x (y >= m.y) turns by -90 degrees about the z axis through m, one below
+// y = m.y (x >= m.x) by +90 degrees (position about m, velocity, orientation; the angular
+// velocity is not turned). force / torque (nullable) turn with the particle: the step
+// evaluates the particle and wall forces before the wrap.
+ORA_API void ora_sector_wrap(int n, double* pos, double* vel, double* quat, double* force, double* torque,
+                             const double* mn) {
+  const double hp = 0.5 * 3.14159265358979323846;
+  const d3 m = mk(mn[0], mn[1], mn[2]);
+  for (int i = 0; i < n; ++i) {
+    d3 p = ld3(pos, i), v = ld3(vel, i);
+    qt q = ldq(quat, i);
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool hit = pass == 0 ? (p.x < m.x && p.y >= m.y) : (p.y < m.y && p.x >= m.x);
+      if (!hit) continue;
+      const d3 om = mk(0., 0., pass == 0 ? -hp : hp);
+      v = rotate_vector(v, om);
+      p = m + rotate_vector(p - m, om);
+      q = rotate_quaternion(q, om);
+      if (force) st3(force, i, rotate_vector(ld3(force, i), om));
+      if (torque) st3(torque, i, rotate_vector(ld3(torque, i), om));
+    }
+    st3(pos, i, p);
+    st3(vel, i, v);
+    quat[4 * i] = q.q0; quat[4 * i + 1] = q.q1; quat[4 * i + 2] = q.q2; quat[4 * i + 3] = q.q3;
+  }
+}
+
+// calculateSectorGhostVelocityPositionOrientationKernel (mySpatialGrid.cu:154-212): sets
+// R90, R180, R270 (3 x n each); a particle is turned by 90 degrees when its cell row along
+// y is 0, by 270 when its cell column along x is 0, by 180 when both, else copied.
+ORA_API void ora_sector_ghosts(int n, const double* pos, const double* vel, const double* quat, const double* mn,
+                               const double* inv, double* gpos, double* gvel, double* gquat) {
+  const double hp = 0.5 * 3.14159265358979323846;
+  const d3 m = mk(mn[0], mn[1], mn[2]);
+  const double ang[3] = {hp, 2.0 * hp, -hp};
+  for (int i = 0; i < n; ++i) {
+    const d3 p = ld3(pos, i), v = ld3(vel, i);
+    const qt q = ldq(quat, i);
+    int c[3];
+    cell_of(p, mn, inv, c);
+    for (int s = 0; s < 3; ++s) {
+      const bool on = s == 0 ? c[1] == 0 : (s == 1 ? (c[1] == 0 && c[0] == 0) : c[0] == 0);
+      d3 gp = p, gv = v;
+      qt gq = q;
+      if (on) {
+        const d3 om = mk(0., 0., ang[s]);
+        gv = rotate_vector(v, om);
+        gp = m + rotate_vector(p - m, om);
+        gq = rotate_quaternion(q, om);
+      }
+      const long long k = (long long)s * n + i;
+      st3(gpos, k, gp);
+      st3(gvel, k, gv);
+      gquat[4 * k] = gq.q0; gquat[4 * k + 1] = gq.q1; gquat[4 * k + 2] = gq.q2; gquat[4 * k + 3] = gq.q3;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Narrowphase.
 // Trilinear value: interpolateLevelSetFunctionValue (LSParticleContactDetectionKernel.cuh:4-32).

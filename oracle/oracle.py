@@ -102,6 +102,8 @@ lib.ora_kick.argtypes = [C.c_int, DP, DP, DP, DP, DP, DP, DP, DP, C.c_double]
 lib.ora_drift.argtypes = [C.c_int, DP, DP, DP, DP, C.c_double]
 lib.ora_mass_props.argtypes = [DP, C.c_int, C.c_int, C.c_int, DP, C.c_double, C.c_double, DP]
 lib.ora_mesh_grid.argtypes = [DP, IP, C.c_int, DP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, DP]
+lib.ora_sector_wrap.argtypes = [C.c_int, DP, DP, DP, DP, DP, DP]
+lib.ora_sector_ghosts.argtypes = [C.c_int, DP, DP, DP, DP, DP, DP, DP, DP]
 lib.ora_set_threads.argtypes = [C.c_int]
 lib.ora_num_threads.restype = C.c_int
 
@@ -145,6 +147,20 @@ def sort_ranges(key, ncells):
 
 def wrap(pos, g, axis):
     lib.ora_wrap(len(pos), _d(pos), _d(f64(g["min"])), _d(f64(g["max"])), int(axis))
+
+
+def sector_wrap(pos, vel, quat, g, force=None, torque=None):
+    """Sector wrap in place (mySpatialGrid.cu:58-85); force / torque, when given, turn with the particles."""
+    lib.ora_sector_wrap(len(pos), _d(pos), _d(vel), _d(quat), _d(force), _d(torque), _d(f64(g["min"])))
+
+
+def sector_ghosts(pos, vel, quat, g):
+    """Sector image sets R90, R180, R270 (mySpatialGrid.cu:154-212): (pos, vel, quat), each 3 x n."""
+    n = len(pos)
+    gp, gv, gq = np.zeros((3 * n, 3)), np.zeros((3 * n, 3)), np.zeros((3 * n, 4))
+    lib.ora_sector_ghosts(n, _d(f64(pos)), _d(f64(vel)), _d(f64(quat)), _d(f64(g["min"])), _d(f64(g["inv"])),
+                          _d(gp), _d(gv), _d(gq))
+    return gp.reshape(3, n, 3), gv.reshape(3, n, 3), gq.reshape(3, n, 4)
 
 
 def ghost_positions(pos, g, mask):
@@ -368,6 +384,18 @@ class OracleSim:
         g = self.pg
         self.pos_detect = P["pos"].copy()
         self.ghost_pos = {}
+        self.ghost_vel, self.ghost_quat = {}, {}
+        if self.periodic & 8:
+            # sector: wrap (position, velocity, orientation), then the three turned image sets
+            self.vel_detect = P["vel"].copy()
+            self.quat_detect = P["quat"].copy()
+            sector_wrap(P["pos"], P["vel"], P["quat"], g)
+            gp, gv, gq = sector_ghosts(P["pos"], P["vel"], P["quat"], g)
+            for s, m in enumerate((8, 16, 32)):
+                self.ghost_pos[m], self.ghost_vel[m], self.ghost_quat[m] = gp[s], gv[s], gq[s]
+                GB = self._bodies(pos=gp[s], quat=gq[s])
+                self._list(f"g{m}", 1, GB, g, hash_keys(gp[s], g, ghost=True))
+            return
         order = [1, 2, 4, 3, 5, 6, 7]
         sets = [m for m in order if (m & self.periodic) == m]
         for ax in range(3):
@@ -390,18 +418,26 @@ class OracleSim:
         self.F[:] = 0.0
         self.T[:] = 0.0
         pos_pp = P["pos"]
+        vel_pp = P["vel"]
         if self.periodic and not self.literal_wrap_arms:
             pos_pp = self.pos_detect
-        PD = DynSet(pos_pp, P["vel"], P["angvel"], P["inv_mass"], P["kn"], P["ks"], P["mu"], P["e"])
+            if self.periodic & 8:
+                vel_pp = self.vel_detect
+        PD = DynSet(pos_pp, vel_pp, P["angvel"], P["inv_mass"], P["kn"], P["ks"], P["mu"], P["e"])
         contact_force(0, self.last["pp"], PD, PD, dt, self.F, self.T, self.flags, self.nthreads)
         if "pw" in self.last:
             W = self.W
             WD = DynSet(W["pos"], W["vel"], W["angvel"], None, None, None, W["mu"], W["e"])
             contact_force(1, self.last["pw"], PD, WD, dt, self.F, self.T, self.flags, self.nthreads)
+        if self.periodic & 8 and not self.literal_wrap_arms:
+            # the wrapped particles' forces and torques turn with them (same wrap, pre-wrap state)
+            sector_wrap(self.pos_detect.copy(), self.vel_detect.copy(), self.quat_detect.copy(), self.pg,
+                        self.F, self.T)
         if self.periodic:
             PW = DynSet(P["pos"], P["vel"], P["angvel"], P["inv_mass"], P["kn"], P["ks"], P["mu"], P["e"])
             for m, gp in self.ghost_pos.items():
-                GD = DynSet(gp, P["vel"], P["angvel"], P["inv_mass"], P["kn"], P["ks"], P["mu"], P["e"])
+                gv = self.ghost_vel.get(m, P["vel"])  # sector images: turned velocity; angular velocity not turned
+                GD = DynSet(gp, gv, P["angvel"], P["inv_mass"], P["kn"], P["ks"], P["mu"], P["e"])
                 contact_force(2, self.last[f"g{m}"], PW, GD, dt, self.F, self.T, self.flags, self.nthreads)
         if self.bonds is not None:
             bond_force(self.bonds, P["pos"], P["quat"], self.F, self.T)
