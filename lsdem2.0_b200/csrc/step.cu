@@ -1082,6 +1082,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     if (ok) {
       a.mb.pair[(size_t)li * a.mb.pcap + pi] = make_int4(A, (KIND << 24) | slot, start, total);
     } else {
+      // the pair index is reserved: mark its entry empty so that the contact pass skips it
+      // (the node queue is full; the batch re-runs with grown capacities)
+      if (pi < a.mb.pcap) a.mb.pair[(size_t)li * a.mb.pcap + pi] = make_int4(-1, 0, 0, 0);
       atomicOr(&a.status->flags, OVF_CONTACT);
       const long long need = start + total > 2LL * (pi + 1) ? start + total : 2LL * (pi + 1);
       atomicMax(&a.status->need_contact, (int)(need < 0x7fffffff ? need : 0x7fffffff));
@@ -1179,6 +1182,7 @@ __global__ void __launch_bounds__(NP_WARPS * 32) k_contacts_f(StepArgs a, int li
   const int np = min(a.mb.ctr[1 + li], a.mb.pcap);
   for (int p = blockIdx.x * NP_WARPS + warp; p < np; p += gridDim.x * NP_WARPS) {
     const int4 e = a.mb.pair[(size_t)li * a.mb.pcap + p];
+    if (e.x < 0) continue;  // reserved by a pair whose nodes did not fit the queue
     const int kind = e.y >> 24, slot = e.y & 0xffffff;
     if (kind == KIND_PP) contacts_pair<KIND_PP>(a, e.x, slot, e.z, e.w, s_mask[warp], s_old[warp]);
     else if (kind == KIND_WALL) contacts_pair<KIND_WALL>(a, e.x, slot, e.z, e.w, s_mask[warp], s_old[warp]);
