@@ -311,6 +311,14 @@ int lsdem_set_triangles(lsdem_solver* s, int kind, int index, const int* tris, i
 int lsdem_write_vtu(lsdem_solver* s, const char* dir, unsigned long long frame, unsigned long long step,
                     double time);
 
+/* Steps without a host hook, profiling or contact recording are replayed from a
+ * CUDA graph of the step's launches (captured once per history parity and
+ * re-captured when the step's arguments change; on the legacy default stream the
+ * replay runs on a private blocking stream, ordered with it both ways). on = 0
+ * launches every kernel of every step instead. Default on. No counterpart in the
+ * reference (which launches each kernel and synchronises with the host every step). */
+int lsdem_set_graphs(lsdem_solver* s, int on);
+
 /* Broadphase cell sort that allocates no device memory: cell keys of n body
  * centres (pos_dev: device array of n x 3 doubles), their stable sorted order
  * and per-cell [start, end) (-1 when empty) for the grid (min, max, inverse

@@ -108,6 +108,7 @@ _SIGS = {
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
     "lsdem_mesh_grid_box": (C.c_int, [DP, C.c_int, C.c_double, C.c_int, DP, IP]),
     "lsdem_set_triangles": (C.c_int, [P, C.c_int, C.c_int, IP, C.c_int]),
+    "lsdem_set_graphs": (C.c_int, [P, C.c_int]),
     "lsdem_write_vtu": (C.c_int, [P, C.c_char_p, C.c_ulonglong, C.c_ulonglong, C.c_double]),
     "lsdem_mesh_grid": (C.c_int, [DP, C.c_int, IP, C.c_int, DP, IP, C.c_double, C.c_int, DP, C.c_int]),
 }
@@ -302,6 +303,10 @@ class Solver:
 
     def set_periodic(self, axes: int):
         self._chk(lib.lsdem_set_periodic(self.h, int(axes)), "set_periodic")
+
+    def set_graphs(self, on=True):
+        """Replay steps from a CUDA graph (default) or launch every kernel."""
+        self._chk(lib.lsdem_set_graphs(self.h, 1 if on else 0), "set_graphs")
 
     def set_triangles(self, kind, index, tris):
         """Triangles of a body's nodes (kind 0 particle, 1 wall) for the mesh output files."""
