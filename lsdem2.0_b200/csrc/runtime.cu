@@ -972,7 +972,9 @@ void resolve_profile(lsdem_solver* s, bool keep) {
 }
 
 // One time step in the reference order (LSSolver.h:1000-1011, 1104-1128).
-void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* user, double t) {
+// The launches of one step up to the external-force hook: integration, cell sort,
+// candidates, narrowphase and contact forces, periodic images, bonds.
+void step_pre(lsdem_solver* s, double dt, bool record) {
   cudaStream_t st = s->stream;
   StepArgs a = make_args(s, dt);
   if (record) {
@@ -1007,16 +1009,28 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
                s->b_state.p};
     launch_bonds(a, b, st);
   }
-  if (hook) hook(user, t);
-  { PhaseTimer pt(s, 7); launch_kick(a, st); }
-  // kernels launched by this step: kick/drift/keys, cell sort (9), packing + candidates,
-  // narrowphase, second kick; periodic: wrap/images, clamped keys, cell sort (8),
-  // image compaction + packing + candidates, ghost narrowphase; bonds
-  // (the precision form adds one contact pass per narrowphase)
+  // kernels launched up to here: kick/drift/keys, cell sort (9), packing + candidates,
+  // narrowphase; periodic: wrap/images, clamped keys, cell sort (8), image compaction +
+  // packing + candidates, ghost narrowphase; bonds (the precision form adds one contact
+  // pass per narrowphase)
   const int nf = s->precision == PREC_FP64 ? 0 : 1;
-  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 14 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  if (a.P.n > 0) s->launches += 13 + nf + (s->nsets > 0 ? 14 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  CK(cudaGetLastError());
+}
+
+// The rest of a step after the hook: the second half kick.
+void step_post(lsdem_solver* s, double dt) {
+  StepArgs a = make_args(s, dt);
+  { PhaseTimer pt(s, 7); launch_kick(a, s->stream); }
+  if (a.P.n > 0) s->launches += 1;
   CK(cudaGetLastError());
   s->hp = 1 - s->hp;
+}
+
+void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* user, double t) {
+  step_pre(s, dt, record);
+  if (hook) hook(user, t);
+  step_post(s, dt);
 }
 
 // Snapshot of everything a batch may change, taken at the batch start.
@@ -1129,7 +1143,7 @@ cudaEvent_t step_start(lsdem_solver* s) {
 // cannot be captured) the graph runs on a private blocking stream: the legacy stream
 // and blocking streams are ordered with each other both ways, so the copies, events
 // and app kernels on the legacy stream keep their order around the step.
-static void step_graph(lsdem_solver* s, double dt) {
+static void step_graph(lsdem_solver* s, double dt, lsdem_hook hook, void* user, double t) {
   const int hp = s->hp;
   uint64_t key = 1469598103934665603ull;
   auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
@@ -1151,7 +1165,7 @@ static void step_graph(lsdem_solver* s, double dt) {
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(gs, cudaStreamCaptureModeRelaxed));
     try {
-      step_once(s, dt, false, nullptr, nullptr, 0.);
+      step_pre(s, dt, false);
     } catch (...) {
       cudaStreamEndCapture(gs, &graph);
       if (graph) cudaGraphDestroy(graph);
@@ -1171,7 +1185,8 @@ static void step_graph(lsdem_solver* s, double dt) {
   }
   CK(cudaGraphLaunch(G.exec, gs));
   s->launches += G.launches;
-  s->hp = 1 - hp;
+  if (hook) hook(user, t);
+  step_post(s, dt);
 }
 
 int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
@@ -1193,8 +1208,8 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
         const bool rec = s->record && (done + k == nsteps - 1);
         cudaEvent_t ea = nullptr;
         if (s->step_timing) ea = (k == 0 && attempt == 0) ? first : step_start(s);
-        if (s->graphs && !hook && !rec && !s->profiling && s->P.n() > 0)
-          step_graph(s, dt);
+        if (s->graphs && !rec && !s->profiling && s->P.n() > 0)
+          step_graph(s, dt, hook, user, t);
         else
           step_once(s, dt, rec, hook, user, t);
         if (ea) {
