@@ -220,7 +220,7 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s);
 // launch li (0: particles and walls, 1: periodic images)
 void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s);
 void launch_kick(const StepArgs& a, cudaStream_t s);
-void launch_periodic(const StepArgs& a, int axes, cudaStream_t s);
+void launch_periodic(const StepArgs& a, int axes, double3* out, cudaStream_t s);
 // g2_off: bucket offsets of the image search's cell sort (cell k at [k + 1])
 void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2_off, cudaStream_t s);
 void launch_clamped_keys(const StepArgs& a, int* key2, cudaStream_t s);

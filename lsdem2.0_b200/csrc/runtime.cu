@@ -373,6 +373,13 @@ struct lsdem_solver {
   DArr<int> cell_idx, cell_start, cell_end, sorted_key;
   DArr<float4> cell_pk;
   DArr<int> bk_counts, bk_fill, bk_offs, bk_scan, bk_big, bk_bigc, bk_tmp;
+  // periodic images as a parallel branch of the step: wrapped positions, the image
+  // sort's own scratch and packed cells, a second stream and the fork / join events
+  DArr<double3> pos_w;
+  DArr<float4> cell_pk2;
+  DArr<int> bk2_counts, bk2_fill, bk2_offs, bk2_scan, bk2_big, bk2_bigc, bk2_tmp;
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   SlotsDev slots[2][3];      // [history parity][kind]
   ContactsDev con[2];
   int hp = 0;                // parity of the last completed step's history
@@ -641,15 +648,22 @@ void set_grid(GridP& g, const double* mn, const double* mx_in, double cell) {  /
   g.ncells = size[0] * size[1] * size[2];
 }
 
-void alloc_bucket(lsdem_solver* s, int n, int ncells) {
+void alloc_bucket(lsdem_solver* s, int n, int ncells, bool second = false) {
   const int nb = ncells + 2;
-  CK(s->bk_counts.alloc(nb + 1));
-  CK(s->bk_fill.alloc(nb + 1));
-  CK(s->bk_offs.alloc(nb + 1));
-  CK(s->bk_scan.alloc(scan_temp_elems(nb + 1)));
-  CK(s->bk_big.alloc((size_t)n / 65 + 1));
-  CK(s->bk_bigc.alloc(1));
-  CK(s->bk_tmp.alloc((size_t)std::max(n, 1)));
+  auto& c = second ? s->bk2_counts : s->bk_counts;
+  auto& f = second ? s->bk2_fill : s->bk_fill;
+  auto& o = second ? s->bk2_offs : s->bk_offs;
+  auto& sc = second ? s->bk2_scan : s->bk_scan;
+  auto& b = second ? s->bk2_big : s->bk_big;
+  auto& bc = second ? s->bk2_bigc : s->bk_bigc;
+  auto& t = second ? s->bk2_tmp : s->bk_tmp;
+  CK(c.alloc(nb + 1));
+  CK(f.alloc(nb + 1));
+  CK(o.alloc(nb + 1));
+  CK(sc.alloc(scan_temp_elems(nb + 1)));
+  CK(b.alloc((size_t)n / 65 + 1));
+  CK(bc.alloc(1));
+  CK(t.alloc((size_t)std::max(n, 1)));
 }
 
 void initialize(lsdem_solver* s) {
@@ -827,6 +841,14 @@ void initialize(lsdem_solver* s) {
     CK(s->g2_idx.alloc(std::max(n, 1)));
     CK(s->g2_start.alloc(s->pg.ncells));
     CK(s->g2_end.alloc(s->pg.ncells));
+    if (!(s->periodic & 8)) {  // translated images: the parallel branch's own buffers
+      CK(s->pos_w.alloc(std::max(n, 1)));
+      CK(s->cell_pk2.alloc(std::max(n, 1)));
+      alloc_bucket(s, n, s->pg.ncells, true);
+      if (!s->st2) CK(cudaStreamCreate(&s->st2));
+      if (!s->ev_fork) CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+      if (!s->ev_join) CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    }
   }
   // history buffers
   if (s->cap_c <= 0) s->cap_c = std::max<long long>(1 << 16, (long long)n * 128);
@@ -989,19 +1011,47 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
     PhaseTimer pt(s, 1);
     bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st);
   }
-  { PhaseTimer pt(s, 2); launch_candidates(a, st); }
-  { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
-  if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 0, st); }
-  if (s->nsets > 0) {
-    {
-      PhaseTimer pt(s, 4);
-      launch_periodic(a, s->periodic, st);
-      launch_clamped_keys(a, s->key2.p, st);
-      bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
-      launch_ghost_candidates(a, s->g2_idx.p, w.offs, st);
+  const bool branch = s->nsets > 0 && !(s->periodic & 8) && !s->profiling;
+  if (branch) {
+    // The periodic images run beside the particle candidates, screen and contact
+    // pass: they read the same pre-wrap positions and write only their own arrays
+    // (wrapped positions into pos_w, the image sort's scratch and packed cells).
+    // Joined, the wrapped positions are copied over before the image narrowphase.
+    StepArgs a2 = a;
+    a2.P.pos = s->pos_w.p;
+    a2.cell_pk = s->cell_pk2.p;
+    BucketScratch w2{s->bk2_counts.p, s->bk2_fill.p, s->bk2_offs.p, s->bk2_scan.p, s->bk2_big.p, s->bk2_bigc.p,
+                     s->bk2_tmp.p};
+    cudaStream_t s2 = s->st2;
+    CK(cudaEventRecord(s->ev_fork, st));
+    CK(cudaStreamWaitEvent(s2, s->ev_fork, 0));
+    launch_periodic(a, s->periodic, s->pos_w.p, s2);
+    launch_clamped_keys(a2, s->key2.p, s2);
+    bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w2, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, s2);
+    launch_ghost_candidates(a2, s->g2_idx.p, w2.offs, s2);
+    CK(cudaEventRecord(s->ev_join, s2));
+    launch_candidates(a, st);
+    launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st);
+    if (s->precision != PREC_FP64) launch_contact_pass(a, 0, st);
+    CK(cudaStreamWaitEvent(st, s->ev_join, 0));
+    if (a.P.n > 0) CK(cudaMemcpyAsync(a.P.pos, s->pos_w.p, sizeof(double3) * a.P.n, cudaMemcpyDeviceToDevice, st));
+    launch_narrowphase(a, 4, st);
+    if (s->precision != PREC_FP64) launch_contact_pass(a, 1, st);
+  } else {
+    { PhaseTimer pt(s, 2); launch_candidates(a, st); }
+    { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
+    if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 0, st); }
+    if (s->nsets > 0) {
+      {
+        PhaseTimer pt(s, 4);
+        launch_periodic(a, s->periodic, a.P.pos, st);
+        launch_clamped_keys(a, s->key2.p, st);
+        bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
+        launch_ghost_candidates(a, s->g2_idx.p, w.offs, st);
+      }
+      { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
+      if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
     }
-    { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
-    if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
   }
   if (!s->bonds.bonded.empty()) {
     PhaseTimer pt(s, 6);
@@ -1303,6 +1353,9 @@ void lsdem_destroy(lsdem_solver* s) {
   for (auto& g : s->sgraph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (s->gstream) cudaStreamDestroy(s->gstream);
+  if (s->st2) cudaStreamDestroy(s->st2);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
   delete s;
 }
 

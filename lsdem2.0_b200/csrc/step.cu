@@ -1352,7 +1352,7 @@ LD void sector_wrap_images(const StepArgs& a, int i, double3& p) {
   }
 }
 
-__global__ void k_periodic(StepArgs a, int axes) {
+__global__ void k_periodic(StepArgs a, int axes, double3* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.P.n) return;
   const GridP& g = a.pg;
@@ -1373,11 +1373,13 @@ __global__ void k_periodic(StepArgs a, int axes) {
       if (__popc(a.G.mask[s]) >= 2) ghost_image(p, g, a.G.mask[s], a.G.gpos[(size_t)s * n + i]);
   }
   for (int s = 0; s < a.G.nsets; ++s) a.G.gkey[(size_t)s * n + i] = ghost_key(a.G.gpos[(size_t)s * n + i], g);
-  a.P.pos[i] = p;
+  out[i] = p;
 }
 
-void launch_periodic(const StepArgs& a, int axes, cudaStream_t s) {
-  if (a.P.n > 0) k_periodic<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, axes);
+// out: where the wrapped positions go (the particles' own positions, or a separate array
+// when the images run beside the particle narrowphase, which still reads the pre-wrap ones)
+void launch_periodic(const StepArgs& a, int axes, double3* out, cudaStream_t s) {
+  if (a.P.n > 0) k_periodic<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, axes, out);
 }
 
 // Clamped cell of every particle after the wrap (search grid for ghost partners).
