@@ -161,7 +161,9 @@ int lsdem_set_capacity(lsdem_solver* s, int pp_slots, int wall_slots, int ghost_
                        int batch_steps);
 
 /* Sizes: 0 particles, 1 walls, 2 bonds, 3 surface nodes, 4 shapes, 5 grid cells,
- * 6 steps taken, 7 overflow re-runs so far, 8 kernels launched by steps so far. */
+ * 6 steps taken, 7 overflow re-runs so far, 8 kernels launched by steps so far,
+ * 9 steps that sorted the cells and rebuilt the neighbour lists (counted while
+ * lsdem_set_neighbour_lists is on). */
 long long lsdem_num(const lsdem_solver* s, int what);
 double lsdem_time(const lsdem_solver* s);
 
@@ -311,13 +313,25 @@ int lsdem_set_triangles(lsdem_solver* s, int kind, int index, const int* tris, i
 int lsdem_write_vtu(lsdem_solver* s, const char* dir, unsigned long long frame, unsigned long long step,
                     double time);
 
-/* Steps without a host hook, profiling or contact recording are replayed from a
- * CUDA graph of the step's launches (captured once per history parity and
- * re-captured when the step's arguments change; on the legacy default stream the
- * replay runs on a private blocking stream, ordered with it both ways). on = 0
- * launches every kernel of every step instead. Default on. No counterpart in the
- * reference (which launches each kernel and synchronises with the host every step). */
+/* Steps without profiling or contact recording are replayed from a CUDA graph of
+ * the step's launches up to the external-force hook (captured once per history
+ * parity and re-captured when the step's arguments change; on the legacy default
+ * stream the replay runs on a private blocking stream, ordered with it both ways);
+ * the hook and the second half kick follow the replay. on = 0 launches every kernel
+ * of every step instead. Default on. No counterpart in the reference (which
+ * launches each kernel and synchronises with the host every step). */
 int lsdem_set_graphs(lsdem_solver* s, int on);
+
+/* Neighbour lists (exact; default on): the candidate search tests, per particle, the
+ * bodies it found within its reach plus a margin (a tenth of the largest bounding
+ * radius) at the last rebuild, keeping those whose cell is in its cell window and
+ * which pass the same bounding-sphere test, in the walk's order. The cell sort and the
+ * rebuild run only in steps where a particle moved 0.04 of the largest bounding
+ * radius since the last rebuild (a periodic wrap included). The candidate pairs,
+ * their order and so every result are the same as with on = 0, which sorts and walks
+ * the 27 cells every step as the reference does (LSSolver.h:1000-1011,
+ * mySpatialGrid.cu, LSParticleContactDetectionKernel.cu). */
+int lsdem_set_neighbour_lists(lsdem_solver* s, int on);
 
 /* Broadphase cell sort that allocates no device memory: cell keys of n body
  * centres (pos_dev: device array of n x 3 doubles), their stable sorted order

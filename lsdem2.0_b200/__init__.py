@@ -109,6 +109,7 @@ _SIGS = {
     "lsdem_mesh_grid_box": (C.c_int, [DP, C.c_int, C.c_double, C.c_int, DP, IP]),
     "lsdem_set_triangles": (C.c_int, [P, C.c_int, C.c_int, IP, C.c_int]),
     "lsdem_set_graphs": (C.c_int, [P, C.c_int]),
+    "lsdem_set_neighbour_lists": (C.c_int, [P, C.c_int]),
     "lsdem_write_vtu": (C.c_int, [P, C.c_char_p, C.c_ulonglong, C.c_ulonglong, C.c_double]),
     "lsdem_mesh_grid": (C.c_int, [DP, C.c_int, IP, C.c_int, DP, IP, C.c_double, C.c_int, DP, C.c_int]),
 }
@@ -307,6 +308,11 @@ class Solver:
     def set_graphs(self, on=True):
         """Replay steps from a CUDA graph (default) or launch every kernel."""
         self._chk(lib.lsdem_set_graphs(self.h, 1 if on else 0), "set_graphs")
+
+    def set_neighbour_lists(self, on=True):
+        """Reuse per-particle neighbour lists between steps (default; exact), sorting the
+        cells only when lists are rebuilt, or sort and walk the 27 cells every step."""
+        self._chk(lib.lsdem_set_neighbour_lists(self.h, 1 if on else 0), "set_neighbour_lists")
 
     def set_triangles(self, kind, index, tris):
         """Triangles of a body's nodes (kind 0 particle, 1 wall) for the mesh output files."""

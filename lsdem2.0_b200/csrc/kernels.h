@@ -18,7 +18,7 @@ namespace lsdem {
 enum { FIX_GRADIENT = 1, FIX_SQRTF = 2 };
 
 // Overflow bits of the device status word.
-enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8 };
+enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8, OVF_NBR = 16 };
 
 // Largest demands seen during a batch (whether or not they overflowed), used
 // to grow capacities ahead of an overflow.
@@ -28,7 +28,9 @@ struct Status {
   int need_wall;     // largest per-particle wall-candidate count
   int need_ghost;    // largest per-particle ghost-candidate count
   int need_contact;  // largest contact total
-  int pad[3];
+  int need_nbr;      // largest per-particle neighbour-list length
+  int builds;        // steps that sorted and rebuilt the neighbour lists
+  int pad;
 };
 
 // Shape templates: SDF grid + surface nodes in cluster order.
@@ -133,10 +135,12 @@ struct BucketScratch {
 };
 
 size_t scan_temp_elems(long long n);
-void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s);
+// gate (optional): the launches return at once when *gate is zero
+void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s,
+              const int* gate = nullptr);
 void scan_i64(const long long* in, long long* out, long long n, long long* tmp, bool inclusive, cudaStream_t s);
 void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorted_idx, int* sorted_key, int* start,
-                 int* end, cudaStream_t s);
+                 int* end, cudaStream_t s, const int* gate = nullptr);
 
 // Precision form: nodes the FP32 screen could not reject, by pair, for the FP64
 // contact pass. One node cursor per step; one pair list per narrowphase launch
@@ -189,6 +193,17 @@ struct StepArgs {
   const MlpInfer* mlp_inf;   // per shape (nullptr: off)
   const MlpNorm* mlp_norm;   // per shape
   const float* mlp_band;     // per shape: trust band + error bound, in template spacings
+  // Neighbour lists (exact, optional): *reuse is set non-zero when a particle moved
+  // more than sqrt(move2) from its position at the last list build; the cell sort and
+  // the list rebuild run only then. The step's kick clears it.
+  int* reuse;
+  double move2;
+  float skin;             // neighbour-list margin beyond the candidate reach (length)
+  double3* xb;            // particle order: position at the last list build
+  int* nbr;               // sorted order of the last sort: entry j of position t at j * n + t
+  int* nbr_cnt;           // sorted order: entries, -1 when the list overflowed
+  int nbr_cap;
+  int* pk_key;            // sorted order: this step's cell key (written with cell_pk)
 };
 
 // Template data for the learned-SDF kernels (mlp.cu).

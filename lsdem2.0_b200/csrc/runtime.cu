@@ -380,6 +380,18 @@ struct lsdem_solver {
   DArr<int> bk2_counts, bk2_fill, bk2_offs, bk2_scan, bk2_big, bk2_bigc, bk2_tmp;
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // neighbour lists (exact; see k_candidates): flag word, positions at the last
+  // rebuild, lists, this step's keys in sorted order
+  bool reuse_on = true;
+  bool force_reuse = true;   // the next step sorts and rebuilds (set after any re-allocation)
+  bool grow_nbr = false;
+  DArr<int> reuse;
+  DArr<double3> xb;
+  DArr<int> nbr, nbr_cnt, pk_key;
+  int nbr_cap = 24;
+  float skin = 0.f;
+  double move2 = 0.;
+  long long builds = 0;      // steps that sorted and rebuilt the lists (lists on)
   SlotsDev slots[2][3];      // [history parity][kind]
   ContactsDev con[2];
   int hp = 0;                // parity of the last completed step's history
@@ -816,6 +828,19 @@ void initialize(lsdem_solver* s) {
   const int n = s->P.n();
   CK(s->cell_idx.alloc(std::max(n, 1)));
   CK(s->cell_pk.alloc(std::max(n, 1)));
+  {
+    // neighbour-list margin: a tenth of the largest bounding radius; rebuilt when a
+    // particle moved 0.4 of it (pairs approach by at most twice that)
+    const double sr = 0.1 * s->rmax_p;
+    s->skin = (float)sr;
+    s->move2 = (0.4 * sr) * (0.4 * sr);
+    CK(s->reuse.alloc(1));
+    CK(s->xb.alloc(std::max(n, 1)));
+    CK(s->nbr_cnt.alloc(std::max(n, 1)));
+    CK(s->pk_key.alloc(std::max(n, 1)));
+    CK(s->nbr.alloc((size_t)std::max(n, 1) * s->nbr_cap));
+    s->force_reuse = true;
+  }
   CK(s->sorted_key.alloc(std::max(n, 1)));
   CK(s->cell_start.alloc(s->pg.ncells));
   CK(s->cell_end.alloc(s->pg.ncells));
@@ -841,10 +866,11 @@ void initialize(lsdem_solver* s) {
     CK(s->g2_idx.alloc(std::max(n, 1)));
     CK(s->g2_start.alloc(s->pg.ncells));
     CK(s->g2_end.alloc(s->pg.ncells));
+    // the image sort's own scratch: the particle sort's offsets stay valid between sorts
+    alloc_bucket(s, n, s->pg.ncells, true);
     if (!(s->periodic & 8)) {  // translated images: the parallel branch's own buffers
       CK(s->pos_w.alloc(std::max(n, 1)));
       CK(s->cell_pk2.alloc(std::max(n, 1)));
-      alloc_bucket(s, n, s->pg.ncells, true);
       if (!s->st2) CK(cudaStreamCreate(&s->st2));
       if (!s->ev_fork) CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
       if (!s->ev_join) CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
@@ -938,6 +964,15 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.flags = s->flags;
   a.precision = s->precision;
   a.rmax = s->rmax_p;
+  const bool reuse = s->reuse_on && s->reuse.p;
+  a.reuse = reuse ? s->reuse.p : nullptr;
+  a.move2 = s->move2;
+  a.skin = s->skin;
+  a.xb = s->xb.p;
+  a.nbr = reuse ? s->nbr.p : nullptr;
+  a.nbr_cnt = s->nbr_cnt.p;
+  a.nbr_cap = s->nbr_cap;
+  a.pk_key = s->pk_key.p;
   a.mb.node = s->mb_node.p; a.mb.cap = (int)s->mb_cap;
   a.mb.pair = s->mb_pair.p; a.mb.pcap = (int)s->mb_pcap;
   a.mb.ctr = s->precision == PREC_FP64 ? nullptr : s->mb_ctr.p;
@@ -1009,8 +1044,11 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
   BucketScratch w{s->bk_counts.p, s->bk_fill.p, s->bk_offs.p, s->bk_scan.p, s->bk_big.p, s->bk_bigc.p, s->bk_tmp.p};
   {
     PhaseTimer pt(s, 1);
-    bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st);
+    bucket_sort(a.P.key, a.P.n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p, s->cell_end.p, st,
+                a.reuse);
   }
+  BucketScratch w2{s->bk2_counts.p, s->bk2_fill.p, s->bk2_offs.p, s->bk2_scan.p, s->bk2_big.p, s->bk2_bigc.p,
+                   s->bk2_tmp.p};
   const bool branch = s->nsets > 0 && !(s->periodic & 8) && !s->profiling;
   if (branch) {
     // The periodic images run beside the particle candidates, screen and contact
@@ -1020,8 +1058,7 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
     StepArgs a2 = a;
     a2.P.pos = s->pos_w.p;
     a2.cell_pk = s->cell_pk2.p;
-    BucketScratch w2{s->bk2_counts.p, s->bk2_fill.p, s->bk2_offs.p, s->bk2_scan.p, s->bk2_big.p, s->bk2_bigc.p,
-                     s->bk2_tmp.p};
+    a2.pk_key = nullptr;
     cudaStream_t s2 = s->st2;
     CK(cudaEventRecord(s->ev_fork, st));
     CK(cudaStreamWaitEvent(s2, s->ev_fork, 0));
@@ -1046,8 +1083,8 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
         PhaseTimer pt(s, 4);
         launch_periodic(a, s->periodic, a.P.pos, st);
         launch_clamped_keys(a, s->key2.p, st);
-        bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
-        launch_ghost_candidates(a, s->g2_idx.p, w.offs, st);
+        bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w2, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, st);
+        launch_ghost_candidates(a, s->g2_idx.p, w2.offs, st);
       }
       { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
       if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
@@ -1059,12 +1096,12 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
                s->b_state.p};
     launch_bonds(a, b, st);
   }
-  // kernels launched up to here: kick/drift/keys, cell sort (9), packing + candidates,
-  // narrowphase; periodic: wrap/images, clamped keys, cell sort (8), image compaction +
-  // packing + candidates, ghost narrowphase; bonds (the precision form adds one contact
-  // pass per narrowphase)
+  // kernels launched up to here: kick/drift/keys, cell sort (10; with neighbour lists
+  // they return at once between rebuilds), packing + candidates, narrowphase; periodic:
+  // wrap/images, clamped keys, cell sort (9), image compaction + packing + candidates,
+  // ghost narrowphase; bonds (the precision form adds one contact pass per narrowphase)
   const int nf = s->precision == PREC_FP64 ? 0 : 1;
-  if (a.P.n > 0) s->launches += 13 + nf + (s->nsets > 0 ? 14 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 15 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
 }
 
@@ -1111,6 +1148,7 @@ void backup(lsdem_solver* s) {
 }
 
 void restore(lsdem_solver* s, int hp0) {
+  s->force_reuse = true;
   cudaStream_t st = s->stream;
   s->hp = hp0;
   const size_t n = (size_t)s->P.n(), nw = (size_t)s->W.n();
@@ -1153,6 +1191,11 @@ bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
   up(s->cap_pp, st.need_pp, st.flags & OVF_PP);
   if (s->W.n() > 0) up(s->cap_w, st.need_wall, st.flags & OVF_WALL);
   if (s->nsets > 0) up(s->cap_g, st.need_ghost, st.flags & OVF_GHOST);
+  if (s->reuse_on) {
+    const int old = s->nbr_cap;
+    up(s->nbr_cap, st.need_nbr, st.flags & OVF_NBR);
+    if (s->nbr_cap != old) s->grow_nbr = true;
+  }
   const long long needc = std::max<long long>(st.need_contact, last_contacts);
   if ((st.flags & OVF_CONTACT) || needc * 5 > s->cap_c * 4) {
     s->cap_c = std::max<long long>(s->cap_c * 2, needc + needc / 2 + 1024);
@@ -1166,6 +1209,11 @@ bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
 // grow); their contents come back from the backup by restore().
 void grow(lsdem_solver* s) {
   ++s->graph_gen;
+  s->force_reuse = true;
+  if (s->grow_nbr) {
+    CK(s->nbr.alloc((size_t)std::max(s->P.n(), 1) * s->nbr_cap));
+    s->grow_nbr = false;
+  }
   alloc_slots(s, true);
   if (s->grow_contacts) {
     const bool g0 = s->con[0].geom, g1 = s->con[1].geom;
@@ -1258,6 +1306,10 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
         const bool rec = s->record && (done + k == nsteps - 1);
         cudaEvent_t ea = nullptr;
         if (s->step_timing) ea = (k == 0 && attempt == 0) ? first : step_start(s);
+        if (s->force_reuse && s->reuse.p) {  // sort and rebuild in this step
+          CK(cudaMemsetAsync(s->reuse.p, 0xff, sizeof(int), st));
+          s->force_reuse = false;
+        }
         if (s->graphs && !rec && !s->profiling && s->P.n() > 0)
           step_graph(s, dt, hook, user, t);
         else
@@ -1288,6 +1340,7 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
     done += B;
     s->steps += B;
     s->time += dt * (double)B;
+    s->builds += stat.builds;
     // grow ahead of an overflow: keep the history just written
     if (plan_growth(s, stat, s->hist_count)) {
       const int hp1 = s->hp;
@@ -1785,6 +1838,7 @@ long long lsdem_num(const lsdem_solver* s, int what) {
     case 6: return s->steps;
     case 7: return s->reruns;
     case 8: return s->launches;
+    case 9: return s->builds;
     default: return -1;
   }
 }
@@ -1936,6 +1990,16 @@ int lsdem_get_hash(lsdem_solver* s, int* key, int* sorted_idx, int* sorted_key, 
   return guard(s, [&] {
     const size_t n = (size_t)s->P.n(), nc = (size_t)s->pg.ncells;
     cudaStream_t st = s->stream;
+    if (s->reuse_on && n) {
+      // with neighbour lists the last sort may predate the current keys: sort them now
+      // (the lists refer to the old order, so the next step rebuilds them)
+      BucketScratch w{s->bk_counts.p, s->bk_fill.p, s->bk_offs.p, s->bk_scan.p, s->bk_big.p, s->bk_bigc.p,
+                      s->bk_tmp.p};
+      bucket_sort(s->dP.key.p, (int)n, s->pg.ncells, w, s->cell_idx.p, s->sorted_key.p, s->cell_start.p,
+                  s->cell_end.p, st);
+      CK(cudaGetLastError());
+      s->force_reuse = true;
+    }
     if (key && n) CK(cudaMemcpyAsync(key, s->dP.key.p, 4 * n, cudaMemcpyDeviceToHost, st));
     if (sorted_idx && n) CK(cudaMemcpyAsync(sorted_idx, s->cell_idx.p, 4 * n, cudaMemcpyDeviceToHost, st));
     if (sorted_key && n) CK(cudaMemcpyAsync(sorted_key, s->sorted_key.p, 4 * n, cudaMemcpyDeviceToHost, st));
@@ -2078,6 +2142,16 @@ void* lsdem_stream(const lsdem_solver* s) { return s ? (void*)s->stream : nullpt
 int lsdem_set_graphs(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   s->graphs = on != 0;
+  return LSDEM_OK;
+}
+
+int lsdem_set_neighbour_lists(lsdem_solver* s, int on) {
+  if (!s) return LSDEM_ERR_ARG;
+  if (s->reuse_on != (on != 0)) {
+    s->reuse_on = on != 0;
+    ++s->graph_gen;
+    s->force_reuse = true;
+  }
   return LSDEM_OK;
 }
 

@@ -15,6 +15,10 @@ static constexpr int SCAN_THREADS = 1024;
 static constexpr int SCAN_ITEMS = 4;
 static constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
+// Launches given a gate flag return at once when it is zero (the step keeps the
+// last sort's results, which are still in place).
+__device__ __forceinline__ bool idle(const int* gate) { return gate && *gate == 0; }
+
 template <typename T>
 __device__ T block_exclusive_scan(T v, T* smem_warp, T* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -43,7 +47,8 @@ __device__ T block_exclusive_scan(T v, T* smem_warp, T* total) {
 }
 
 template <typename T>
-__global__ void k_scan_tile_sums(const T* __restrict__ in, long long n, T* __restrict__ sums) {
+__global__ void k_scan_tile_sums(const T* __restrict__ in, long long n, T* __restrict__ sums, const int* gate) {
+  if (idle(gate)) return;
   __shared__ T sw[32];
   long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
   T s = 0;
@@ -57,7 +62,8 @@ __global__ void k_scan_tile_sums(const T* __restrict__ in, long long n, T* __res
 
 // Exclusive scan of `n` tile sums in place by a single block, chunk by chunk.
 template <typename T>
-__global__ void k_scan_sums(T* sums, long long n) {
+__global__ void k_scan_sums(T* sums, long long n, const int* gate) {
+  if (idle(gate)) return;
   __shared__ T sw[32];
   T carry = 0;
   for (long long c = 0; c < n; c += SCAN_TILE) {
@@ -84,7 +90,8 @@ __global__ void k_scan_sums(T* sums, long long n) {
 
 template <typename T>
 __global__ void k_scan_apply(const T* __restrict__ in, T* __restrict__ out, long long n, const T* __restrict__ sums,
-                             int inclusive) {
+                             int inclusive, const int* gate) {
+  if (idle(gate)) return;
   __shared__ T sw[32];
   long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
   T v[SCAN_ITEMS];
@@ -108,19 +115,19 @@ __global__ void k_scan_apply(const T* __restrict__ in, T* __restrict__ out, long
 size_t scan_temp_elems(long long n) { return (size_t)((n + SCAN_TILE - 1) / SCAN_TILE) + 1; }
 
 template <typename T>
-void scan_impl(const T* in, T* out, long long n, T* tmp, bool inclusive, cudaStream_t s) {
+void scan_impl(const T* in, T* out, long long n, T* tmp, bool inclusive, cudaStream_t s, const int* gate) {
   if (n <= 0) return;
   long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-  k_scan_tile_sums<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, tmp);
-  k_scan_sums<T><<<1, SCAN_THREADS, 0, s>>>(tmp, tiles);
-  k_scan_apply<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, out, n, tmp, inclusive ? 1 : 0);
+  k_scan_tile_sums<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, tmp, gate);
+  k_scan_sums<T><<<1, SCAN_THREADS, 0, s>>>(tmp, tiles, gate);
+  k_scan_apply<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, out, n, tmp, inclusive ? 1 : 0, gate);
 }
 
-void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s) {
-  scan_impl<int>(in, out, n, tmp, inclusive, s);
+void scan_i32(const int* in, int* out, long long n, int* tmp, bool inclusive, cudaStream_t s, const int* gate) {
+  scan_impl<int>(in, out, n, tmp, inclusive, s, gate);
 }
 void scan_i64(const long long* in, long long* out, long long n, long long* tmp, bool inclusive, cudaStream_t s) {
-  scan_impl<long long>(in, out, n, tmp, inclusive, s);
+  scan_impl<long long>(in, out, n, tmp, inclusive, s, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -130,14 +137,24 @@ void scan_i64(const long long* in, long long* out, long long n, long long* tmp, 
 // which, as in the reference, sort after every cell and belong to none.
 __device__ __forceinline__ int bucket_of(int k, int ncells) { return k < 0 ? 0 : (k >= ncells ? ncells + 1 : k + 1); }
 
-__global__ void k_bucket_hist(const int* __restrict__ key, int n, int ncells, int* __restrict__ counts) {
+__global__ void k_bucket_clear(int* __restrict__ counts, int* __restrict__ fill, int m, int* __restrict__ big_count,
+                               const int* gate) {
+  if (idle(gate)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) { counts[i] = 0; fill[i] = 0; }
+  if (i == 0) *big_count = 0;
+}
+
+__global__ void k_bucket_hist(const int* __restrict__ key, int n, int ncells, int* __restrict__ counts, const int* gate) {
+  if (idle(gate)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   atomicAdd(&counts[bucket_of(key[i], ncells)], 1);
 }
 
 __global__ void k_bucket_scatter(const int* __restrict__ key, int n, int ncells, const int* __restrict__ offs,
-                                 int* __restrict__ fill, int* __restrict__ sorted_idx) {
+                                 int* __restrict__ fill, int* __restrict__ sorted_idx, const int* gate) {
+  if (idle(gate)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int b = bucket_of(key[i], ncells);
@@ -154,7 +171,8 @@ __global__ void k_bucket_scatter(const int* __restrict__ key, int n, int ncells,
 // bodies in tiles: two block-wide scans of the membership flags give each
 // member its rank. Exits at once when neither bucket is longer than 64.
 __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells, const int* __restrict__ offs,
-                                  int* __restrict__ sorted_idx) {
+                                  int* __restrict__ sorted_idx, const int* gate) {
+  if (idle(gate)) return;
   __shared__ int sw[32];
   const int L = ncells + 1;
   const int n0 = offs[1] - offs[0], nL = offs[L + 1] - offs[L];
@@ -175,13 +193,14 @@ __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells
 }
 
 // Cell ranges [start, end) of every cell (-1 when empty; findStartAndEnd,
-// buildHashStartEnd.cu:47-67) and the stable order inside each bucket, and the stable order inside each bucket (the
+// buildHashStartEnd.cu:47-67) and the stable order inside each bucket (the
 // scatter leaves members in arbitrary order): one warp per bucket, members of
 // buckets up to 64 long are ranked by particle index in registers; longer
 // buckets go to k_bucket_big.
 __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int ncells, int* __restrict__ sorted_idx,
                              int* __restrict__ start, int* __restrict__ end, int* __restrict__ big_list,
-                             int* __restrict__ big_count) {
+                             int* __restrict__ big_count, const int* gate) {
+  if (idle(gate)) return;
   const int lane = threadIdx.x & 31;
   for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbuckets; b += (gridDim.x * blockDim.x) >> 5) {
     const int s = offs[b], e = offs[b + 1], L = e - s;
@@ -209,8 +228,9 @@ __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int nce
   }
 }
 __global__ void k_bucket_big(const int* __restrict__ offs, const int* __restrict__ big_list,
-                             const int* __restrict__ big_count, int* __restrict__ sorted_idx, int* __restrict__ tmp) {
-  if ((int)blockIdx.x >= *big_count) return;
+                             const int* __restrict__ big_count, int* __restrict__ sorted_idx, int* __restrict__ tmp,
+                             const int* gate) {
+  if (idle(gate) || (int)blockIdx.x >= *big_count) return;
   const int b = big_list[blockIdx.x];
   const int s = offs[b], e = offs[b + 1], L = e - s;
   for (int k = threadIdx.x; k < L; k += blockDim.x) tmp[s + k] = sorted_idx[s + k];
@@ -224,30 +244,29 @@ __global__ void k_bucket_big(const int* __restrict__ offs, const int* __restrict
 }
 
 __global__ void k_sorted_keys(const int* __restrict__ key, const int* __restrict__ sorted_idx, int n,
-                              int* __restrict__ sorted_key) {
+                              int* __restrict__ sorted_key, const int* gate) {
+  if (idle(gate)) return;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < n) sorted_key[p] = key[sorted_idx[p]];
 }
 
 void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorted_idx, int* sorted_key, int* start,
-                 int* end, cudaStream_t s) {
+                 int* end, cudaStream_t s, const int* gate) {
   const int nb = ncells + 2;  // bucket 0: key -1, 1..ncells: cells, ncells+1: keys past the last cell
-  cudaMemsetAsync(w.counts, 0, sizeof(int) * (size_t)(nb + 1), s);
-  cudaMemsetAsync(w.fill, 0, sizeof(int) * (size_t)(nb + 1), s);
-  cudaMemsetAsync(w.big_count, 0, sizeof(int), s);
-  if (n > 0) k_bucket_hist<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.counts);
+  k_bucket_clear<<<(nb + 1 + 255) / 256, 256, 0, s>>>(w.counts, w.fill, nb + 1, w.big_count, gate);
+  if (n > 0) k_bucket_hist<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.counts, gate);
   // exclusive scan over nb + 1 entries: offs[nb] = n
-  scan_i32(w.counts, w.offs, nb + 1, w.scan_tmp, false, s);
+  scan_i32(w.counts, w.offs, nb + 1, w.scan_tmp, false, s, gate);
   if (n > 0) {
-    k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx);
-    k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx);
+    k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx, gate);
+    k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx, gate);
   }
   k_bucket_fix<<<(unsigned)((nb + 7) / 8), 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list,
-                                                        w.big_count);
+                                                        w.big_count, gate);
   // at most n / 65 buckets can exceed 64 members
   int max_big = n / 65 + 1;
-  k_bucket_big<<<max_big, 256, 0, s>>>(w.offs, w.big_list, w.big_count, sorted_idx, w.tmp);
-  if (sorted_key && n > 0) k_sorted_keys<<<(n + 255) / 256, 256, 0, s>>>(key, sorted_idx, n, sorted_key);
+  k_bucket_big<<<max_big, 256, 0, s>>>(w.offs, w.big_list, w.big_count, sorted_idx, w.tmp, gate);
+  if (sorted_key && n > 0) k_sorted_keys<<<(n + 255) / 256, 256, 0, s>>>(key, sorted_idx, n, sorted_key, gate);
 }
 
 }  // namespace lsdem

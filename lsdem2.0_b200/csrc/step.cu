@@ -86,6 +86,12 @@ __global__ void k_integrate_first(StepArgs a) {
     P.force[i] = d3(0., 0., 0.);
     P.torque[i] = d3(0., 0., 0.);
     P.key[i] = hash_key(x, a.pg);
+    if (a.reuse) {
+      // a move beyond the neighbour-list margin (a periodic wrap included) needs a new
+      // sort and new lists
+      const double3 m = x - a.xb[i];
+      if (dot(m, m) > a.move2) atomicOr(a.reuse, 2);
+    }
     if (a.pgh.cnt) a.pgh.cnt[i] = 0;
   } else if (i < a.P.n + a.W.n) {
     const int k = i - a.P.n;
@@ -106,6 +112,7 @@ void launch_integrate_first(const StepArgs& a, cudaStream_t s) {
 
 __global__ void k_kick(StepArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && a.reuse) *a.reuse = 0;  // the next step's first kernel sets it afresh
   if (i >= a.P.n) return;
   const BodyView& P = a.P;
   const double im = P.invmass[i];
@@ -196,6 +203,20 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
   const int B = idx[k];
   const double3 x = a.P.pos[B];
   a.cell_pk[k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)a.P.radius[B]);
+  if (a.pk_key) a.pk_key[k] = a.P.key[B];
+}
+
+// Bounding-sphere test of the candidate search on the FP32 copies (centre and
+// bounding radius): the reach carries a margin that covers their rounding
+// (relative 1e-5 plus 1e-6 of the coordinates). Written with explicitly rounded
+// operations so that every caller evaluates it to the same bits.
+LD float reach_f(float4 pa, float n1a, float4 pb) {
+  const float n1 = __fadd_rn(n1a, __fadd_rn(__fadd_rn(fabsf(pb.x), fabsf(pb.y)), fabsf(pb.z)));
+  return __fmaf_rn(1e-6f, n1, __fmul_rn(__fadd_rn(pa.w, pb.w), 1.0f + 1e-5f));
+}
+LD float dist2_f(float4 pa, float4 pb) {
+  const float dx = __fsub_rn(pb.x, pa.x), dy = __fsub_rn(pb.y, pa.y), dz = __fsub_rn(pb.z, pa.z);
+  return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
 }
 
 // Candidate partners of each particle A.
@@ -203,49 +224,134 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
 // reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
 // node's 27-cell window since cells are at least 2 max radius wide). The test
-// runs on the FP32 copies with a margin that covers their rounding (relative
-// 1e-5 of the reach plus 1e-6 of the coordinates), so the candidates are a
-// superset of the exact ones; the narrowphase decides every node exactly.
+// runs on the FP32 copies (reach_f), so the candidates are a superset of the
+// exact ones; the narrowphase decides every node exactly.
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches and
 // whose interpolated phi is not provably positive over it (wall_far).
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
 // mostly share a cell, so they walk the same 27 cells (z, y, x order) in step
 // and their occupant loads are broadcasts. Slots are filled in cell-walk then
 // sorted-occupant order.
+// The walk visits the cells of the window in ascending key order and the occupants
+// of a cell in ascending index (stable sort), so its partners come in ascending
+// (cell key, index) order.
+//
+// Neighbour lists: a step that sorts and rebuilds them (*reuse != 0) also keeps, per
+// sorted position, the sorted positions k of the walk's partners within reach + skin
+// (plus 1e-5 of the coordinates, beyond the FP32 rounding of either test). Until the
+// next rebuild the sort is not run (thread t and position k keep their bodies) and
+// every particle stays within sqrt(move2) = 0.4 skin of its position at the build, so
+// a pair that passes the test now was within reach + skin then. A listed partner is a
+// walk partner when its current cell is in the window of A's current clamped cell and
+// it passes the same FP32 test; sorted by (current key, index) the listed partners
+// are exactly the walk's, in the walk's order.
 __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int n = 0, nw = 0;
+  int n = 0, nw = 0, nl = 0;
   if (t < a.P.n) {
     const int A = a.cell_idx[t];
     const double3 xA = a.P.pos[A];
     const double rA = a.P.radius[A];
     const float4 pa = a.cell_pk[t];
-    const float3 xf = make_float3(pa.x, pa.y, pa.z);
-    const float rf = pa.w, n1a = fabsf(pa.x) + fabsf(pa.y) + fabsf(pa.z);
-    const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
+    const float n1a = __fadd_rn(__fadd_rn(fabsf(pa.x), fabsf(pa.y)), fabsf(pa.z));
     const int cap = a.pp.cap;
     int* out = a.pp.id + (size_t)A * cap;
-    // the (up to) 3 cells of a row along x are contiguous in the sorted order
-    const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < a.pg.size.x - 1 ? c.x + 1 : a.pg.size.x - 1;
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int z = c.z + dz;
-      if (z < 0 || z >= a.pg.size.z) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int y = c.y + dy;
-        if (y < 0 || y >= a.pg.size.y) continue;
-        const int h0 = lin3(make_int3(x0, y, z), a.pg.size);
-        const int st = __ldg(a.cell_off + h0 + 1), en = __ldg(a.cell_off + h0 + (x1 - x0) + 2);
-#pragma unroll 4
-        for (int k = st; k < en; ++k) {
-          const float4 pb = __ldg(a.cell_pk + k);  // read-only: loads may run ahead of the slot stores
-          const float dx = pb.x - xf.x, dy = pb.y - xf.y, dz = pb.z - xf.z;
-          const float R = (rf + pb.w) * (1.0f + 1e-5f) + 1e-6f * (n1a + fabsf(pb.x) + fabsf(pb.y) + fabsf(pb.z));
-          if (dx * dx + dy * dy + dz * dz > R * R) continue;
-          const int B = __ldg(a.cell_idx + k);
-          if (B <= A) continue;
+    const bool rebuild = a.nbr && *a.reuse != 0;
+    if (t == 0 && rebuild) atomicAdd(&a.status->builds, 1);
+    const int listed = a.nbr && !rebuild ? a.nbr_cnt[t] : -1;
+    const int3 c = clamp_cell(cell_of(xA, a.pg), a.pg.size);
+    if (listed >= 0) {
+      const int sx = a.pg.size.x, sxy = a.pg.size.x * a.pg.size.y;
+      int lk = -1, lb = -1;
+      bool ordered = true;
+      // four entries at a time: their list reads, then their key, centre and index
+      // gathers, are issued together rather than one dependent chain per entry
+      for (int j0 = 0; j0 < listed; j0 += 4) {
+        int kk[4], kb[4], Bs[4];
+        float4 pb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) kk[u] = j0 + u < listed ? __ldg(a.nbr + (size_t)(j0 + u) * a.P.n + t) : -1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (kk[u] >= 0) {
+            kb[u] = a.pk_key[kk[u]];
+            pb[u] = __ldg(a.cell_pk + kk[u]);
+            Bs[u] = __ldg(a.cell_idx + kk[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (kk[u] < 0) continue;
+          const int k = kb[u];
+          if (k < 0 || k >= a.pg.ncells) continue;
+          const int bx = k % sx, by = (k / sx) % a.pg.size.y, bz = k / sxy;
+          if (abs(bx - c.x) > 1 || abs(by - c.y) > 1 || abs(bz - c.z) > 1) continue;
+          const float R = reach_f(pa, n1a, pb[u]);
+          if (dist2_f(pa, pb[u]) > __fmul_rn(R, R)) continue;
+          const int B = Bs[u];
+          if (k < lk || (k == lk && B < lb)) ordered = false;
+          lk = k;
+          lb = B;
           if (n < cap) out[n] = B;
           ++n;
         }
+      }
+      if (!ordered && n <= cap) {
+        // a partner changed cells since the build: restore the walk's order
+        for (int u = 1; u < n; ++u) {
+          const int B = out[u], kb = a.P.key[B];
+          int v = u - 1;
+          for (; v >= 0; --v) {
+            const int C = out[v], kc = a.P.key[C];
+            if (kc < kb || (kc == kb && C < B)) break;
+            out[v + 1] = C;
+          }
+          out[v + 1] = B;
+        }
+      }
+    } else {
+      // the (up to) 3 cells of a row along x are contiguous in the sorted order
+      const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < a.pg.size.x - 1 ? c.x + 1 : a.pg.size.x - 1;
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int z = c.z + dz;
+        if (z < 0 || z >= a.pg.size.z) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int y = c.y + dy;
+          if (y < 0 || y >= a.pg.size.y) continue;
+          const int h0 = lin3(make_int3(x0, y, z), a.pg.size);
+          const int st = __ldg(a.cell_off + h0 + 1), en = __ldg(a.cell_off + h0 + (x1 - x0) + 2);
+#pragma unroll 4
+          for (int k = st; k < en; ++k) {
+            const float4 pb = __ldg(a.cell_pk + k);  // read-only: loads may run ahead of the slot stores
+            const float R = reach_f(pa, n1a, pb);
+            const float d2 = dist2_f(pa, pb);
+            if (rebuild) {
+              const float n1 = __fadd_rn(n1a, __fadd_rn(__fadd_rn(fabsf(pb.x), fabsf(pb.y)), fabsf(pb.z)));
+              const float Rs = __fmul_rn(__fmaf_rn(1e-5f, n1, __fadd_rn(R, a.skin)), 1.0f + 1e-4f);
+              if (d2 > __fmul_rn(Rs, Rs)) continue;
+              const int B = __ldg(a.cell_idx + k);
+              if (B <= A) continue;
+              if (nl < a.nbr_cap) a.nbr[(size_t)nl * a.P.n + t] = k;
+              ++nl;
+              if (d2 > __fmul_rn(R, R)) continue;
+              if (n < cap) out[n] = B;
+              ++n;
+            } else {
+              if (d2 > __fmul_rn(R, R)) continue;
+              const int B = __ldg(a.cell_idx + k);
+              if (B <= A) continue;
+              if (n < cap) out[n] = B;
+              ++n;
+            }
+          }
+        }
+      }
+      if (rebuild) {
+        // an overflowed list would need a walk on an unsorted step: the batch re-runs
+        // with longer lists
+        a.nbr_cnt[t] = nl <= a.nbr_cap ? nl : -1;
+        if (nl > a.nbr_cap) atomicOr(&a.status->flags, OVF_NBR);
+        a.xb[A] = xA;
       }
     }
     a.pp.cnt[A] = n < cap ? n : cap;
@@ -274,9 +380,11 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
   // largest demand of the warp, one atomic per warp
   n = __reduce_max_sync(FULL, n);
   nw = __reduce_max_sync(FULL, nw);
+  nl = __reduce_max_sync(FULL, nl);
   if ((threadIdx.x & 31) == 0) {
     if (n > 0) atomicMax(&a.status->need_pp, n);
     if (nw > 0) atomicMax(&a.status->need_wall, nw);
+    if (nl > 0) atomicMax(&a.status->need_nbr, nl);
   }
 }
 
@@ -1495,7 +1603,9 @@ void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2
   long long n = (long long)a.G.nsets * a.P.n;
   if (n <= 0) return;
   k_ghost_compact<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
-  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(a, g2_idx);  // the candidate walk's copy is spent
+  StepArgs g = a;
+  g.pk_key = nullptr;  // the particle keys stay in the particle grid's order
+  k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(g, g2_idx);  // the candidate walk's copy is spent
   int blocks = num_sms() * 16;
   k_ghost_candidates<<<blocks, 128, 0, s>>>(a, g2_idx, g2_off);
 }
