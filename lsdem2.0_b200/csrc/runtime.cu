@@ -1052,9 +1052,10 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
   const bool branch = s->nsets > 0 && !(s->periodic & 8) && !s->profiling;
   if (branch) {
     // The periodic images run beside the particle candidates, screen and contact
-    // pass: they read the same pre-wrap positions and write only their own arrays
-    // (wrapped positions into pos_w, the image sort's scratch and packed cells).
-    // Joined, the wrapped positions are copied over before the image narrowphase.
+    // pass, which read the pre-wrap positions: the image branch writes the wrapped
+    // positions into pos_w and screens the images against them (its own sort scratch,
+    // packed cells, pair list, slots and contact-pass queue; forces and contacts are
+    // added with atomics). Joined, the wrapped positions are copied over.
     StepArgs a2 = a;
     a2.P.pos = s->pos_w.p;
     a2.cell_pk = s->cell_pk2.p;
@@ -1066,14 +1067,14 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
     launch_clamped_keys(a2, s->key2.p, s2);
     bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w2, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, s2);
     launch_ghost_candidates(a2, s->g2_idx.p, w2.offs, s2);
+    launch_narrowphase(a2, 4, s2);
+    if (s->precision != PREC_FP64) launch_contact_pass(a2, 1, s2);
     CK(cudaEventRecord(s->ev_join, s2));
     launch_candidates(a, st);
     launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st);
     if (s->precision != PREC_FP64) launch_contact_pass(a, 0, st);
     CK(cudaStreamWaitEvent(st, s->ev_join, 0));
     if (a.P.n > 0) CK(cudaMemcpyAsync(a.P.pos, s->pos_w.p, sizeof(double3) * a.P.n, cudaMemcpyDeviceToDevice, st));
-    launch_narrowphase(a, 4, st);
-    if (s->precision != PREC_FP64) launch_contact_pass(a, 1, st);
   } else {
     { PhaseTimer pt(s, 2); launch_candidates(a, st); }
     { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
