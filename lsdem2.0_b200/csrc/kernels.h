@@ -57,10 +57,20 @@ struct ShapeView {
   const float4* node_pos_f;     // FP32 copy of node_pos
   const float* lip;             // 2 per shape, in spacings: largest |phi| difference of grid
                                 //   neighbours; largest gradient-norm bound of a grid cell
+  // support tables (cube map of SUP_M x SUP_M cells per face, per shape, template units,
+  // rounded up): nodes, and the grid points bounding the solid (cells with phi <= 0)
+  const float* sup_n;
+  const float* sup_s;
 };
 
 // Arithmetic form of the narrowphase and contact forces.
 enum { PREC_FP64 = 0, PREC_FP32_FP16 = 1, PREC_FP32_BF16 = 2 };
+
+// Support tables: cells per cube-map face side.
+constexpr int SUP_M = 24;
+constexpr int SUP_CELLS = 6 * SUP_M * SUP_M;
+void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
+                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, cudaStream_t s);
 
 // A set of rigid bodies (particles or walls).
 struct BodyView {

@@ -388,6 +388,10 @@ struct lsdem_solver {
   DArr<int> reuse;
   DArr<double3> xb;
   DArr<int> nbr, nbr_cnt, pk_key;
+  // support tables of the shapes (pair separation test of the candidate search)
+  DArr<double3> sup_pts;
+  DArr<long long> sup_off;
+  DArr<float> sup_n, sup_s;
   int nbr_cap = 24;
   float skin = 0.f;
   double move2 = 0.;
@@ -718,6 +722,52 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
   {
+    // support tables: per shape, the grid points that bound the cells with a corner
+    // phi <= 0 (those cells dilated by one point in every direction, then only the
+    // points with a 6-neighbour outside the set), template units
+    std::vector<double3> pts;
+    std::vector<long long> poff{0};
+    for (const ShapeHost& sh : s->shapes) {
+      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
+      const size_t N = (size_t)nx * ny * nz;
+      auto id = [&](int x, int y, int z) { return (size_t)x + (size_t)nx * (y + (size_t)ny * z); };
+      std::vector<uint8_t> m(N), t(N);
+      for (size_t k = 0; k < N; ++k) m[k] = sh.sdf[k] <= 0.;
+      // separable dilation by one point along x, y, z (the 27-neighbourhood)
+      for (int ax = 0; ax < 3; ++ax) {
+        for (int z = 0; z < nz; ++z)
+          for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+              const int c[3] = {x, y, z}, lim[3] = {nx, ny, nz};
+              uint8_t v = m[id(x, y, z)];
+              if (c[ax] > 0) v |= m[id(x - (ax == 0), y - (ax == 1), z - (ax == 2))];
+              if (c[ax] + 1 < lim[ax]) v |= m[id(x + (ax == 0), y + (ax == 1), z + (ax == 2))];
+              t[id(x, y, z)] = v;
+            }
+        m.swap(t);
+      }
+      for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+          for (int x = 0; x < nx; ++x) {
+            if (!m[id(x, y, z)]) continue;
+            const bool edge = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
+            if (!edge && m[id(x - 1, y, z)] && m[id(x + 1, y, z)] && m[id(x, y - 1, z)] && m[id(x, y + 1, z)] &&
+                m[id(x, y, z - 1)] && m[id(x, y, z + 1)])
+              continue;
+            pts.push_back(make_double3(sh.origin[0] + sh.h * x, sh.origin[1] + sh.h * y, sh.origin[2] + sh.h * z));
+          }
+      poff.push_back((long long)pts.size());
+    }
+    const int ns = (int)s->shapes.size();
+    CK(s->sup_pts.upload(pts.data(), pts.size(), st));
+    CK(s->sup_off.upload(poff.data(), poff.size(), st));
+    CK(s->sup_n.alloc((size_t)ns * SUP_CELLS));
+    CK(s->sup_s.alloc((size_t)ns * SUP_CELLS));
+    launch_support_tables(ns, s->s_node_pos.p, s->s_node_off.p, s->s_node_cnt.p, s->sup_pts.p, s->sup_off.p,
+                          s->sup_n.p, s->sup_s.p, st);
+    CK(cudaGetLastError());
+  }
+  {
     std::vector<float4> sub;
     for (const ShapeHost& sh : s->shapes)
       for (size_t q = 0; q < sh.sub.size() / 4; ++q) {
@@ -926,6 +976,8 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.cell_off = s->s_cell_off.p;
   a.S.node_pos_f = s->s_node_f.p;
   a.S.lip = s->s_lip.p;
+  a.S.sup_n = s->sup_n.p;
+  a.S.sup_s = s->sup_s.p;
   a.pg = s->pg;
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;

@@ -206,6 +206,126 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
   if (a.pk_key) a.pk_key[k] = a.P.key[B];
 }
 
+// ---------------------------------------------------------------------------
+// Support tables and the separation test of a candidate pair.
+// A direction u falls in one cell of a cube map (face of the largest |component|,
+// then SUP_M x SUP_M cells of the face's gnomonic square). For every direction v in
+// a cell, v . p <= c . p + delta |p|, where c is the cell's centre direction and
+// delta the largest distance from c to the cell (reached at a corner: v . c is
+// quasi-concave over the square). The tables hold, per shape and cell, the largest
+// c . p + delta |p| over the template's surface nodes (sup_n) and over the grid
+// points of every cell with a corner phi <= 0 (sup_s; the points where a trilinear
+// phi can be <= 0 lie in those cells, and the maximum of this convex function over
+// them is reached at points with a 6-neighbour outside the set). delta carries 1e-5
+// beyond its exact value for the FP32 rounding of the direction (pair_separated).
+// Unit direction of face f at gnomonic coordinates (p, q).
+LD double3 sup_dir(int f, double p, double q) {
+  const double sg = (f & 1) ? -1.0 : 1.0;
+  double3 v = f < 2 ? d3(sg, p, q) : (f < 4 ? d3(q, sg, p) : d3(p, q, sg));
+  return (1.0 / sqrt(dot(v, v))) * v;
+}
+
+// One warp per (shape, cell): the two table entries.
+__global__ void k_support_tables(int nshapes, const double3* __restrict__ node_pos, const int* __restrict__ node_off,
+                                 const int* __restrict__ node_cnt, const double3* __restrict__ pts,
+                                 const long long* __restrict__ pts_off, float* __restrict__ sup_n,
+                                 float* __restrict__ sup_s) {
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= (long long)nshapes * SUP_CELLS) return;
+  const int sh = (int)(w / SUP_CELLS), cell = (int)(w % SUP_CELLS);
+  const int f = cell / (SUP_M * SUP_M), j = (cell / SUP_M) % SUP_M, i = cell % SUP_M;
+  const double h = 2.0 / SUP_M;
+  const double p0 = -1.0 + h * i, q0 = -1.0 + h * j;
+  const double3 c = sup_dir(f, p0 + 0.5 * h, q0 + 0.5 * h);
+  double delta = 0.;
+  for (int k = 0; k < 4; ++k) {
+    const double3 v = sup_dir(f, p0 + h * (k & 1), q0 + h * (k >> 1));
+    const double3 e = v - c;
+    delta = fmax(delta, sqrt(dot(e, e)));
+  }
+  delta = delta * (1.0 + 1e-9) + 1e-5;
+  double mn = -1e30, ms = -1e30;
+  for (int k = lane; k < node_cnt[sh]; k += 32) {
+    const double3 p = node_pos[node_off[sh] + k];
+    mn = fmax(mn, dot(c, p) + delta * sqrt(dot(p, p)));
+  }
+  for (long long k = pts_off[sh] + lane; k < pts_off[sh + 1]; k += 32) {
+    const double3 p = pts[k];
+    ms = fmax(ms, dot(c, p) + delta * sqrt(dot(p, p)));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmax(mn, __shfl_xor_sync(FULL, mn, o));
+    ms = fmax(ms, __shfl_xor_sync(FULL, ms, o));
+  }
+  if (lane == 0) {
+    // relative 1e-9 covers the rounding of the sums above
+    sup_n[w] = mn > -1e29 ? __double2float_ru(mn + 1e-9 * fabs(mn) + 1e-30) : -1e30f;
+    sup_s[w] = ms > -1e29 ? __double2float_ru(ms + 1e-9 * fabs(ms) + 1e-30) : -1e30f;
+  }
+}
+
+void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
+                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, cudaStream_t s) {
+  const long long warps = (long long)nshapes * SUP_CELLS;
+  if (warps <= 0) return;
+  k_support_tables<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(nshapes, node_pos, node_off, node_cnt, pts,
+                                                                       pts_off, sup_n, sup_s);
+}
+
+// The separation test's direction: the cube-map cell of a direction depends only on
+// its ratios, so the unnormalised centre difference is rotated into the body frame, in
+// FP32 with explicitly rounded operations (relative error below 1e-6, covered by the
+// tables' 1e-5 margin on delta; the list filter and the walk of k_candidates inline the
+// test at two places, and explicit rounding keeps them deciding every pair alike).
+LD float3 rot_inv_f(float3 v, Quat qd) {
+  const float w = (float)qd.q0, a = -(float)qd.q1, b = -(float)qd.q2, c = -(float)qd.q3;
+  const float tx = __fmul_rn(2.0f, __fmaf_rn(b, v.z, -__fmul_rn(c, v.y)));
+  const float ty = __fmul_rn(2.0f, __fmaf_rn(c, v.x, -__fmul_rn(a, v.z)));
+  const float tz = __fmul_rn(2.0f, __fmaf_rn(a, v.y, -__fmul_rn(b, v.x)));
+  return make_float3(__fadd_rn(__fmaf_rn(w, tx, v.x), __fmaf_rn(b, tz, -__fmul_rn(c, ty))),
+                     __fadd_rn(__fmaf_rn(w, ty, v.y), __fmaf_rn(c, tx, -__fmul_rn(a, tz))),
+                     __fadd_rn(__fmaf_rn(w, tz, v.z), __fmaf_rn(a, ty, -__fmul_rn(b, tx))));
+}
+LD int sup_cell_f(float3 u) {
+  const float ax = fabsf(u.x), ay = fabsf(u.y), az = fabsf(u.z);
+  int f;
+  float m, p, q;
+  if (ax >= ay && ax >= az) { f = u.x >= 0.f ? 0 : 1; m = ax; p = u.y; q = u.z; }
+  else if (ay >= az) { f = u.y >= 0.f ? 2 : 3; m = ay; p = u.z; q = u.x; }
+  else { f = u.z >= 0.f ? 4 : 5; m = az; p = u.x; q = u.y; }
+  if (!(m > 0.f)) return 0;
+  const float r = __frcp_rn(m);
+  int i = (int)floorf(__fmul_rn(__fmaf_rn(p, r, 1.0f), 0.5f * SUP_M));
+  int j = (int)floorf(__fmul_rn(__fmaf_rn(q, r, 1.0f), 0.5f * SUP_M));
+  i = i < 0 ? 0 : (i > SUP_M - 1 ? SUP_M - 1 : i);
+  j = j < 0 ? 0 : (j > SUP_M - 1 ? SUP_M - 1 : j);
+  return (f * SUP_M + j) * SUP_M + i;
+}
+
+// Separating-axis test of the pair (A, B) along the line of centres u: every node of
+// A projects onto u at most scale_A sup_n(A, R_A^T u) beyond x_A, and every point
+// where B's interpolated phi is <= 0 at least scale_B sup_s(B, -R_B^T u) before x_B;
+// if the two reaches sum to less than |x_B - x_A| (with margins far above the FP64
+// rounding of the node and grid-coordinate arithmetic), no node of A can be inside B,
+// and the pair has no contact. Compared squared, in FP64.
+LD bool pair_separated(const StepArgs& a, double3 xA, Quat qA, double scA, int shA, int B) {
+  const double3 xB = a.P.pos[B];
+  const double dx = __dsub_rn(xB.x, xA.x), dy = __dsub_rn(xB.y, xA.y), dz = __dsub_rn(xB.z, xA.z);
+  const double D2 = __fma_rn(dx, dx, __fma_rn(dy, dy, __dmul_rn(dz, dz)));
+  if (!(D2 > 0.)) return false;
+  const float3 df = make_float3((float)dx, (float)dy, (float)dz);
+  const float3 ua = rot_inv_f(df, qA);
+  const float3 ub = rot_inv_f(make_float3(-df.x, -df.y, -df.z), a.P.quat[B]);
+  const float hA = __ldg(a.S.sup_n + (size_t)shA * SUP_CELLS + sup_cell_f(ua));
+  const float hB = __ldg(a.S.sup_s + (size_t)a.P.shape[B] * SUP_CELLS + sup_cell_f(ub));
+  const double reach = __fma_rn(scA, (double)hA, __dmul_rn(a.P.scale[B], (double)hB));
+  if (!(reach > 0.)) return reach < 0.;  // both sets empty or behind their centres
+  const double n1 = fabs(xA.x) + fabs(xA.y) + fabs(xA.z) + fabs(xB.x) + fabs(xB.y) + fabs(xB.z);
+  const double r = __fma_rn(reach, 1.0 + 1e-9, __dmul_rn(1e-12, n1));
+  return __dmul_rn(r, r) < __dmul_rn(D2, 1.0 - 1e-9);
+}
+
 // Bounding-sphere test of the candidate search on the FP32 copies (centre and
 // bounding radius): the reach carries a margin that covers their rounding
 // (relative 1e-5 plus 1e-6 of the coordinates). Written with explicitly rounded
@@ -225,7 +345,9 @@ LD float dist2_f(float4 pa, float4 pb) {
 // reference's |node - xB| <= rB test, which in turn implies B lies in the
 // node's 27-cell window since cells are at least 2 max radius wide). The test
 // runs on the FP32 copies (reach_f), so the candidates are a superset of the
-// exact ones; the narrowphase decides every node exactly.
+// exact ones; the narrowphase decides every node exactly. A pair whose reaches along
+// the line of centres fall short of the distance (pair_separated) has no node of A
+// inside B and is dropped.
 // Wall partners: visible walls whose SDF grid box the bounding sphere reaches and
 // whose interpolated phi is not provably positive over it (wall_far).
 // One thread per particle, threads in cell-sorted order: the lanes of a warp
@@ -256,6 +378,9 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     const float n1a = __fadd_rn(__fadd_rn(fabsf(pa.x), fabsf(pa.y)), fabsf(pa.z));
     const int cap = a.pp.cap;
     int* out = a.pp.id + (size_t)A * cap;
+    const Quat qA = a.P.quat[A];
+    const double scA = a.P.scale[A];
+    const int shA = a.P.shape[A];
     const bool rebuild = a.nbr && *a.reuse != 0;
     if (t == 0 && rebuild) atomicAdd(&a.status->builds, 1);
     const int listed = a.nbr && !rebuild ? a.nbr_cnt[t] : -1;
@@ -289,6 +414,7 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
           const float R = reach_f(pa, n1a, pb[u]);
           if (dist2_f(pa, pb[u]) > __fmul_rn(R, R)) continue;
           const int B = Bs[u];
+          if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
           if (k < lk || (k == lk && B < lb)) ordered = false;
           lk = k;
           lb = B;
@@ -334,12 +460,14 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
               if (nl < a.nbr_cap) a.nbr[(size_t)nl * a.P.n + t] = k;
               ++nl;
               if (d2 > __fmul_rn(R, R)) continue;
+              if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
               if (n < cap) out[n] = B;
               ++n;
             } else {
               if (d2 > __fmul_rn(R, R)) continue;
               const int B = __ldg(a.cell_idx + k);
               if (B <= A) continue;
+              if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
               if (n < cap) out[n] = B;
               ++n;
             }
