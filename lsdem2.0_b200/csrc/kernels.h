@@ -61,6 +61,7 @@ struct ShapeView {
   // rounded up): nodes, and the grid points bounding the solid (cells with phi <= 0)
   const float* sup_n;
   const float* sup_s;
+  const float* sup_r;           // per shape: largest |p| over the sup_s points, rounded up
 };
 
 // Arithmetic form of the narrowphase and contact forces.
@@ -70,7 +71,8 @@ enum { PREC_FP64 = 0, PREC_FP32_FP16 = 1, PREC_FP32_BF16 = 2 };
 constexpr int SUP_M = 24;
 constexpr int SUP_CELLS = 6 * SUP_M * SUP_M;
 void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
-                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, cudaStream_t s);
+                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, float* sup_r,
+                           cudaStream_t s);
 
 // A set of rigid bodies (particles or walls).
 struct BodyView {
@@ -213,7 +215,8 @@ struct StepArgs {
   int* nbr;               // sorted order of the last sort: entry j of position t at j * n + t
   int* nbr_cnt;           // sorted order: entries, -1 when the list overflowed
   int nbr_cap;
-  int* pk_key;            // sorted order: this step's cell key (written with cell_pk)
+  int4* pk_meta;          // sorted order, written with cell_pk: cell key, body index, shape, FP32 scale bits
+  float4* pk_q;           // sorted order, written with cell_pk: FP32 orientation
 };
 
 // Template data for the learned-SDF kernels (mlp.cu).

@@ -387,11 +387,13 @@ struct lsdem_solver {
   bool grow_nbr = false;
   DArr<int> reuse;
   DArr<double3> xb;
-  DArr<int> nbr, nbr_cnt, pk_key;
+  DArr<int> nbr, nbr_cnt;
+  DArr<int4> pk_meta;
+  DArr<float4> pk_q;
   // support tables of the shapes (pair separation test of the candidate search)
   DArr<double3> sup_pts;
   DArr<long long> sup_off;
-  DArr<float> sup_n, sup_s;
+  DArr<float> sup_n, sup_s, sup_r;
   int nbr_cap = 24;
   float skin = 0.f;
   double move2 = 0.;
@@ -763,8 +765,9 @@ void initialize(lsdem_solver* s) {
     CK(s->sup_off.upload(poff.data(), poff.size(), st));
     CK(s->sup_n.alloc((size_t)ns * SUP_CELLS));
     CK(s->sup_s.alloc((size_t)ns * SUP_CELLS));
+    CK(s->sup_r.alloc((size_t)std::max(ns, 1)));
     launch_support_tables(ns, s->s_node_pos.p, s->s_node_off.p, s->s_node_cnt.p, s->sup_pts.p, s->sup_off.p,
-                          s->sup_n.p, s->sup_s.p, st);
+                          s->sup_n.p, s->sup_s.p, s->sup_r.p, st);
     CK(cudaGetLastError());
   }
   {
@@ -887,7 +890,8 @@ void initialize(lsdem_solver* s) {
     CK(s->reuse.alloc(1));
     CK(s->xb.alloc(std::max(n, 1)));
     CK(s->nbr_cnt.alloc(std::max(n, 1)));
-    CK(s->pk_key.alloc(std::max(n, 1)));
+    CK(s->pk_meta.alloc(std::max(n, 1)));
+    CK(s->pk_q.alloc(std::max(n, 1)));
     CK(s->nbr.alloc((size_t)std::max(n, 1) * s->nbr_cap));
     s->force_reuse = true;
   }
@@ -978,6 +982,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.lip = s->s_lip.p;
   a.S.sup_n = s->sup_n.p;
   a.S.sup_s = s->sup_s.p;
+  a.S.sup_r = s->sup_r.p;
   a.pg = s->pg;
   a.wg = s->wg;
   a.cell_idx = s->cell_idx.p; a.cell_start = s->cell_start.p; a.cell_end = s->cell_end.p;
@@ -1024,7 +1029,8 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.nbr = reuse ? s->nbr.p : nullptr;
   a.nbr_cnt = s->nbr_cnt.p;
   a.nbr_cap = s->nbr_cap;
-  a.pk_key = s->pk_key.p;
+  a.pk_meta = s->pk_meta.p;
+  a.pk_q = s->pk_q.p;
   a.mb.node = s->mb_node.p; a.mb.cap = (int)s->mb_cap;
   a.mb.pair = s->mb_pair.p; a.mb.pcap = (int)s->mb_pcap;
   a.mb.ctr = s->precision == PREC_FP64 ? nullptr : s->mb_ctr.p;
@@ -1111,7 +1117,7 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
     StepArgs a2 = a;
     a2.P.pos = s->pos_w.p;
     a2.cell_pk = s->cell_pk2.p;
-    a2.pk_key = nullptr;
+    a2.pk_meta = nullptr;
     cudaStream_t s2 = s->st2;
     CK(cudaEventRecord(s->ev_fork, st));
     CK(cudaStreamWaitEvent(s2, s->ev_fork, 0));

@@ -203,7 +203,11 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
   const int B = idx[k];
   const double3 x = a.P.pos[B];
   a.cell_pk[k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)a.P.radius[B]);
-  if (a.pk_key) a.pk_key[k] = a.P.key[B];
+  if (a.pk_meta) {
+    a.pk_meta[k] = make_int4(a.P.key[B], B, a.P.shape[B], __float_as_int((float)a.P.scale[B]));
+    const Quat q = a.P.quat[B];
+    a.pk_q[k] = make_float4((float)q.q0, (float)q.q1, (float)q.q2, (float)q.q3);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -229,7 +233,7 @@ LD double3 sup_dir(int f, double p, double q) {
 __global__ void k_support_tables(int nshapes, const double3* __restrict__ node_pos, const int* __restrict__ node_off,
                                  const int* __restrict__ node_cnt, const double3* __restrict__ pts,
                                  const long long* __restrict__ pts_off, float* __restrict__ sup_n,
-                                 float* __restrict__ sup_s) {
+                                 float* __restrict__ sup_s, float* __restrict__ sup_r) {
   const int lane = threadIdx.x & 31;
   const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= (long long)nshapes * SUP_CELLS) return;
@@ -258,6 +262,12 @@ __global__ void k_support_tables(int nshapes, const double3* __restrict__ node_p
     mn = fmax(mn, __shfl_xor_sync(FULL, mn, o));
     ms = fmax(ms, __shfl_xor_sync(FULL, ms, o));
   }
+  if (cell == 0) {  // the largest |p| of the solid's points
+    double r = 0.;
+    for (long long k = pts_off[sh] + lane; k < pts_off[sh + 1]; k += 32) r = fmax(r, sqrt(dot(pts[k], pts[k])));
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(FULL, r, o));
+    if (lane == 0) sup_r[sh] = __double2float_ru(r * (1.0 + 1e-9));
+  }
   if (lane == 0) {
     // relative 1e-9 covers the rounding of the sums above
     sup_n[w] = mn > -1e29 ? __double2float_ru(mn + 1e-9 * fabs(mn) + 1e-30) : -1e30f;
@@ -266,20 +276,21 @@ __global__ void k_support_tables(int nshapes, const double3* __restrict__ node_p
 }
 
 void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
-                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, cudaStream_t s) {
+                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, float* sup_r,
+                           cudaStream_t s) {
   const long long warps = (long long)nshapes * SUP_CELLS;
   if (warps <= 0) return;
   k_support_tables<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(nshapes, node_pos, node_off, node_cnt, pts,
-                                                                       pts_off, sup_n, sup_s);
+                                                                       pts_off, sup_n, sup_s, sup_r);
 }
 
-// The separation test's direction: the cube-map cell of a direction depends only on
-// its ratios, so the unnormalised centre difference is rotated into the body frame, in
-// FP32 with explicitly rounded operations (relative error below 1e-6, covered by the
-// tables' 1e-5 margin on delta; the list filter and the walk of k_candidates inline the
-// test at two places, and explicit rounding keeps them deciding every pair alike).
-LD float3 rot_inv_f(float3 v, Quat qd) {
-  const float w = (float)qd.q0, a = -(float)qd.q1, b = -(float)qd.q2, c = -(float)qd.q3;
+// The separation test runs in FP32 on the packed records of the candidate search, with
+// explicitly rounded operations (the list filter and the walk of k_candidates inline it
+// at two places; explicit rounding keeps them deciding every pair alike). The cube-map
+// cell of a direction depends only on its ratios, so the unnormalised centre difference
+// is rotated into each body frame.
+LD float3 rot_inv_f(float3 v, float4 q) {
+  const float w = q.x, a = -q.y, b = -q.z, c = -q.w;
   const float tx = __fmul_rn(2.0f, __fmaf_rn(b, v.z, -__fmul_rn(c, v.y)));
   const float ty = __fmul_rn(2.0f, __fmaf_rn(c, v.x, -__fmul_rn(a, v.z)));
   const float tz = __fmul_rn(2.0f, __fmaf_rn(a, v.y, -__fmul_rn(b, v.x)));
@@ -306,24 +317,28 @@ LD int sup_cell_f(float3 u) {
 // Separating-axis test of the pair (A, B) along the line of centres u: every node of
 // A projects onto u at most scale_A sup_n(A, R_A^T u) beyond x_A, and every point
 // where B's interpolated phi is <= 0 at least scale_B sup_s(B, -R_B^T u) before x_B;
-// if the two reaches sum to less than |x_B - x_A| (with margins far above the FP64
-// rounding of the node and grid-coordinate arithmetic), no node of A can be inside B,
-// and the pair has no contact. Compared squared, in FP64.
-LD bool pair_separated(const StepArgs& a, double3 xA, Quat qA, double scA, int shA, int B) {
-  const double3 xB = a.P.pos[B];
-  const double dx = __dsub_rn(xB.x, xA.x), dy = __dsub_rn(xB.y, xA.y), dz = __dsub_rn(xB.z, xA.z);
-  const double D2 = __fma_rn(dx, dx, __fma_rn(dy, dy, __dmul_rn(dz, dz)));
-  if (!(D2 > 0.)) return false;
-  const float3 df = make_float3((float)dx, (float)dy, (float)dz);
-  const float3 ua = rot_inv_f(df, qA);
-  const float3 ub = rot_inv_f(make_float3(-df.x, -df.y, -df.z), a.P.quat[B]);
+// if the two reaches sum to less than |x_B - x_A|, no node of A can be inside B and the
+// pair has no contact. Margins: the FP32 centres differ from the FP64 ones by at most
+// 2^-24 of each coordinate, so the distance by 1.2e-7 (n1 + D) and the direction by
+// 3e-7 (n1 + D) / D, plus 2e-6 for the FP32 orientation and rotation; a direction error
+// e moves a support by at most e times the set's largest |p| (the bounding radius for
+// A's nodes, scale_B sup_r for B's solid). Each margin is taken several times over.
+LD bool pair_separated(const StepArgs& a, float4 pa, float n1a, float4 qa, float scA, int shA, float4 pb, float4 qb,
+                       float scB, int shB) {
+  const float dx = __fsub_rn(pb.x, pa.x), dy = __fsub_rn(pb.y, pa.y), dz = __fsub_rn(pb.z, pa.z);
+  const float D2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+  if (!(D2 > 0.f)) return false;
+  const float3 ua = rot_inv_f(make_float3(dx, dy, dz), qa);
+  const float3 ub = rot_inv_f(make_float3(-dx, -dy, -dz), qb);
   const float hA = __ldg(a.S.sup_n + (size_t)shA * SUP_CELLS + sup_cell_f(ua));
-  const float hB = __ldg(a.S.sup_s + (size_t)a.P.shape[B] * SUP_CELLS + sup_cell_f(ub));
-  const double reach = __fma_rn(scA, (double)hA, __dmul_rn(a.P.scale[B], (double)hB));
-  if (!(reach > 0.)) return reach < 0.;  // both sets empty or behind their centres
-  const double n1 = fabs(xA.x) + fabs(xA.y) + fabs(xA.z) + fabs(xB.x) + fabs(xB.y) + fabs(xB.z);
-  const double r = __fma_rn(reach, 1.0 + 1e-9, __dmul_rn(1e-12, n1));
-  return __dmul_rn(r, r) < __dmul_rn(D2, 1.0 - 1e-9);
+  const float hB = __ldg(a.S.sup_s + (size_t)shB * SUP_CELLS + sup_cell_f(ub));
+  const float reach = __fmaf_rn(scA, hA, __fmul_rn(scB, hB));
+  const float D = __fsqrt_rn(D2);
+  const float n1 = __fadd_rn(n1a, __fadd_rn(__fadd_rn(fabsf(pb.x), fabsf(pb.y)), fabsf(pb.z)));
+  const float eps = __fadd_rn(__fdiv_rn(__fmul_rn(4e-7f, __fadd_rn(n1, D)), D), 4e-6f);
+  const float rho = __fadd_rn(pa.w, __fmul_rn(scB, __ldg(a.S.sup_r + shB)));
+  const float slack = __fmaf_rn(eps, rho, __fmaf_rn(1e-6f, n1, __fmul_rn(1e-5f, D)));
+  return __fmul_rn(__fadd_rn(reach, slack), 1.0f + 1e-5f) < D;
 }
 
 // Bounding-sphere test of the candidate search on the FP32 copies (centre and
@@ -378,9 +393,11 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     const float n1a = __fadd_rn(__fadd_rn(fabsf(pa.x), fabsf(pa.y)), fabsf(pa.z));
     const int cap = a.pp.cap;
     int* out = a.pp.id + (size_t)A * cap;
-    const Quat qA = a.P.quat[A];
-    const double scA = a.P.scale[A];
-    const int shA = a.P.shape[A];
+    const float4 qA = a.pk_q[t];
+    const int4 mA = a.pk_meta[t];
+    const float scA = __int_as_float(mA.w);
+    const int shA = mA.z;
+    const bool sep = a.S.sup_n != nullptr;
     const bool rebuild = a.nbr && *a.reuse != 0;
     if (t == 0 && rebuild) atomicAdd(&a.status->builds, 1);
     const int listed = a.nbr && !rebuild ? a.nbr_cnt[t] : -1;
@@ -392,29 +409,30 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
       // four entries at a time: their list reads, then their key, centre and index
       // gathers, are issued together rather than one dependent chain per entry
       for (int j0 = 0; j0 < listed; j0 += 4) {
-        int kk[4], kb[4], Bs[4];
-        float4 pb[4];
+        int kk[4];
+        int4 mb[4];
+        float4 pb[4], qb[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) kk[u] = j0 + u < listed ? __ldg(a.nbr + (size_t)(j0 + u) * a.P.n + t) : -1;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           if (kk[u] >= 0) {
-            kb[u] = a.pk_key[kk[u]];
+            mb[u] = a.pk_meta[kk[u]];
             pb[u] = __ldg(a.cell_pk + kk[u]);
-            Bs[u] = __ldg(a.cell_idx + kk[u]);
+            qb[u] = a.pk_q[kk[u]];
           }
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           if (kk[u] < 0) continue;
-          const int k = kb[u];
+          const int k = mb[u].x;
           if (k < 0 || k >= a.pg.ncells) continue;
           const int bx = k % sx, by = (k / sx) % a.pg.size.y, bz = k / sxy;
           if (abs(bx - c.x) > 1 || abs(by - c.y) > 1 || abs(bz - c.z) > 1) continue;
           const float R = reach_f(pa, n1a, pb[u]);
           if (dist2_f(pa, pb[u]) > __fmul_rn(R, R)) continue;
-          const int B = Bs[u];
-          if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
+          const int B = mb[u].y;
+          if (sep && pair_separated(a, pa, n1a, qA, scA, shA, pb[u], qb[u], __int_as_float(mb[u].w), mb[u].z)) continue;
           if (k < lk || (k == lk && B < lb)) ordered = false;
           lk = k;
           lb = B;
@@ -455,19 +473,21 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
               const float n1 = __fadd_rn(n1a, __fadd_rn(__fadd_rn(fabsf(pb.x), fabsf(pb.y)), fabsf(pb.z)));
               const float Rs = __fmul_rn(__fmaf_rn(1e-5f, n1, __fadd_rn(R, a.skin)), 1.0f + 1e-4f);
               if (d2 > __fmul_rn(Rs, Rs)) continue;
-              const int B = __ldg(a.cell_idx + k);
+              const int4 mb = a.pk_meta[k];
+              const int B = mb.y;
               if (B <= A) continue;
               if (nl < a.nbr_cap) a.nbr[(size_t)nl * a.P.n + t] = k;
               ++nl;
               if (d2 > __fmul_rn(R, R)) continue;
-              if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
+              if (sep && pair_separated(a, pa, n1a, qA, scA, shA, pb, a.pk_q[k], __int_as_float(mb.w), mb.z)) continue;
               if (n < cap) out[n] = B;
               ++n;
             } else {
               if (d2 > __fmul_rn(R, R)) continue;
-              const int B = __ldg(a.cell_idx + k);
+              const int4 mb = a.pk_meta[k];
+              const int B = mb.y;
               if (B <= A) continue;
-              if (a.S.sup_n && pair_separated(a, xA, qA, scA, shA, B)) continue;
+              if (sep && pair_separated(a, pa, n1a, qA, scA, shA, pb, a.pk_q[k], __int_as_float(mb.w), mb.z)) continue;
               if (n < cap) out[n] = B;
               ++n;
             }
@@ -1732,7 +1752,7 @@ void launch_ghost_candidates(const StepArgs& a, const int* g2_idx, const int* g2
   if (n <= 0) return;
   k_ghost_compact<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
   StepArgs g = a;
-  g.pk_key = nullptr;  // the particle keys stay in the particle grid's order
+  g.pk_meta = nullptr;  // the particle records stay in the particle grid's order
   k_pack_cells<<<(a.P.n + 255) / 256, 256, 0, s>>>(g, g2_idx);  // the candidate walk's copy is spent
   int blocks = num_sms() * 16;
   k_ghost_candidates<<<blocks, 128, 0, s>>>(a, g2_idx, g2_off);
