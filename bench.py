@@ -88,7 +88,7 @@ B_PAIR_SCREEN = 120
 # DRAM bytes (read + write) per k_screen_f launch, mean of the particle-pair and image
 # launches, from one ncu capture of the default workload in the FP32/BF16 form
 # (profiles/k_screen_f_polydisperse100k_dram.md); other workloads and forms report null.
-SCREEN_TRAFFIC_DEFAULT = (25.91e6 + 0.75e6 + 10.90e6) / 2
+SCREEN_TRAFFIC_DEFAULT = (22.89e6 + 0.22e6 + 11.57e6) / 2
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
 
