@@ -27,7 +27,13 @@ at 30 rpm (all shapes scaled by one factor so that they fit the drum); "scale" 2
 particles from 16 superquadrics (1,500 nodes) periodic in x and y with walls in z.
 
 One step = one full time step (half kick, drift, cell sort, candidates,
-narrowphase + contact forces, periodic images, half kick) of the whole scene.
+narrowphase + contact forces, periodic images, half kick) of the whole scene. The
+cell sort and the 27-cell candidate walk run in the steps that rebuild the
+neighbour lists (when a particle moved 0.04 of the largest bounding radius since
+the last rebuild; a periodic wrap counts); the other steps test each particle's
+list and find the same candidate pairs in the same order (lsdem_set_neighbour_lists,
+tests/test_gpu_neighbour_lists.py). Every step runs the narrowphase and the
+contact forces of every candidate pair.
 Multi-GPU: independent replicas (the step has no data-parallel split in this
 build), one process per GPU, timing = max over ranks, value = total over ranks.
 """
@@ -398,6 +404,7 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learne
     sv.step(dt, max(3, args.warmup))
     launches0 = sv.num(8)
     reruns0 = sv.num(7)
+    builds0 = sv.num(9)
     sv.set_step_timing(True, L2_FLUSH_BYTES)
     barrier()
     if clocks is not None:
@@ -411,7 +418,7 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learne
     assert step_calls == args.steps, (step_calls, args.steps)
     sv.set_step_timing(False)
     res = {"ms": step_ms, "launches": sv.num(8) - launches0, "reruns": sv.num(7) - reruns0,
-           "stats": sv.step_stats(), **info}
+           "builds": sv.num(9) - builds0, "stats": sv.step_stats(), **info}
     # the same number of steps timed as one region, L2 not flushed
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -570,6 +577,8 @@ def main():
             "screen_per_step": head.get("screen"),
             "gpu_launches": head["launches"],
             "overflow_reruns": head["reruns"],
+            # timed steps that sorted the cells and rebuilt the neighbour lists
+            "neighbour_list_rebuilds": head["builds"],
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:
