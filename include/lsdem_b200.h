@@ -186,7 +186,9 @@ int lsdem_get_shape(const lsdem_solver* s, int shape, double* nodes, double* sdf
 
 /* Broadphase of the last step: particle cell keys (-1 outside), stable sorted
  * particle index and key, per-cell [start, end) or -1 (launchUpdateSpatialGridHashStartEnd,
- * mySpatialGrid.h:33-49 / buildHashStartEnd.h). Grid: min, max, inverse cell size, cell counts. */
+ * mySpatialGrid.h:33-49 / buildHashStartEnd.h). Grid: min, max, inverse cell size, cell counts.
+ * With neighbour lists on (lsdem_set_neighbour_lists), lsdem_get_hash sorts the last step's
+ * keys when called, and the next step rebuilds the lists. */
 int lsdem_get_grid(const lsdem_solver* s, double* min3, double* max3, double* inv3, int* size3);
 int lsdem_get_wall_grid(const lsdem_solver* s, double* min3, double* max3, double* inv3, int* size3);
 int lsdem_get_hash(lsdem_solver* s, int* key, int* sorted_idx, int* sorted_key, int* cell_start, int* cell_end);
