@@ -85,13 +85,15 @@ __global__ void k_integrate_first(StepArgs a) {
     }
     P.force[i] = d3(0., 0., 0.);
     P.torque[i] = d3(0., 0., 0.);
-    P.key[i] = hash_key(x, a.pg);
+    const int key = hash_key(x, a.pg);
     if (a.reuse) {
       // a move beyond the neighbour-list margin (a periodic wrap included) needs a new
-      // sort and new lists
+      // sort and new lists; so does a body entering or leaving the domain, since the
+      // lists hold only bodies that were in a cell at the build
       const double3 m = x - a.xb[i];
-      if (dot(m, m) > a.move2) atomicOr(a.reuse, 2);
+      if (dot(m, m) > a.move2 || (key < 0) != (P.key[i] < 0)) atomicOr(a.reuse, 2);
     }
+    P.key[i] = key;
     if (a.pgh.cnt) a.pgh.cnt[i] = 0;
   } else if (i < a.P.n + a.W.n) {
     const int k = i - a.P.n;
@@ -354,6 +356,17 @@ LD float dist2_f(float4 pa, float4 pb) {
   return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
 }
 
+// Cell index along one axis of the point v, by floor and clamped to [0, n - 1]:
+// monotone in v and equal to the key's int() cell for points inside the grid.
+LD int ball_axis(double v, double mn, double inv, int n) {
+  const double f = floor((v - mn) * inv);
+  return f <= 0.0 ? 0 : (f >= (double)(n - 1) ? n - 1 : (int)f);
+}
+LD int3 ball_cell(double3 p, const GridP& g) {
+  return make_int3(ball_axis(p.x, g.mn.x, g.inv.x, g.size.x), ball_axis(p.y, g.mn.y, g.inv.y, g.size.y),
+                   ball_axis(p.z, g.mn.z, g.inv.z, g.size.z));
+}
+
 // Candidate partners of each particle A.
 // Particle partners: B > A, visible (in a cell), bounding spheres within
 // reach (|xA - xB| <= rA + rB is necessary for any node of A to pass the
@@ -456,14 +469,30 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
     } else {
       // the (up to) 3 cells of a row along x are contiguous in the sorted order
       const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < a.pg.size.x - 1 ? c.x + 1 : a.pg.size.x - 1;
-      for (int dz = -1; dz <= 1; ++dz) {
-        const int z = c.z + dz;
-        if (z < 0 || z >= a.pg.size.z) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-          const int y = c.y + dy;
-          if (y < 0 || y >= a.pg.size.y) continue;
-          const int h0 = lin3(make_int3(x0, y, z), a.pg.size);
-          const int st = __ldg(a.cell_off + h0 + 1), en = __ldg(a.cell_off + h0 + (x1 - x0) + 2);
+      // A rebuild lists every body within reach + skin of A, and that ball can reach
+      // past the 27 cells (cells are only 2 rmax wide; reach + skin is up to 2.1 rmax):
+      // it walks the cells the ball overlaps (at most two more per side), with a
+      // rounding margin far beyond the FP32 list test's, and takes candidates only
+      // from the 27-cell window, so the candidates and their order are the walk's.
+      int3 lo = make_int3(x0, max(c.y - 1, 0), max(c.z - 1, 0));
+      int3 hi = make_int3(x1, min(c.y + 1, a.pg.size.y - 1), min(c.z + 1, a.pg.size.z - 1));
+      if (rebuild) {
+        const double R = rA + a.rmax + (double)a.skin;
+        const double ext = 1.001 * R + 1e-4 * (fabs(xA.x) + fabs(xA.y) + fabs(xA.z) + 4.0 * R);
+        const int3 e0 = ball_cell(xA - d3(ext, ext, ext), a.pg), e1 = ball_cell(xA + d3(ext, ext, ext), a.pg);
+        lo = make_int3(min(lo.x, e0.x), min(lo.y, e0.y), min(lo.z, e0.z));
+        hi = make_int3(max(hi.x, e1.x), max(hi.y, e1.y), max(hi.z, e1.z));
+      }
+      for (int z = lo.z; z <= hi.z; ++z) {
+        for (int y = lo.y; y <= hi.y; ++y) {
+          const int h0 = lin3(make_int3(lo.x, y, z), a.pg.size);
+          const int st = __ldg(a.cell_off + h0 + 1), en = __ldg(a.cell_off + h0 + (hi.x - lo.x) + 2);
+          // sorted positions of the row's cells inside the 27-cell window
+          int wst = 0, wen = 0;
+          if (abs(z - c.z) <= 1 && abs(y - c.y) <= 1) {
+            wst = __ldg(a.cell_off + h0 + (x0 - lo.x) + 1);
+            wen = __ldg(a.cell_off + h0 + (x1 - lo.x) + 2);
+          }
 #pragma unroll 4
           for (int k = st; k < en; ++k) {
             const float4 pb = __ldg(a.cell_pk + k);  // read-only: loads may run ahead of the slot stores
@@ -478,11 +507,13 @@ __global__ void __launch_bounds__(128) k_candidates(StepArgs a) {
               if (B <= A) continue;
               if (nl < a.nbr_cap) a.nbr[(size_t)nl * a.P.n + t] = k;
               ++nl;
+              if (k < wst || k >= wen) continue;
               if (d2 > __fmul_rn(R, R)) continue;
               if (sep && pair_separated(a, pa, n1a, qA, scA, shA, pb, a.pk_q[k], __int_as_float(mb.w), mb.z)) continue;
               if (n < cap) out[n] = B;
               ++n;
             } else {
+              if (k < wst || k >= wen) continue;
               if (d2 > __fmul_rn(R, R)) continue;
               const int4 mb = a.pk_meta[k];
               const int B = mb.y;

@@ -106,3 +106,64 @@ def test_reuse_equals_full_walk(lsdem, prec, periodic):
     for k in ("pos", "vel", "angvel", "quat"):
         scale = max(np.abs(b[k]).max(), 1e-30)
         assert np.abs(a[k] - b[k]).max() <= 1e-12 * scale, k
+
+
+def _two_pair_scene(lsdem):
+    """Two pairs of (5, 4, 3) mm ellipsoids with their long axes on the line of centres,
+    2.05 bounding radii apart (0.25 mm gap) across two cell faces: the lower-index body
+    sits 0.05 mm before a face, so at the build its partner is two cells away, outside its
+    27-cell window, but within reach plus the margin. The bodies then close the gap by
+    0.19 mm each, less than the rebuild distance (0.2 mm), and touch: the walk finds the
+    pairs in the window of the moved cells, so the lists must hold them. Pair 1 lies along
+    +x (the partner above the owner's cell), pair 2 along -z (below it)."""
+    from lsdem_b200 import scenes
+    shp = scenes.make_ellipsoid((5e-3, 4e-3, 3e-3), 16, 300)
+    probe = {"shape": shp, "pos": np.array([[0.05, 0.05, 0.05]]), "quat": np.array([[1.0, 0, 0, 0]]),
+             "vel": np.zeros((1, 3)), "kn": 1e5, "ks": 8e4, "mu": 0.5, "e": 0.6, "density": 2500.0,
+             "min": np.zeros(3), "max": np.full(3, 0.1), "gravity": np.zeros(3), "floor": None}
+    sv = load_scene(lsdem, scenes, probe)
+    r = float(sv.particle_params()["radius"][0])
+    w = 1.0 / sv.grid()["inv"]
+    sv.close()
+    assert np.allclose(w, w[0]) and 2 * r <= w[0] < 2.1 * r
+    d = 2.05 * r
+    eps = 5e-5
+    s = np.sqrt(0.5)
+    qz = np.array([s, 0.0, -s, 0.0])  # body x axis along world z
+    pos = np.array([[3 * w[0] - eps, 0.05, 0.05], [3 * w[0] - eps + d, 0.05, 0.05],
+                    [0.08, 0.08, 6 * w[0] + eps], [0.08, 0.08, 6 * w[0] + eps - d]])
+    quat = np.array([[1.0, 0, 0, 0], [1.0, 0, 0, 0], qz, qz])
+    v = 4.0
+    vel = np.array([[v, 0, 0], [-v, 0, 0], [0, 0, -v], [0, 0, v]])
+    return dict(probe, pos=pos, quat=quat, vel=vel), r
+
+
+@pytest.mark.parametrize("prec", [0, 2])
+def test_lists_hold_partners_beyond_the_27_cells(lsdem, prec):
+    from lsdem_b200 import scenes
+    sc, r = _two_pair_scene(lsdem)
+    dt, steps = 2e-6, 24
+    assert v_moved(sc, dt, steps) < 0.4 * 0.1 * r  # below the rebuild distance
+    runs = []
+    for reuse in (True, False):
+        sv = load_scene(lsdem, scenes, sc, precision=prec, **CAP)
+        sv.set_neighbour_lists(reuse)
+        per = []
+        for _ in range(steps):
+            sv.step(dt, 1)
+            s = sv.step_stats()
+            per.append((s["pairs_particle"], s["contacts"]))
+        runs.append((per, sv.num(9), sv.contacts(lsdem.CONTACT_PARTICLE), sv.state()))
+        sv.close()
+    (pa, builds, ca, sa), (pb, _, cb, sb) = runs
+    assert builds == 1  # the lists were built once, before the bodies moved
+    assert pb[0] == (0, 0) and max(x[0] for x in pb) == 2 and max(x[1] for x in pb) > 0  # both pairs touch
+    assert pa == pb
+    oa, ob = canon(ca), canon(cb)
+    assert np.array_equal(ca["node"][oa], cb["node"][ob]) and np.array_equal(ca["partner"][oa], cb["partner"][ob])
+    for k in ("pos", "vel"):
+        assert np.abs(sa[k] - sb[k]).max() <= 1e-12 * np.abs(sb[k]).max(), k
+
+
+def v_moved(sc, dt, steps):
+    return float(np.abs(sc["vel"]).max()) * dt * steps

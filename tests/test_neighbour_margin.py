@@ -10,6 +10,12 @@ restated in numpy float32 (each add and multiply rounded to FP32; fused multiply
 rounded once), on random polydisperse packings placed near the origin and far from it,
 with every pair moved towards each other by the full rebuild distance each, and the
 margin shown to be needed: without the skin, pairs are missed.
+
+The rebuild also has to reach the listed bodies: cells are only 2 rmax wide and reach +
+skin is up to 2.1 rmax, so a listed partner can lie two cells away. The rebuild walk's
+cell range (the 27 cells widened to the ball of reach + skin) is restated and checked on
+near-largest bodies: every pair found after the moves was listed, while a walk of the
+27 cells alone would miss some.
 """
 import numpy as np
 
@@ -84,3 +90,62 @@ def test_lists_hold_every_pair_after_moves_far_from_origin():
 def test_the_margin_is_needed():
     passes, listed = _check(np.zeros(3), skin_scale=0.0, seed=2)
     assert (passes & ~listed).any()
+
+
+def _walk_window(xa, ra, rmax, skin, mn, w, size):
+    """Cells the rebuild walks for owners at xa (k_candidates): the 27 cells around the
+    clamped cell, widened to every cell the ball of reach + skin overlaps."""
+    c = np.clip(np.floor((xa - mn) / w).astype(np.int64), 0, size - 1)
+    R = ra + rmax + skin
+    ext = 1.001 * R + 1e-4 * (np.abs(xa).sum(axis=1) + 4.0 * R)
+    e0 = np.clip(np.floor((xa - ext[:, None] - mn) / w), 0, size - 1).astype(np.int64)
+    e1 = np.clip(np.floor((xa + ext[:, None] - mn) / w), 0, size - 1).astype(np.int64)
+    lo = np.minimum(np.clip(c - 1, 0, size - 1), e0)
+    hi = np.maximum(np.clip(c + 1, 0, size - 1), e1)
+    return c, lo, hi
+
+
+def _window_check(offset, seed):
+    """Pairs of near-largest bodies at 1.9-2.1 bounding radii along random directions,
+    owners anywhere in their cells (cell = 2 rmax, the narrowest grid). Returns, per
+    pair, whether it passes the plain test and lies in the 27-cell window after both
+    bodies moved the rebuild distance towards each other, whether the rebuild walk
+    listed it, and whether a walk of the 27 cells alone would have."""
+    rng = np.random.default_rng(seed)
+    n = 200_000
+    rmax = 1e-3
+    ra, rb = rmax * rng.uniform(0.9, 1.0, n), rmax * rng.uniform(0.9, 1.0, n)
+    w = 2.0 * rmax
+    mn = offset - 0.5
+    size = np.full(3, int(1.0 / w))
+    xa = offset + rng.uniform(-0.2, 0.2, size=(n, 3))
+    u = rng.standard_normal((n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    xb = xa + (rng.uniform(1.9, 2.1, n) * rmax)[:, None] * u
+    sr = 0.1 * rmax
+    skin = f32(sr)
+    pa, pb = _packed(xa, ra), _packed(xb, rb)
+    R, n1 = _reach(pa, pb)
+    Rs = (_fma(np.full_like(n1, f32(1e-5)), n1, (R + skin).astype(f32)) * f32(1.0 + 1e-4)).astype(f32)
+    within = _dist2(pa, pb) <= (Rs * Rs).astype(f32)
+    c, lo, hi = _walk_window(xa, ra, rmax, sr, mn, w, size)
+    cb = np.floor((xb - mn) / w).astype(np.int64)
+    walked = ((cb >= lo) & (cb <= hi)).all(axis=1)
+    in27 = (np.abs(cb - c) <= 1).all(axis=1)
+    move = 0.4 * sr
+    xa1, xb1 = xa + move * u, xb - move * u
+    qa, qb = _packed(xa1, ra), _packed(xb1, rb)
+    R1, _ = _reach(qa, qb)
+    c1 = np.clip(np.floor((xa1 - mn) / w).astype(np.int64), 0, size - 1)
+    cb1 = np.floor((xb1 - mn) / w).astype(np.int64)
+    found = (_dist2(qa, qb) <= (R1 * R1).astype(f32)) & (np.abs(cb1 - c1) <= 1).all(axis=1)
+    return found, within & walked, within & in27
+
+
+def test_rebuild_walk_lists_partners_beyond_the_27_cells():
+    for offset, seed in ((np.zeros(3), 3), (np.full(3, 3.0), 4)):
+        found, listed, listed27 = _window_check(offset, seed)
+        assert found.sum() > 1000
+        assert not (found & ~listed).any()
+        # a walk of the 27 cells alone misses pairs that later pass
+        assert (found & ~listed27).any()
