@@ -346,8 +346,10 @@ int lsdem_set_neighbour_lists(lsdem_solver* s, int on);
  * or fixed budget). Its scratch is one fixed device array of the library, which
  * limits a call to 262,144 bodies and 262,144 cells (LSDEM_ERR_ARG beyond, with
  * a message on stderr). The first call on a device looks up that array's device
- * address, so it should come before any stream capture. All calls share the
- * array; calls that overlap on the GPU race. */
+ * address, so it should come before any stream capture; that address is kept
+ * for the life of the process, so the entry point must not be used on a device
+ * again after cudaDeviceReset. All calls share the array; calls that overlap on
+ * the GPU race. */
 int lsdem_cell_sort_static(const void* pos_dev, int n, const double* min3, const double* max3, const double* inv3,
                            const int* size3, int* key_dev, int* sorted_idx_dev, int* sorted_key_dev,
                            int* cell_start_dev, int* cell_end_dev, void* stream);

@@ -134,7 +134,7 @@ void scan_i64(const long long* in, long long* out, long long n, long long* tmp, 
 // Bucket sort by cell key.
 // Bucket of a key: 0 for -1 (outside the domain), 1 + key for a cell, and a
 // last bucket for keys >= ncells (a centre rounding onto the upper domain face),
-// which, as in the reference, sort after every cell and belong to none.
+// which, as in the reference, sort after every cell, by key, and belong to none.
 __device__ __forceinline__ int bucket_of(int k, int ncells) { return k < 0 ? 0 : (k >= ncells ? ncells + 1 : k + 1); }
 
 __global__ void k_bucket_clear(int* __restrict__ counts, int* __restrict__ fill, int m, int* __restrict__ big_count,
@@ -192,14 +192,19 @@ __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells
   }
 }
 
+// (key, index) order: a stable sort by key puts the keys past the last cell, which
+// share the last bucket, in ascending key and then index order.
+__device__ __forceinline__ bool key_idx_less(int ka, int a, int kb, int b) { return ka < kb || (ka == kb && a < b); }
+
 // Cell ranges [start, end) of every cell (-1 when empty; findStartAndEnd,
 // buildHashStartEnd.cu:47-67) and the stable order inside each bucket (the
 // scatter leaves members in arbitrary order): one warp per bucket, members of
-// buckets up to 64 long are ranked by particle index in registers; longer
-// buckets go to k_bucket_big.
-__global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int ncells, int* __restrict__ sorted_idx,
-                             int* __restrict__ start, int* __restrict__ end, int* __restrict__ big_list,
-                             int* __restrict__ big_count, const int* gate) {
+// buckets up to 64 long are ranked by particle index in registers (the last
+// bucket by key, then index); longer buckets go to k_bucket_big, except the -1
+// bucket, which k_special_buckets has put in index order.
+__global__ void k_bucket_fix(const int* __restrict__ key, const int* __restrict__ offs, int nbuckets, int ncells,
+                             int* __restrict__ sorted_idx, int* __restrict__ start, int* __restrict__ end,
+                             int* __restrict__ big_list, int* __restrict__ big_count, const int* gate) {
   if (idle(gate)) return;
   const int lane = threadIdx.x & 31;
   for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbuckets; b += (gridDim.x * blockDim.x) >> 5) {
@@ -209,32 +214,58 @@ __global__ void k_bucket_fix(const int* __restrict__ offs, int nbuckets, int nce
       end[b - 1] = L > 0 ? e : -1;
     }
     if (L <= 1) continue;
-    if ((b == 0 || b == ncells + 1) && L > 64) continue;  // placed in index order by k_special_buckets
+    if (b == 0 && L > 64) continue;  // placed in index order by k_special_buckets
     if (L > 64) {
+      // the last bucket was put in index order by k_special_buckets; k_bucket_big
+      // re-ranks it by key
       if (lane == 0) big_list[atomicAdd(big_count, 1)] = b;
       continue;
     }
     const int v0 = lane < L ? sorted_idx[s + lane] : 0x7fffffff;
     const int v1 = lane + 32 < L ? sorted_idx[s + 32 + lane] : 0x7fffffff;
     int r0 = 0, r1 = 0;
-    for (int j = 0; j < 32; ++j) {
-      const int u0 = __shfl_sync(0xffffffffu, v0, j), u1 = __shfl_sync(0xffffffffu, v1, j);
-      r0 += (u0 < v0) + (u1 < v0);
-      r1 += (u0 < v1) + (u1 < v1);
+    if (b == ncells + 1) {
+      const int k0 = lane < L ? key[v0] : 0x7fffffff, k1 = lane + 32 < L ? key[v1] : 0x7fffffff;
+      for (int j = 0; j < 32; ++j) {
+        const int u0 = __shfl_sync(0xffffffffu, v0, j), u1 = __shfl_sync(0xffffffffu, v1, j);
+        const int w0 = __shfl_sync(0xffffffffu, k0, j), w1 = __shfl_sync(0xffffffffu, k1, j);
+        r0 += key_idx_less(w0, u0, k0, v0) + key_idx_less(w1, u1, k0, v0);
+        r1 += key_idx_less(w0, u0, k1, v1) + key_idx_less(w1, u1, k1, v1);
+      }
+    } else {
+      for (int j = 0; j < 32; ++j) {
+        const int u0 = __shfl_sync(0xffffffffu, v0, j), u1 = __shfl_sync(0xffffffffu, v1, j);
+        r0 += (u0 < v0) + (u1 < v0);
+        r1 += (u0 < v1) + (u1 < v1);
+      }
     }
     __syncwarp();
     if (lane < L) sorted_idx[s + r0] = v0;
     if (lane + 32 < L) sorted_idx[s + r1] = v1;
   }
 }
-__global__ void k_bucket_big(const int* __restrict__ offs, const int* __restrict__ big_list,
-                             const int* __restrict__ big_count, int* __restrict__ sorted_idx, int* __restrict__ tmp,
-                             const int* gate) {
+// One block per bucket longer than 64: rank of each member by index (by key, then
+// index, in the last bucket, whose keys differ).
+__global__ void k_bucket_big(const int* __restrict__ key, const int* __restrict__ offs, int ncells,
+                             const int* __restrict__ big_list, const int* __restrict__ big_count,
+                             int* __restrict__ sorted_idx, int* __restrict__ tmp, const int* gate) {
   if (idle(gate) || (int)blockIdx.x >= *big_count) return;
   const int b = big_list[blockIdx.x];
   const int s = offs[b], e = offs[b + 1], L = e - s;
   for (int k = threadIdx.x; k < L; k += blockDim.x) tmp[s + k] = sorted_idx[s + k];
   __syncthreads();
+  if (b == ncells + 1) {
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+      const int v = tmp[s + k], kv = key[v];
+      int r = 0;
+      for (int m = 0; m < L; ++m) {
+        const int u = tmp[s + m];
+        r += key_idx_less(key[u], u, kv, v);
+      }
+      sorted_idx[s + r] = v;
+    }
+    return;
+  }
   for (int k = threadIdx.x; k < L; k += blockDim.x) {
     const int v = tmp[s + k];
     int r = 0;
@@ -261,11 +292,11 @@ void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorte
     k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx, gate);
     k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx, gate);
   }
-  k_bucket_fix<<<(unsigned)((nb + 7) / 8), 256, 0, s>>>(w.offs, nb, ncells, sorted_idx, start, end, w.big_list,
+  k_bucket_fix<<<(unsigned)((nb + 7) / 8), 256, 0, s>>>(key, w.offs, nb, ncells, sorted_idx, start, end, w.big_list,
                                                         w.big_count, gate);
   // at most n / 65 buckets can exceed 64 members
   int max_big = n / 65 + 1;
-  k_bucket_big<<<max_big, 256, 0, s>>>(w.offs, w.big_list, w.big_count, sorted_idx, w.tmp, gate);
+  k_bucket_big<<<max_big, 256, 0, s>>>(key, w.offs, ncells, w.big_list, w.big_count, sorted_idx, w.tmp, gate);
   if (sorted_key && n > 0) k_sorted_keys<<<(n + 255) / 256, 256, 0, s>>>(key, sorted_idx, n, sorted_key, gate);
 }
 

@@ -14,7 +14,10 @@
 // Host code cannot name the device array's address directly: the symbol seen
 // by host code is a host-side stand-in. The first call on each device looks the
 // device address up with cudaGetSymbolAddress while that device is current,
-// so that first call should come before any stream capture. Every call shares
+// so that first call should come before any stream capture. The address is kept
+// for the life of the process: after cudaDeviceReset on a device, the library's
+// device array may sit elsewhere, so this entry point must not be called on that
+// device again in the same process. Every call shares
 // the array and it keeps the last call's contents; each call clears what must
 // start at zero. Calls that overlap on the GPU (for example on two streams at
 // once) race on the shared array.
@@ -63,8 +66,11 @@ extern "C" int lsdem_cell_sort_static(const void* pos_dev, int n, const double* 
     fprintf(stderr, "lsdem_cell_sort_static: null or negative argument\n");
     return LSDEM_ERR_ARG;
   }
-  const long long ncells = (long long)size3[0] * size3[1] * size3[2];
-  if (size3[0] < 1 || size3[1] < 1 || size3[2] < 1 || ncells > kMaxCells || n > kMaxBodies) {
+  // each factor is checked before the product, which then cannot overflow
+  const bool sizes_ok = size3[0] >= 1 && size3[1] >= 1 && size3[2] >= 1 && size3[0] <= kMaxCells &&
+                        size3[1] <= kMaxCells && size3[2] <= kMaxCells;
+  const long long ncells = sizes_ok ? (long long)size3[0] * size3[1] * size3[2] : -1;
+  if (!sizes_ok || ncells > kMaxCells || n > kMaxBodies) {
     fprintf(stderr,
             "lsdem_cell_sort_static: %d bodies / %lld cells exceed the fixed scratch (at most %d bodies and %d "
             "cells)\n",
