@@ -309,6 +309,7 @@ class OracleSim:
       walls: dict(shape, pos, vel, angvel, quat, radius, mu, e, origin, invh) or None
       bonds: dict(ids, B, geo, frames, bonded, state) or None
       domain: (min, max), gravity, periodic axes mask
+      grid_cell (optional): particle grid cell size (default 2 x the largest radius)
     """
 
     def __init__(self, model, flags=0, nthreads=1, literal_wrap_arms=False):
@@ -342,7 +343,10 @@ class OracleSim:
         self.F = np.zeros((self.np_, 3))
         self.T = np.zeros((self.np_, 3))
         rp = float(np.max(self.P["radius"])) if self.np_ else 0.0
-        self.pg = grid_set(self.dmin, self.dmax, 2.0 * rp if self.np_ else 0.0)
+        # grid_cell: the cell size of a larger system this model is a part of (a spatial
+        # sub-box keeps the whole system's grid, so keys and windows are the same)
+        cell = float(model["grid_cell"]) if model.get("grid_cell") else (2.0 * rp if self.np_ else 0.0)
+        self.pg = grid_set(self.dmin, self.dmax, cell)
         if self.W is not None and len(self.W["pos"]):
             self.wg = grid_set(self.dmin, self.dmax, 2.0 * float(np.max(self.W["radius"])))
             self.w_sdf_off = offs[i32(self.W["shape"])].astype(np.int64)
