@@ -1,30 +1,33 @@
 """Benchmark of the level-set DEM time step (particle-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload polydisperse|small|bonded|drum|scale] [--form fp32-bf16|fp32-fp16|fp64]
+                    [--workload scale|polydisperse|small|bonded|drum]
+                    [--form fp32-bf16-learned|fp32-bf16|fp32-fp16|fp64]
 
-Workload (default "polydisperse", the precision-form configuration, which fits one
-GPU): 100,000 particles from 4 templates (ellipsoid 1:0.8:0.6, superquadric
-exponent 4, rounded cube, capsule of aspect 2) with log-normal bounding
-diameters (median 2 mm, sigma 0.25), 48^3 SDF grids, 2,000 surface nodes each,
-0.1 m triply periodic cube, velocities N(0, 0.1 m/s), linear contact (kn 1e5,
+Workload (default "scale", the largest configuration that fits one GPU and the one the
+"plain grid vs FP32 + learned SDF" comparison is stated for): 2,000,000 particles from 16
+seeded superquadrics (exponents uniform 2-6, semi-axes uniform 1-2.5 mm, 1,500 surface
+nodes, 48-node grids along the longest axis from the mesh distance of each shape's
+20,480-triangle mesh), periodic in x and y with a floor and a ceiling, settling under
+gravity from a random loose packing (solid fraction 0.25), linear contact (kn 1e5,
 kt 0.8 kn, mu 0.5, e 0.6), dt 5e-7 s. Synthetic, seeded (no dataset).
 
-The headline form is the configuration's own precision form: the narrowphase
-screens nodes in FP32 against BF16 SDF templates, rejecting only nodes that
-error bounds prove the FP64 test rejects; the remaining nodes and all contacts
-are evaluated in FP64 (positions, integration, spring history stay FP64). The
-same run times the FP16-template form and the plain FP64 form (the reference's
-arithmetic, bit-exact pair lists) and states each precision form's force error
-against the FP64 path from the same state.
+The headline form is FP32 + learned SDF: one 3-64-64-1 SiLU network per shape, trained on
+the GPU, screens nodes before the FP32 screen on BF16 grid templates; both only reject
+nodes that measured or proven error bounds show the FP64 test rejects, and the remaining
+nodes and all contacts are evaluated in FP64 (positions, integration, spring history stay
+FP64). The same run times the plain grid form (FP64, the reference's arithmetic, bit-exact
+pair lists) and the FP32 grid screen without the network, and states each FP32 form's force,
+torque and energy error against the FP64 path from the same state.
 
 Other workloads (--workload; each a stated configuration of the method, synthetic and seeded):
-"small" 2,000 ellipsoids (5, 4, 3 mm) falling on a floor, 32^3 grids, 1,000 nodes, dt 1e-6 s;
-"bonded" 50,000 aligned ellipsoids (2, 1.6, 1.2 mm) on a jittered HCP lattice with ~286,000
-V-bonds, floor and a top wall moving down at 0.1 m/s, dt 2e-7 s; "drum" 500,000 particles from
-64 superquadrics (64^3 grids, 1,500 nodes) in a drum of radius 0.15 m and length 0.1 m turning
-at 30 rpm (all shapes scaled by one factor so that they fit the drum); "scale" 2,000,000
-particles from 16 superquadrics (1,500 nodes) periodic in x and y with walls in z.
+"polydisperse" 100,000 particles from 4 templates (48^3 grids, 2,000 nodes), log-normal sizes,
+0.1 m triply periodic cube, velocities N(0, 0.1 m/s); "small" 2,000 ellipsoids (5, 4, 3 mm)
+falling on a floor, 32^3 grids, 1,000 nodes, dt 1e-6 s; "bonded" 50,000 aligned ellipsoids (2,
+1.6, 1.2 mm) on a jittered HCP lattice with ~286,000 V-bonds, floor and a top wall moving down
+at 0.1 m/s, dt 2e-7 s; "drum" 500,000 particles from 64 superquadrics (64^3 grids, 1,500
+nodes) in a drum of radius 0.15 m and length 0.1 m turning at 30 rpm (all shapes scaled by one
+factor so that they fit the drum).
 
 One step = one full time step (half kick, drift, cell sort, candidates,
 narrowphase + contact forces, periodic images, half kick) of the whole scene. The
@@ -289,13 +292,67 @@ def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
             "contact_energy_rel": abs(ep - e64) / e64 if e64 > 0 else None}
 
 
+SAMPLE_PARTICLES = 4000  # host sample of the large-scale workload (CPU baseline, reference arm)
+
+
+def _oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as ora  # the checker, timed as the CPU baseline / reference arm only
+    return ora
+
+
+def _scenes_host():
+    """The scenes module loaded on its own (it imports nothing of the package), so that the
+    reference arm prepares its sample without loading the CUDA library."""
+    spec = importlib.util.spec_from_file_location("lsdem_scenes_host", ROOT / "lsdem2.0_b200" / "scenes.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def scale_sample(ora, scenes, T):
+    """The bounded host sample of the large-scale workload: SAMPLE_PARTICLES bodies of its 16
+    superquadrics (grids T), periodic in x and y, floor and ceiling, the same solid fraction
+    (scenes.settling_sample), as an oracle model."""
+    def mass_fn(sdf, size, origin, h):
+        o = ora.mass_props(sdf, size, origin, h, 1.0)
+        return o[0], o[1:4].copy(), o[10:16].copy()
+    smp = scenes.settling_sample(mass_fn, T, SAMPLE_PARTICLES, seed=scenes.seed_for(4) + 7919)
+    return ora.model_from_scene(smp), smp
+
+
+def time_oracle(ora, model, dt, steps, min_seconds, max_steps):
+    """Steps of the FP64 oracle on all host threads: one untimed (history), then at least
+    `steps`, and more until `min_seconds` (at most `max_steps`). Returns (steps, seconds, threads)."""
+    threads = os.cpu_count() or 1
+    ora.set_threads(threads)
+    sim = ora.OracleSim(model, nthreads=threads)
+    sim.step(dt)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps or (time.perf_counter() - t0 < min_seconds and done < max_steps):
+        sim.step(dt)
+        done += 1
+    return done, time.perf_counter() - t0, threads
+
+
 def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_seconds=10.0, max_steps=200):
     """FP64 oracle step (the reference algorithm restated on the CPU, all host threads) on a
-    bounded sample: the particles inside a corner sub-box of the same scene (for the bonded,
-    drum and settling workloads the cluster of particles nearest the median position). At least
-    `steps` steps are timed, and more until `min_seconds` of CPU work (at most `max_steps`)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as ora  # the checker, timed here as the CPU baseline
+    bounded sample. Large-scale workload: a smaller box of the same configuration
+    (scale_sample, the same templates). Others: the particles inside a corner sub-box of the
+    same scene (for the bonded and drum workloads the cluster of particles nearest the median
+    position). At least `steps` steps are timed, and more until `min_seconds` of CPU work (at
+    most `max_steps`)."""
+    ora = _oracle()
+    if workload == "scale" and "raw_templates" in sc:
+        from lsdem_b200 import scenes
+        model, smp = scale_sample(ora, scenes, sc["raw_templates"])
+        done, t, threads = time_oracle(ora, model, sc["dt"], steps, min_seconds, max_steps)
+        m = len(smp["pos"])
+        return {"value": m * done / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                "sample": (f"{m} particles of the same 16 superquadrics in a box periodic in x and y with floor and "
+                           f"ceiling at the same solid fraction ({smp['max'][0]:.4f} m side), random sequential "
+                           f"addition, {done} steps of the FP64 oracle (reference per-node 27-cell algorithm)")}
 
     n = len(sc["pos"])
     pos = np.asarray(sc["pos"])
@@ -340,17 +397,7 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_second
         dmin, dmax = lo, sub_hi
     model = ora.model_from_solver(sv)
     model.update(domain=(dmin, dmax), gravity=sc["gravity"], periodic=0)
-    threads = os.cpu_count() or 1
-    ora.set_threads(threads)
-    sim = ora.OracleSim(model, nthreads=threads)
-    sim.step(sc["dt"])  # untimed first step (history)
-    t0 = time.perf_counter()
-    done = 0
-    while done < steps or (time.perf_counter() - t0 < min_seconds and done < max_steps):
-        sim.step(sc["dt"])
-        done += 1
-    t = time.perf_counter() - t0
-    steps = done
+    steps, t, threads = time_oracle(ora, model, sc["dt"], steps, min_seconds, max_steps)
     m = len(idx)
     return {"value": m * steps / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
             "sample": (f"{m} particles of the same scene in a {frac:.3f}-scaled corner sub-box, {steps} steps "
@@ -359,25 +406,94 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_second
                   f"them), {steps} steps of the FP64 oracle (reference per-node 27-cell algorithm)")}
 
 
+def fundem_config0(binary, scenes, workdir):
+    """Config 0 (2,000 ellipsoids on a floor, 32^3 grids, 1,000 nodes) through an LSSolver app
+    built from tests/apps/c0_bench.cpp: device time of steps 200-1900 from CUDA events
+    recorded in the app's external-force hook. Returns ms per step, or None."""
+    if not Path(binary).exists():
+        return None
+    workdir.mkdir(parents=True, exist_ok=True)
+    sc = scenes.ellipsoid_falling()
+    nsteps, k0, k1 = 2000, 200, 1900
+    scene, res = workdir / "c0.bin", workdir / "c0.res"
+    scenes.write_c0_app_scene(scene, sc, nsteps, k0, k1)
+    r = subprocess.run([str(binary), str(scene), str(workdir / "out"), str(res)], capture_output=True, text=True,
+                       timeout=900)
+    if r.returncode != 0:
+        return None
+    steps, window, ms, _ = scenes.read_c0_app_result(res)
+    return {"ms_per_step": ms / window, "window_steps": window, "particles": len(sc["pos"])}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference algorithm's CPU implementation (the FP64 oracle port;
-    the reference has no CPU path of its own) on the host cores, same metric and workload."""
+    the reference has no CPU path of its own) on the host cores, same metric and workload.
+    For the large-scale workload everything is prepared on the host (the CUDA library is not
+    loaded): the same 16 templates from the oracle's host grid generator, a smaller box of
+    the same configuration, the oracle's own mass properties. Beside it, the reference's own
+    CUDA build runs the config-0 app on this box's GPU (when it was built)."""
     if rank != 0:
         return
-    lsdem = _package()
-    import torch  # noqa: F401  (device 0 hosts the scene preparation)
-    sc, cfg = build_scene(lsdem, args.workload, 0, args.particles)
-    cb = cpu_baseline(lsdem, sc, args.workload, steps=max(1, min(args.steps, 3)))
+    ora = _oracle()
+    scenes = _scenes_host()
+    if args.workload == "scale":
+        rng = np.random.default_rng(scenes.seed_for(4))
+        t0 = time.perf_counter()
+        T = scenes.superquadric_templates_host(lambda v, f, o, size, h: ora.mesh_grid(v, f, o, size, h), rng, 16,
+                                               (2.0, 6.0), (1e-3, 2.5e-3), 48, 1500)
+        t_prep = time.perf_counter() - t0
+        model, smp = scale_sample(ora, scenes, T)
+        steps, t, threads = time_oracle(ora, model, 5e-7, max(1, args.steps), 0.0, max(1, args.steps))
+        m = len(smp["pos"])
+        cfg = {"workload": "settling-2000000-superquadrics-16", "particles": 2_000_000, "templates": 16,
+               "nodes_per_particle": 1500, "sdf_grid": "48 nodes on the longest axis", "periodic": "xy",
+               "walls": "z", "solid_fraction": 0.25, "dt_s": 5e-7}
+        cb = {"value": m * steps / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+              "sample": (f"{m} particles of the same 16 superquadrics (grids from the oracle's host generator, "
+                         f"{t_prep:.0f} s) in a box periodic in x and y with floor and ceiling at the same solid "
+                         f"fraction ({smp['max'][0]:.4f} m side), {steps} steps of the FP64 oracle "
+                         f"(reference per-node 27-cell algorithm)")}
+    else:
+        lsdem = _package()
+        import torch  # noqa: F401  (device 0 hosts the scene preparation)
+        sc, cfg = build_scene(lsdem, args.workload, 0, args.particles)
+        cb = cpu_baseline(lsdem, sc, args.workload, steps=max(1, min(args.steps, 3)))
     line = {"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "impl": "reference", "config": cfg, "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if not args.no_fundem:
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            fd = fundem_config0(ROOT / "oracle" / "_ref" / "c0_bench_fundem", scenes, Path(d))
+        if fd is not None:
+            line["fundem_gpu_config0"] = dict(fd, build="the reference's own CUDA kernels and LSSolver.h (sm_100a), "
+                                                        "app tests/apps/c0_bench.cpp")
     print(json.dumps(line), flush=True)
 
 
 L2_FLUSH_BYTES = 256 << 20  # > the 126 MB L2
+
+
+def build_c0_app():
+    """Builds tests/apps/c0_bench.cpp against the drop-in LSSolver header and this library
+    (nvcc, sm_100a) under the package's build folder; returns the executable or None."""
+    import shutil
+    app = ROOT / "tests" / "apps" / "c0_bench.cpp"
+    out = ROOT / "lsdem2.0_b200" / "_build" / "c0_bench_b200"
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if out.exists() and out.stat().st_mtime >= app.stat().st_mtime:
+        return out
+    if not Path(nvcc).exists():
+        return None
+    out.parent.mkdir(exist_ok=True)
+    r = subprocess.run([nvcc, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I", str(ROOT / "include"), "-I", str(ROOT / "include" / "kernel"), str(app),
+                        "-L", str(ROOT / "lsdem2.0_b200"), "-llsdem_b200", "-Xlinker", "-rpath", "-Xlinker",
+                        str(ROOT / "lsdem2.0_b200"), "-o", str(out)], capture_output=True, text=True)
+    return out if r.returncode == 0 else None
 
 
 def max_over_ranks(dist, value, device):
@@ -446,13 +562,15 @@ def time_form(lsdem, torch, sc, args, local, prec, dist, barrier, clocks, learne
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="polydisperse", choices=["polydisperse", "small", "bonded", "drum", "scale"])
-    ap.add_argument("--form", default="fp32-bf16", choices=list(FORMS))
+    ap.add_argument("--workload", default="scale", choices=["polydisperse", "small", "bonded", "drum", "scale"])
+    ap.add_argument("--form", default="fp32-bf16-learned", choices=list(FORMS))
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fundem", action="store_true", help="skip the config-0 app leg")
+    ap.add_argument("--all-forms", action="store_true", help="also time the FP16-template form")
     ap.add_argument("--headline-only", action="store_true", help="skip the other forms and the error check")
     ap.add_argument("--particles", type=int, default=100_000, help="polydisperse workload size (profiling cases)")
     args = ap.parse_args()
@@ -518,7 +636,7 @@ def main():
     forms = {}
     if not args.headline_only:
         for name, p in FORMS.items():
-            if name == args.form:
+            if name == args.form or (name == "fp32-fp16" and not args.all_forms):
                 continue
             svf, r = time_form(lsdem, torch, sc, args, local, p, dist, barrier, None, learned="learned" in name)
             svf.close()
@@ -529,9 +647,20 @@ def main():
                 forms[name]["training"] = r["training"]
                 forms[name]["screen_per_step"] = r.get("screen")
         for name, p in FORMS.items():
-            if p != 0:
+            if p != 0 and (name != "fp32-fp16" or args.all_forms):
                 err = force_error(lsdem, sc, args.workload, local, p, learned="learned" in name)
                 forms.setdefault(name, {})["error_vs_fp64"] = err
+
+    # the config-0 app through the drop-in LSSolver header (same source as the reference
+    # arm's build of the reference), built here against this library
+    dropin0 = None
+    if rank == 0 and not args.no_fundem:
+        import tempfile
+        from lsdem_b200 import scenes
+        exe = build_c0_app()
+        if exe is not None:
+            with tempfile.TemporaryDirectory() as d:
+                dropin0 = fundem_config0(exe, scenes, Path(d))
 
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -557,6 +686,9 @@ def main():
         forms[args.form] = dict(forms.get(args.form, {}), value=value, ms_per_step=ms_step,
                                 warm_l2={"value": n * world * args.steps / (head["warm_ms"] * 1e-3),
                                          "ms_per_step": head["warm_ms"] / args.steps})
+        per_s = world * args.steps / (head["ms"] * 1e-3)  # steps per second, all ranks
+        scr = head.get("screen") or {}
+        plain = forms.get("fp64", {}).get("value")
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -567,6 +699,9 @@ def main():
                               f"its events (per-step algorithmic traffic {b_step / 1e6:.0f} MB)",
                            contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs),
             "forms": forms,
+            "headline_over_plain_grid": (value / plain) if plain else None,
+            "contacts_per_s": stats["contacts"] * per_s,
+            "node_tests_per_s": scr.get("node_tests", 0.0) * per_s if scr else None,
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
@@ -581,6 +716,9 @@ def main():
             "neighbour_list_rebuilds": head["builds"],
             "clocks": clk.summary(),
         }
+        if dropin0 is not None:
+            line["dropin_gpu_config0"] = dict(dropin0, build="tests/apps/c0_bench.cpp against include/kernel/LSSolver.h "
+                                                              "and this library (FP64 form)")
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(lsdem, sc, args.workload)
         print(json.dumps(line), flush=True)

@@ -18,6 +18,7 @@ phi > 0 on the free side), built with published methods:
 from __future__ import annotations
 
 import math
+import struct
 
 import numpy as np
 
@@ -308,8 +309,10 @@ def random_quaternions(rng, n):
     return np.stack([s2 * np.cos(b), s1 * np.sin(a), s1 * np.cos(a), s2 * np.sin(b)], 1)
 
 
-def rsa_positions(rng, n, radii, lo, hi, max_tries=200, periodic=False):
-    """Random sequential addition of non-overlapping spheres (radii per particle) in the box [lo, hi]."""
+def rsa_positions(rng, n, radii, lo, hi, max_tries=200, periodic=False, placed_out=None):
+    """Random sequential addition of non-overlapping spheres (radii per particle) in the box [lo, hi].
+    placed_out (optional boolean array of n): a sphere that finds no room is skipped (marked
+    False there, position NaN) instead of raising."""
     lo = np.asarray(lo, np.float64)
     hi = np.asarray(hi, np.float64)
     L = hi - lo
@@ -348,9 +351,14 @@ def rsa_positions(rng, n, radii, lo, hi, max_tries=200, periodic=False):
                 pos[i] = p
                 grid.setdefault(tuple(c), []).append(i)
                 placed += 1
+                if placed_out is not None:
+                    placed_out[i] = True
                 break
         else:
-            raise RuntimeError(f"RSA could not place particle {i} (fraction too high)")
+            if placed_out is None:
+                raise RuntimeError(f"RSA could not place particle {i} (fraction too high)")
+            placed_out[i] = False
+            pos[i] = np.nan
     return pos
 
 
@@ -660,9 +668,7 @@ def superquadric_templates(lsdem, rng, count, exponents, semi_axes, n_grid, n_no
     on the GPU by the reference's buildGrid rule with a spacing that puts about n_grid nodes
     along the longest axis; the surface nodes are Fibonacci directions scaled onto the surface."""
     T = []
-    for _ in range(count):
-        p = float(rng.uniform(*exponents))
-        ax = rng.uniform(*semi_axes, size=3)
+    for p, ax in superquadric_specs(rng, count, exponents, semi_axes):
         ee = en = 2.0 / p
         v, f = superellipsoid_mesh(ax, ee, en, level)
         h = 2.0 * float(ax.max()) / (n_grid - 1 - 2 * pad)
@@ -670,6 +676,91 @@ def superquadric_templates(lsdem, rng, count, exponents, semi_axes, n_grid, n_no
         T.append({"nodes": superellipsoid_nodes(ax, ee, en, n_nodes), "sdf": sdf, "size": size, "origin": origin,
                   "spacing": h, "exponent": p, "semi_axes": ax})
     return T
+
+
+def superquadric_specs(rng, count, exponents, semi_axes):
+    """Exponent and semi-axes of each of `count` seeded superquadrics (the draws of
+    superquadric_templates, in its order)."""
+    out = []
+    for _ in range(count):
+        p = float(rng.uniform(*exponents))
+        ax = rng.uniform(*semi_axes, size=3)
+        out.append((p, ax))
+    return out
+
+
+def mesh_grid_box_np(verts, spacing, pad=2):
+    """Grid box of buildGrid around a mesh (LevelSetObjectGenerator.h:122-170): the vertices'
+    bounding box grown by max(1, pad) spacings, snapped outward to multiples of the spacing
+    (the same operations as the library's lsdem_mesh_grid_box, so the same bits)."""
+    v = np.asarray(verts, np.float64).reshape(-1, 3)
+    mn, mx = v.min(axis=0), v.max(axis=0)
+    padding = float(max(1, pad)) * spacing
+    lo = spacing * np.floor((mn - padding) / spacing)
+    hi = spacing * np.ceil((mx + padding) / spacing)
+    size = (np.floor((hi - lo) / spacing + 0.5) + 1).astype(np.int32)
+    return lo, size
+
+
+def superquadric_templates_host(grid_fn, rng, count, exponents, semi_axes, n_grid, n_nodes, level=5, pad=2):
+    """superquadric_templates without the library: the same shapes (same draws of `rng`), with
+    each grid from grid_fn(verts, tris, origin, size, spacing) (a host mesh-grid routine that
+    computes the reference's buildGrid values, e.g. the oracle's)."""
+    T = []
+    for p, ax in superquadric_specs(rng, count, exponents, semi_axes):
+        ee = en = 2.0 / p
+        v, f = superellipsoid_mesh(ax, ee, en, level)
+        h = 2.0 * float(ax.max()) / (n_grid - 1 - 2 * pad)
+        origin, size = mesh_grid_box_np(v, h, pad)
+        T.append({"nodes": superellipsoid_nodes(ax, ee, en, n_nodes), "sdf": grid_fn(v, f, origin, size, h),
+                  "size": size, "origin": origin, "spacing": h, "exponent": p, "semi_axes": ax})
+    return T
+
+
+def settling_sample(mass_fn, T, n, seed, solid_fraction=0.25, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0,
+                    dt=5e-7, exclusion=0.85):
+    """A bounded sample of the large-scale workload for host-side timing: n particles of the
+    templates T (as drawn for that workload) in a box periodic in x and y with a floor and a
+    ceiling, at the same solid fraction, placed by random sequential addition of spheres of
+    `exclusion` x the bounding radius (this module's host RSA), random orientations, at rest.
+    mass_fn(sdf, size, origin, spacing) -> (mass, centroid, inv_inertia) at density 1 (the
+    reference's smoothed-Heaviside integration, LSSolver.h:66-135). Deep initial overlaps are
+    not re-placed (no device is used)."""
+    rng = np.random.default_rng(seed)
+    tm = []
+    for t in T:
+        mass, c, iI = mass_fn(t["sdf"], t["size"], t["origin"], t["spacing"])
+        tm.append({"nodes": t["nodes"] - c, "sdf": t["sdf"], "size": t["size"], "origin": t["origin"] - c,
+                   "spacing": t["spacing"], "mass": mass, "inv_inertia": iI,
+                   "bound": float(np.max(np.linalg.norm(t["nodes"] - c, axis=1)))})
+    shape = rng.integers(0, len(tm), size=n).astype(np.int32)
+    vol = np.array([t["mass"] for t in tm])[shape].sum()
+    L = (vol / solid_fraction) ** (1.0 / 3.0)
+    bound = np.array([t["bound"] for t in tm])[shape]
+    b = float(bound.max())
+    order = np.argsort(-bound, kind="stable")
+    pos = np.empty((n, 3))
+    placed = np.zeros(n, bool)
+    pos[order] = rsa_positions(rng, n, exclusion * bound[order], np.array([0.0, 0.0, b]), np.array([L, L, L - b]),
+                               max_tries=300, periodic=True, placed_out=placed)
+    ok = np.empty(n, bool)
+    ok[order] = placed
+    H = L + b
+    if not ok.all():
+        # as the full workload: bodies that find no room go to a reserve slab above the
+        # packing (bounding spheres at 20 % fraction, no overlaps)
+        left = np.nonzero(~ok)[0]
+        slab = len(left) * (4.0 / 3.0) * math.pi * float(np.mean(bound[left] ** 3)) / 0.2 / (L * L) + 2 * b
+        pos[left] = rsa_positions(rng, len(left), bound[left], np.array([0.0, 0.0, L + b]),
+                                  np.array([L, L, L + b + slab]), max_tries=20000, periodic=True)
+        H = L + b + slab
+    scale = np.ones(n)
+    inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
+    walls = [plane_wall(L, [0.5 * L, 0.5 * L, 0.0], True, mu, e), plane_wall(L, [0.5 * L, 0.5 * L, H], False, mu, e)]
+    return {"templates": tm, "shape": shape, "scale": scale, "pos": pos, "quat": random_quaternions(rng, n),
+            "vel": np.zeros((n, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
+            "mu": mu, "e": e, "dt": dt, "min": np.zeros(3), "max": np.array([L, L, H]),
+            "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 3, "walls": walls, "solid_fraction": solid_fraction}
 
 
 def bonded_hcp(lsdem, n=50_000, axes=(2e-3, 1.6e-3, 1.2e-3), n_grid=32, n_nodes=1000, gap=0.05, jitter=0.02,
@@ -835,4 +926,40 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
             "vel": np.zeros((n, 3)), "inv_mass": inv_mass, "inv_inertia": inv_inertia, "kn": kn, "ks": kt_ratio * kn,
             "mu": mu, "e": e, "dt": dt, "min": np.zeros(3), "max": np.array([L, L, H]),
             "gravity": np.array([0.0, 0.0, -9.81]), "periodic": 3, "walls": walls, "rsa": rsa,
-            "solid_fraction": solid_fraction}
+            "solid_fraction": solid_fraction, "raw_templates": T}
+
+
+def write_c0_app_scene(path, sc, nsteps, k0, k1):
+    """Scene file of the config-0 app (tests/apps/c0_bench.cpp, written against the LSSolver
+    API only, so the same source builds against the reference and against the drop-in):
+    magic "LSDEMC0", shape (node count, grid size, spacing, origin, nodes, SDF), particles
+    (count, positions, quaternions, velocities), material (kn, ks, mu, e, density), the floor
+    wall (grid, spacing, origin, SDF, position, quaternion, mu, e, vertices, two triangles),
+    dt, domain, gravity, and the step count with the timed window (k0, k1]."""
+    s, f = sc["shape"], sc["floor"]
+    n = len(sc["pos"])
+    d = lambda a: np.ascontiguousarray(a, np.float64).tobytes()
+    i32 = lambda *v: struct.pack(f"<{len(v)}i", *v)
+    cx, cy = 0.5 * (sc["min"][0] + sc["max"][0]), 0.5 * (sc["min"][1] + sc["max"][1])
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+    with open(path, "wb") as fh:
+        fh.write(b"LSDEMC0\0")
+        fh.write(i32(len(s["nodes"]), *[int(v) for v in s["size"]], n))
+        fh.write(d([s["spacing"]]) + d(s["origin"]) + d(s["nodes"]) + d(s["sdf"]))
+        fh.write(d(sc["pos"]) + d(sc["quat"]) + d(sc["vel"]))
+        fh.write(d([sc["kn"], sc["ks"], sc["mu"], sc["e"], sc["density"]]))
+        fh.write(i32(*[int(v) for v in f["size"]]) + d([f["spacing"]]) + d(f["origin"]) + d(f["sdf"]))
+        fh.write(d([cx, cy, sc["min"][2]]) + d([1.0, 0.0, 0.0, 0.0]) + d([sc["mu"], sc["e"]]))
+        fh.write(i32(len(f["verts"]), len(tris)) + d(f["verts"]) + tris.tobytes())
+        fh.write(d([sc["dt"]]) + d(sc["min"]) + d(sc["max"]) + d(sc["gravity"]))
+        fh.write(i32(nsteps, k0, k1))
+
+
+def read_c0_app_result(path):
+    """(steps run, window length, window device time in ms, velocities at the window's end)
+    from the result file of the config-0 app."""
+    raw = open(path, "rb").read()
+    steps, window, nvel = struct.unpack("<3i", raw[:12])
+    ms = struct.unpack("<d", raw[12:20])[0]
+    vel = np.frombuffer(raw[20:20 + 24 * nvel], np.float64).reshape(nvel, 3)
+    return steps, window, ms, vel

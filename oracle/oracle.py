@@ -482,3 +482,63 @@ def model_from_solver(sv, with_walls=True):
         bonds = {"ids": b["ids"], "B": bp["B"], "geo": bp["geo"], "frames": bp["frames"], "bonded": b["bonded"],
                  "state": b["state"]}
     return {"shapes": shapes, "particles": particles, "walls": walls, "bonds": bonds}
+
+
+def model_from_scene(sc):
+    """The oracle model of a multi-template scene dict (the scenes module's layout), built on
+    the host with the solver's set-up rules and no device: per-particle grid origin scaled
+    and inverse spacing 1 / (scale h), bounding radius max |scale * node|
+    (LSParticle.h:175-181), quaternions normalised, kn / ks / mu clamped at 0, restitution
+    outside (0, 1] set to 1 (LSParticle.h:193-202); wall radius = largest vertex distance
+    (LSSolver.h:255-271)."""
+    T = sc["templates"]
+    shapes = [{"nodes": f64(t["nodes"], (-1, 3)), "sdf": f64(t["sdf"]), "size": i32(t["size"]),
+               "origin": f64(t["origin"]), "spacing": float(t["spacing"])} for t in T]
+    sh = i32(sc["shape"])
+    n = len(sh)
+    scale = f64(sc["scale"])
+    cache = {}
+
+    def body_radius(s, c):
+        if (s, c) not in cache:
+            p = shapes[s]["nodes"] * c if c != 1.0 else shapes[s]["nodes"]
+            cache[(s, c)] = float(np.max(np.sqrt(p[:, 0] * p[:, 0] + p[:, 1] * p[:, 1] + p[:, 2] * p[:, 2])))
+        return cache[(s, c)]
+    radius = np.array([body_radius(int(sh[i]), float(scale[i])) for i in range(n)])
+    origin = np.array([shapes[s]["origin"] * (scale[i] if scale[i] != 1.0 else 1.0) for i, s in enumerate(sh)])
+    invh = np.array([1.0 / (shapes[s]["spacing"] * scale[i] if scale[i] != 1.0 else shapes[s]["spacing"])
+                     for i, s in enumerate(sh)])
+    q = f64(sc["quat"], (-1, 4))
+    q = q / np.sqrt((q ** 2).sum(axis=1))[:, None]
+    full = lambda v: np.full(n, float(v)) if np.ndim(v) == 0 else f64(v)
+    res = full(sc["e"])
+    res = np.where((res <= 0.0) | (res > 1.0), 1.0, res)
+    particles = {"shape": sh, "scale": scale, "pos": f64(sc["pos"], (-1, 3)).copy(),
+                 "vel": f64(sc.get("vel", np.zeros((n, 3))), (-1, 3)).copy(),
+                 "angvel": f64(sc.get("angvel", np.zeros((n, 3))), (-1, 3)).copy(), "quat": q,
+                 "inv_mass": f64(sc["inv_mass"]), "inv_inertia": f64(sc["inv_inertia"], (-1, 6)),
+                 "radius": radius, "kn": np.maximum(full(sc["kn"]), 0.0), "ks": np.maximum(full(sc["ks"]), 0.0),
+                 "mu": np.maximum(full(sc["mu"]), 0.0), "e": res, "origin": origin, "invh": invh}
+    walls = None
+    if sc.get("walls"):
+        W = sc["walls"]
+        k0 = len(shapes)
+        for w in W:
+            shapes.append({"nodes": np.zeros((0, 3)), "sdf": f64(w["sdf"]), "size": i32(w["size"]),
+                           "origin": f64(w["origin"]), "spacing": float(w["spacing"])})
+        wq = np.array([f64(w["quat"]) / np.sqrt((f64(w["quat"]) ** 2).sum()) for w in W])
+        walls = {"shape": np.arange(k0, k0 + len(W), dtype=np.int32),
+                 "pos": np.array([f64(w["pos"]) for w in W]),
+                 "vel": np.array([f64(w.get("vel", np.zeros(3)) if w.get("vel") is not None else np.zeros(3))
+                                  for w in W]),
+                 "angvel": np.array([f64(w.get("angvel", np.zeros(3)) if w.get("angvel") is not None
+                                         else np.zeros(3)) for w in W]),
+                 "quat": wq, "radius": np.array([float(np.max(np.sqrt((f64(w["verts"], (-1, 3)) ** 2).sum(1))))
+                                                 for w in W]),
+                 "mu": np.array([max(float(w["mu"]), 0.0) for w in W]),
+                 "e": np.array([float(w["e"]) if 0.0 < float(w["e"]) <= 1.0 else 1.0 for w in W]),
+                 "origin": np.array([f64(w["origin"]) for w in W]),
+                 "invh": np.array([1.0 / float(w["spacing"]) for w in W])}
+    return {"shapes": shapes, "particles": particles, "walls": walls, "bonds": None,
+            "domain": (f64(sc["min"]), f64(sc["max"])), "gravity": f64(sc["gravity"]),
+            "periodic": int(sc.get("periodic", 0))}

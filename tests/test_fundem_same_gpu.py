@@ -57,23 +57,8 @@ def build_ours(app=APP, out=OURS) -> None:
 
 
 def write_scene(path, sc, nsteps, k0, k1):
-    s, f = sc["shape"], sc["floor"]
-    n = len(sc["pos"])
-    d = lambda a: np.ascontiguousarray(a, np.float64).tobytes()
-    i32 = lambda *v: struct.pack(f"<{len(v)}i", *v)
-    cx, cy = 0.5 * (sc["min"][0] + sc["max"][0]), 0.5 * (sc["min"][1] + sc["max"][1])
-    tris = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
-    with open(path, "wb") as fh:
-        fh.write(b"LSDEMC0\0")
-        fh.write(i32(len(s["nodes"]), *[int(v) for v in s["size"]], n))
-        fh.write(d([s["spacing"]]) + d(s["origin"]) + d(s["nodes"]) + d(s["sdf"]))
-        fh.write(d(sc["pos"]) + d(sc["quat"]) + d(sc["vel"]))
-        fh.write(d([sc["kn"], sc["ks"], sc["mu"], sc["e"], sc["density"]]))
-        fh.write(i32(*[int(v) for v in f["size"]]) + d([f["spacing"]]) + d(f["origin"]) + d(f["sdf"]))
-        fh.write(d([cx, cy, sc["min"][2]]) + d([1.0, 0.0, 0.0, 0.0]) + d([sc["mu"], sc["e"]]))
-        fh.write(i32(len(f["verts"]), len(tris)) + d(f["verts"]) + tris.tobytes())
-        fh.write(d([sc["dt"]]) + d(sc["min"]) + d(sc["max"]) + d(sc["gravity"]))
-        fh.write(i32(nsteps, k0, k1))
+    from lsdem_b200 import scenes
+    scenes.write_c0_app_scene(path, sc, nsteps, k0, k1)
 
 
 def _structure(path):
@@ -126,11 +111,8 @@ def run(binary, scene, outdir, result):
     r = subprocess.run([str(binary), str(scene), str(outdir), str(result)], capture_output=True, text=True,
                        timeout=900)
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
-    raw = result.read_bytes()
-    steps, window, nvel = struct.unpack("<3i", raw[:12])
-    ms = struct.unpack("<d", raw[12:20])[0]
-    vel = np.frombuffer(raw[20:20 + 24 * nvel], np.float64).reshape(nvel, 3)
-    return steps, window, ms, vel
+    from lsdem_b200 import scenes
+    return scenes.read_c0_app_result(result)
 
 
 @pytest.mark.skipif(not FUNDEM.exists(), reason="oracle/_ref/c0_bench_fundem not built (needs the reference tree)")
