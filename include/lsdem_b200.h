@@ -36,12 +36,14 @@ extern "C" {
 
 typedef struct lsdem_solver lsdem_solver;
 
-/* External force hook, called once per step after the contact and bond
- * forces and before the second half kick, with the simulation time of the
+/* External force hook, called exactly once per step after the contact and
+ * bond forces and before the second half kick, with the simulation time of the
  * step. Replaces the virtual LSSolver::addExternalForceTorque (LSSolver.h:508).
  * Kernels it launches on the solver's stream (or the legacy default stream
- * when the solver uses it) see the step's forces. When a step batch is
- * re-run after a capacity overflow, the hook is called again for those steps. */
+ * when the solver uses it) see the step's forces. With a hook, lsdem_step reads
+ * each step's capacity status before the hook runs (one host synchronisation per
+ * step, as the reference's per-step reads); a step whose lists overflowed is re-run
+ * with grown capacities before its hook is called, so no step's hook runs twice. */
 typedef void (*lsdem_hook)(void* user, double time);
 
 /* Solver lifetime. Replaces LSSolver(dir, stream, maxGPUThread, device) (LSSolver.h:14).
@@ -144,7 +146,13 @@ int lsdem_set_precision(lsdem_solver* s, int mode);
 int lsdem_set_periodic(lsdem_solver* s, int axes);
 
 /* Uploads the model and builds the grids for the domain [min, max)
- * (LSSolver::upload + checkSolverInput, LSSolver.h:566-623). */
+ * (LSSolver::upload + checkSolverInput, LSSolver.h:566-623). Called again after
+ * steps (a new solve() phase), it starts from the current state with the host-side
+ * edits made since (moves, wall velocities, new bodies or bonds), keeps the last
+ * step's forces for the first half kick and, while the bodies, their surface nodes and
+ * the periodic image sets are unchanged, the contact history (the reference keeps its
+ * contact arrays, SolidInteraction.h:24-27); the simulation time restarts at 0, as each
+ * of the reference's phases (LSSolver.h:994-996). */
 int lsdem_initialize(lsdem_solver* s, const double* min3, const double* max3, const double* gravity3);
 
 /* Advances nsteps time steps of size dt (loop body of LSSolver::compute*, LSSolver.h:1000-1128):
@@ -334,6 +342,17 @@ int lsdem_set_graphs(lsdem_solver* s, int on);
  * the 27 cells every step as the reference does (LSSolver.h:1000-1011,
  * mySpatialGrid.cu, LSParticleContactDetectionKernel.cu). */
 int lsdem_set_neighbour_lists(lsdem_solver* s, int on);
+
+/* Snapshot of the dynamic state (no counterpart in the reference, which writes its
+ * state only as VTU frames): particle position, velocity, angular velocity,
+ * orientation, force and torque, wall pose and velocities, bond flags and state, the
+ * contact history of the last step (candidate slots, contact nodes and FP64 springs),
+ * time and step count, in one binary file. lsdem_snapshot_load restores it into a
+ * solver initialized with the same bodies, surface nodes, bonds and image sets
+ * (LSDEM_ERR_ARG otherwise), growing capacities to the file's; the steps that follow
+ * are those the saved solver would have taken. Both need lsdem_initialize first. */
+int lsdem_snapshot_save(lsdem_solver* s, const char* path);
+int lsdem_snapshot_load(lsdem_solver* s, const char* path);
 
 /* Broadphase cell sort that allocates no device memory: cell keys of n body
  * centres (pos_dev: device array of n x 3 doubles), their stable sorted order

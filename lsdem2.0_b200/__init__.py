@@ -112,6 +112,8 @@ _SIGS = {
     "lsdem_set_neighbour_lists": (C.c_int, [P, C.c_int]),
     "lsdem_write_vtu": (C.c_int, [P, C.c_char_p, C.c_ulonglong, C.c_ulonglong, C.c_double]),
     "lsdem_mesh_grid": (C.c_int, [DP, C.c_int, IP, C.c_int, DP, IP, C.c_double, C.c_int, DP, C.c_int]),
+    "lsdem_snapshot_save": (C.c_int, [P, C.c_char_p]),
+    "lsdem_snapshot_load": (C.c_int, [P, C.c_char_p]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -313,6 +315,14 @@ class Solver:
         """Reuse per-particle neighbour lists between steps (default; exact), sorting the
         cells only when lists are rebuilt, or sort and walk the 27 cells every step."""
         self._chk(lib.lsdem_set_neighbour_lists(self.h, 1 if on else 0), "set_neighbour_lists")
+
+    def snapshot_save(self, path):
+        """Writes the dynamic state and contact history to a binary snapshot file."""
+        self._chk(lib.lsdem_snapshot_save(self.h, str(path).encode()), "snapshot_save")
+
+    def snapshot_load(self, path):
+        """Restores a snapshot into this (initialized, same-model) solver."""
+        self._chk(lib.lsdem_snapshot_load(self.h, str(path).encode()), "snapshot_load")
 
     def set_triangles(self, kind, index, tris):
         """Triangles of a body's nodes (kind 0 particle, 1 wall) for the mesh output files."""

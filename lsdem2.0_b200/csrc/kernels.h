@@ -18,7 +18,7 @@ namespace lsdem {
 enum { FIX_GRADIENT = 1, FIX_SQRTF = 2 };
 
 // Overflow bits of the device status word.
-enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8, OVF_NBR = 16 };
+enum { OVF_PP = 1, OVF_WALL = 2, OVF_GHOST = 4, OVF_CONTACT = 8, OVF_NBR = 16, OVF_NET = 32 };
 
 // Largest demands seen during a batch (whether or not they overflowed), used
 // to grow capacities ahead of an overflow.
@@ -30,6 +30,9 @@ struct Status {
   int need_contact;  // largest contact total
   int need_nbr;      // largest per-particle neighbour-list length
   int builds;        // steps that sorted and rebuilt the neighbour lists
+  int need_netq;     // learned form: largest rows of one shape's network queue
+  int need_pend;     // learned form: largest count of nodes awaiting the network
+  int errors;        // a bounded wait in a kernel gave up (results of the batch not valid)
   int pad;
 };
 
@@ -173,6 +176,25 @@ struct PairLists {
   int* ctr;      // [kind] entries appended this step (nullptr: lists not built)
 };
 
+// Learned form, per narrowphase launch (0: particles and walls, 1: periodic images):
+// the screen passes every node it cannot reject by the partner's bounds to the
+// network of the partner's shape (rows grouped by shape, for 128-row tensor-core
+// tiles) and keeps, per pair in node order, the nodes awaiting the verdict; the
+// network pass writes each verdict (after the grid test of the nodes it keeps) and
+// the compaction pass queues the surviving nodes of each pair for the FP64 pass.
+struct NetView {
+  float4* row;            // nshapes * qcap: (u.x, u.y, u.z, pending index bits)
+  int* cnt;               // nshapes: rows appended this step
+  int qcap;               // rows per shape
+  float4* pend_g;         // pcap: grid point in the partner's grid (x, y, z), the pair's threshold T
+  int* pend_n;            // pcap: node index; bit 31 set: within the error of the grid boundary
+  unsigned char* pend_v;  // pcap: 1 when the node goes on to the FP64 test
+  int pcap;
+  int4* pair;             // paircap: {A, kind << 24 | slot, pending start, pending count}
+  int paircap;
+  int* ctr;               // [0] pending cursor, [1] pair records
+};
+
 struct StepArgs {
   BodyView P;       // particles
   BodyView W;       // walls
@@ -205,6 +227,8 @@ struct StepArgs {
   const MlpInfer* mlp_inf;   // per shape (nullptr: off)
   const MlpNorm* mlp_norm;   // per shape
   const float* mlp_band;     // per shape: trust band + error bound, in template spacings
+  NetView net[2];            // learned form, per narrowphase launch
+  int nshapes;
   // Neighbour lists (exact, optional): *reuse is set non-zero when a particle moved
   // more than sqrt(move2) from its position at the last list build; the cell sort and
   // the list rebuild run only then. The step's kick clears it.
@@ -235,11 +259,13 @@ void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long s
 cudaError_t mlp_train_step(float* params, const float4* samples, int nshapes, int S, int B, long long it,
                            float* partial, float* loss, float* m1, float* m2, float lr, int step, cudaStream_t st);
 void mlp_pack(const float* params, int nshapes, MlpInfer* out, cudaStream_t st);
+// fail (device int): set to 1 when a tensor-core wait gave up (results not valid)
 void mlp_validate(const MlpShapeData& D, int nshapes, const MlpInfer* inf, int S2, unsigned long long seed,
-                  const float* delta, unsigned* err_bits, cudaStream_t st);
+                  const float* delta, unsigned* err_bits, int* fail, cudaStream_t st);
 cudaError_t mlp_grad_once(const float* params, const float4* pts, int n, float* partial, float* loss, cudaStream_t st);
 void mlp_forward(const float* params, const float4* pts, int n, float* y, cudaStream_t st);
-void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, cudaStream_t st);
+void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, int* fail,
+               cudaStream_t st);
 
 void launch_integrate_first(const StepArgs& a, cudaStream_t s);
 void launch_candidates(const StepArgs& a, cudaStream_t s);

@@ -1,5 +1,6 @@
 // Learned per-shape SDF: training data, forward/backward/Adam training kernels,
-// inference tables and the validation pass that measures each network's error.
+// inference tables and the validation pass that measures each network's error
+// (with the tensor-core inference code of mlp.cuh, the code the narrowphase uses).
 //
 // Training data of shape s: points of the template's grid box, half uniform and
 // half near the surface (a surface node moved by a normal-distributed offset of
@@ -197,23 +198,20 @@ __global__ void k_mlp_adam(float* params, float* m1, float* m2, const float* __r
   params[at] -= lr * mh / (sqrtf(vh) + eps);
 }
 
-// Inference tables from the FP32 weights (one block per shape).
+// Inference tables from the FP32 weights (one block per shape): W2 in BF16 in the
+// swizzled B-operand layout, layer-1 rows with their bias, b2, w3, b3.
 __global__ void k_mlp_pack(const float* __restrict__ params, MlpInfer* out) {
   const int s = blockIdx.x;
   const float* P = params + (size_t)s * MLP_NP;
   MlpInfer& M = out[s];
-  for (int k = threadIdx.x; k < 256; k += blockDim.x) {
-    const int nt = k >> 5, lane = k & 31, g = lane >> 2, t = lane & 3, n = nt * 8 + g;
-    unsigned v = 0u;
-    if (t == 0) v = pack_bf16x2(P[MLP_W1 + 3 * n], P[MLP_W1 + 3 * n + 1]);
-    if (t == 1) v = pack_bf16x2(P[MLP_W1 + 3 * n + 2], P[MLP_B1 + n]);
-    M.w1b[k] = v;
-  }
-  for (int k = threadIdx.x; k < 64 * 72; k += blockDim.x) {
-    const int j = k / 72, i = k % 72;
-    M.w2[k] = __float2bfloat16_rn(i < 64 ? P[MLP_W2 + 64 * j + i] : 0.f);
+  for (int k = threadIdx.x; k < 512; k += blockDim.x) {
+    const int n = k >> 3, c = k & 7;  // output unit n, inputs 8c .. 8c + 7
+    const float* w = P + MLP_W2 + 64 * n + 8 * c;
+    M.w2[n * 8 + (c ^ (n & 7))] = make_uint4(pack_bf16x2(w[0], w[1]), pack_bf16x2(w[2], w[3]),
+                                             pack_bf16x2(w[4], w[5]), pack_bf16x2(w[6], w[7]));
   }
   for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+    M.w1[k] = make_float4(P[MLP_W1 + 3 * k], P[MLP_W1 + 3 * k + 1], P[MLP_W1 + 3 * k + 2], P[MLP_B1 + k]);
     M.b2[k] = P[MLP_B2 + k];
     M.w3[k] = P[MLP_W3 + k];
   }
@@ -230,16 +228,14 @@ __global__ void k_mlp_pack(const float* __restrict__ params, MlpInfer* out) {
 // phi_net - phi_grid over the points with phi_grid <= delta[s] (the one-sided
 // bound that makes a rejection by the network safe). Float bits of running
 // maxima of non-negative values (which order as integers).
-__global__ void __launch_bounds__(128) k_mlp_validate(MlpShapeData D, const MlpInfer* __restrict__ inf, int S2,
-                                                      unsigned long long seed, const float* __restrict__ delta,
-                                                      unsigned* err_bits) {
-  __shared__ __align__(16) __nv_bfloat16 sw2[4][64 * 72];
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_validate(MlpShapeData D, const MlpInfer* __restrict__ inf, int S2,
+                                                           unsigned long long seed, const float* __restrict__ delta,
+                                                           unsigned* err_bits, int* fail) {
+  extern __shared__ unsigned char dyn[];
+  MlpTcSmem* T = mlp_tc_smem(dyn);
+  mlp_tc_setup(T);
   const int s = blockIdx.y;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const MlpInfer& M = inf[s];
-  mlp_stage_w2(M, sw2[warp]);
-  unsigned w1b[8];
-  for (int nt = 0; nt < 8; ++nt) w1b[nt] = M.w1b[nt * 32 + lane];
+  mlp_tc_stage(T, inf[s], s);
   const MlpNorm nm = D.norm[s];
   const int3 gs = D.gsize[s];
   const double3 o = D.origin[s];
@@ -248,8 +244,9 @@ __global__ void __launch_bounds__(128) k_mlp_validate(MlpShapeData D, const MlpI
   const long long total = ngrid + S2;
   const float dlt = delta[s];
   float emax = 0.f, ein = 0.f;
-  for (long long k0 = ((long long)blockIdx.x * 4 + warp) * 32; k0 < total; k0 += (long long)gridDim.x * 128) {
-    const long long k = k0 + lane;
+  bool ok = true;
+  for (long long k0 = (long long)blockIdx.x * MLP_TILE; k0 < total && ok; k0 += (long long)gridDim.x * MLP_TILE) {
+    const long long k = k0 + threadIdx.x;
     double3 p = o;
     double phi = 0.0;
     const bool act = k < total;
@@ -270,21 +267,24 @@ __global__ void __launch_bounds__(128) k_mlp_validate(MlpShapeData D, const MlpI
     } else if (act) {
       phi = D.sdf[D.sdf_off[s]];  // no nodes: the grid's first node again
     }
-    const float ux = (float)((p.x - nm.cx) / nm.R), uy = (float)((p.y - nm.cy) / nm.R), uz = (float)((p.z - nm.cz) / nm.R);
-    const float net = mlp_eval_warp(M, w1b, sw2[warp], ux, uy, uz) * nm.R;
-    if (act) {
+    mlp_tc_layer1(T, (float)((p.x - nm.cx) / nm.R), (float)((p.y - nm.cy) / nm.R), (float)((p.z - nm.cz) / nm.R));
+    ok = mlp_tc_mma(T);
+    const float net = mlp_tc_output(T) * nm.R;
+    if (act && ok) {
       emax = fmaxf(emax, fabsf(net - (float)phi));
       if (phi <= (double)dlt) ein = fmaxf(ein, net - (float)phi);
     }
   }
+  if (!ok && threadIdx.x == 0) atomicExch(fail, 1);
   for (int off = 16; off > 0; off >>= 1) {
     emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, off));
     ein = fmaxf(ein, __shfl_xor_sync(0xffffffffu, ein, off));
   }
-  if (lane == 0) {
+  if ((threadIdx.x & 31) == 0) {
     atomicMax(&err_bits[2 * s], __float_as_uint(emax));
     atomicMax(&err_bits[2 * s + 1], __float_as_uint(ein));
   }
+  mlp_tc_teardown(T, ok);
 }
 
 // Forward pass of the FP32 master weights over n points (the gradient check and
@@ -307,20 +307,23 @@ __global__ void k_mlp_forward(const float* __restrict__ P, const float4* __restr
 
 // Network of the narrowphase at n points (template-frame units): phi for each,
 // through the inference code (the ablation and the consistency checks).
-__global__ void __launch_bounds__(128) k_mlp_infer(const MlpInfer* __restrict__ inf, MlpNorm nm, const double3* pts, int n,
-                                                   float* phi) {
-  __shared__ __align__(16) __nv_bfloat16 sw2[4][64 * 72];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  mlp_stage_w2(*inf, sw2[warp]);
-  unsigned w1b[8];
-  for (int nt = 0; nt < 8; ++nt) w1b[nt] = inf->w1b[nt * 32 + lane];
-  for (int k0 = (blockIdx.x * 4 + warp) * 32; k0 < n; k0 += gridDim.x * 128) {
-    const int k = k0 + lane;
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_infer(const MlpInfer* __restrict__ inf, MlpNorm nm, const double3* pts,
+                                                        int n, float* phi, int* fail) {
+  extern __shared__ unsigned char dyn[];
+  MlpTcSmem* T = mlp_tc_smem(dyn);
+  mlp_tc_setup(T);
+  mlp_tc_stage(T, *inf, 0);
+  bool ok = true;
+  for (int k0 = blockIdx.x * MLP_TILE; k0 < n && ok; k0 += gridDim.x * MLP_TILE) {
+    const int k = k0 + threadIdx.x;
     const double3 p = k < n ? pts[k] : make_double3(nm.cx, nm.cy, nm.cz);
-    const float v = mlp_eval_warp(*inf, w1b, sw2[warp], (float)((p.x - nm.cx) / nm.R), (float)((p.y - nm.cy) / nm.R),
-                                  (float)((p.z - nm.cz) / nm.R));
-    if (k < n) phi[k] = v * nm.R;
+    mlp_tc_layer1(T, (float)((p.x - nm.cx) / nm.R), (float)((p.y - nm.cy) / nm.R), (float)((p.z - nm.cz) / nm.R));
+    ok = mlp_tc_mma(T);
+    const float v = mlp_tc_output(T);
+    if (k < n) phi[k] = ok ? v * nm.R : __int_as_float(0x7fc00000);
   }
+  if (!ok && threadIdx.x == 0) atomicExch(fail, 1);
+  mlp_tc_teardown(T, ok);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,9 +352,19 @@ void mlp_pack(const float* params, int nshapes, MlpInfer* out, cudaStream_t st) 
   k_mlp_pack<<<nshapes, 256, 0, st>>>(params, out);
 }
 
+// The inference kernels' dynamic shared memory (above the 48 KB default only with the attribute).
+static void mlp_tc_attr() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_mlp_validate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_TC_SMEM);
+  cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_TC_SMEM);
+  done = true;
+}
+
 void mlp_validate(const MlpShapeData& D, int nshapes, const MlpInfer* inf, int S2, unsigned long long seed,
-                  const float* delta, unsigned* err_bits, cudaStream_t st) {
-  k_mlp_validate<<<dim3(148, nshapes), 128, 0, st>>>(D, inf, S2, seed, delta, err_bits);
+                  const float* delta, unsigned* err_bits, int* fail, cudaStream_t st) {
+  mlp_tc_attr();
+  k_mlp_validate<<<dim3(148, nshapes), MLP_TILE, MLP_TC_SMEM, st>>>(D, inf, S2, seed, delta, err_bits, fail);
 }
 
 cudaError_t mlp_grad_once(const float* params, const float4* pts, int n, float* partial, float* loss, cudaStream_t st) {
@@ -370,8 +383,11 @@ void mlp_forward(const float* params, const float4* pts, int n, float* y, cudaSt
   if (n > 0) k_mlp_forward<<<(n + 127) / 128, 128, 0, st>>>(params, pts, n, y);
 }
 
-void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, cudaStream_t st) {
-  if (n > 0) k_mlp_infer<<<(n + 127) / 128, 128, 0, st>>>(inf, nm, pts, n, phi);
+void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, int* fail,
+               cudaStream_t st) {
+  mlp_tc_attr();
+  const int tiles = (n + MLP_TILE - 1) / MLP_TILE;
+  if (n > 0) k_mlp_infer<<<tiles < 1184 ? tiles : 1184, MLP_TILE, MLP_TC_SMEM, st>>>(inf, nm, pts, n, phi, fail);
 }
 
 }  // namespace lsdem

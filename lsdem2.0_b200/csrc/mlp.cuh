@@ -2,12 +2,18 @@
 //
 // Input: the point in the template frame (template units) normalised by the
 // shape's centre c and radius R, u = (p - c) / R; output phi / R. Training
-// (mlp.cu) keeps FP32 master weights; inference runs 32 points per warp on the
-// tensor cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation) with the
-// bias of layer 1 folded in as a fourth input column, the layer-1 accumulators
-// reused in registers as layer-2 A fragments, and SiLU evaluated in packed BF16
-// (x/2 (1 + tanh(x/2)) with tanh.approx.bf16x2). Every use of the network in the
-// narrowphase is bounded by the error measured with this same inference code.
+// (mlp.cu) keeps FP32 master weights. Inference runs 128 points per CTA tile on
+// the 5th-generation tensor cores:
+//   layer 1 (3 -> 64) and its SiLU on the CUDA cores, one thread per point, the
+//     activations rounded to BF16 and stored as the A operand in shared memory
+//     (K-major, 128-byte swizzle);
+//   layer 2 (64 -> 64) as one 128 x 64 x 64 tcgen05.mma (kind::f16, BF16
+//     operands, FP32 accumulators in tensor memory), issued by one thread, its
+//     completion signalled through an mbarrier by tcgen05.commit;
+//   bias, SiLU and the output dot product (64 -> 1) read back from tensor memory
+//     with tcgen05.ld, each warp its own 32 lanes (= its 32 points).
+// SiLU is x/2 (1 + tanh(x/2)) in packed BF16 (tanh.approx.bf16x2). Every use of
+// the network is bounded by the error measured with this same code.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -25,14 +31,15 @@ enum : int {
   MLP_NP = 4484    // stride (16-byte multiple)
 };
 
-// Inference tables of one shape, built from the FP32 weights.
-//  w1b[nt * 32 + lane]: the layer-1 B fragment (bf16x2) of n-tile nt for lane
-//    (rows 2t, 2t+1 of [W1^T; b1^T; 0] at column 8 nt + g, g = lane / 4, t = lane % 4);
-//  w2[64][72]: W2 in BF16, row = output unit, 72-element rows (ldmatrix, no bank
-//    conflicts); b2 and w3 in FP32; b3.
+// Inference tables of one shape, built from the FP32 weights (k_mlp_pack).
+//  w2: W2 in BF16 as the tensor core's B operand (N = 64 output units x K = 64
+//    inputs, K-major, 128-byte swizzle): row n holds the 64 inputs of output unit
+//    n (128 bytes); its 16-byte chunk c is stored at chunk c ^ (n % 8). Copied
+//    as is to a 1024-byte-aligned shared-memory tile.
+//  w1: (W1 row j, b1[j]); b2, w3 in FP32; b3.
 struct MlpInfer {
-  unsigned w1b[256];
-  __nv_bfloat16 w2[64 * 72];
+  uint4 w2[512];
+  float4 w1[64];
   float b2[64];
   float w3[64];
   float b3;
@@ -45,8 +52,28 @@ struct MlpNorm {
   float err;             // max |phi_net - phi_grid| over the validation points
   float err_in;          // max phi_net - phi_grid where phi_grid <= delta
   float delta;           // trust band: 2 % of the shape's size
-  float pad;
+  float r_over_h;        // R / template grid spacing (phi / R -> phi / spacing)
 };
+
+// Points per tensor-core tile (= threads of an inference CTA) and TMEM columns.
+constexpr int MLP_TILE = 128;
+constexpr int MLP_TMEM_COLS = 64;
+// Shared memory of one inference CTA: A tile (16 KB) and B tile (8 KB), both
+// 1024-byte aligned, layer-1/3 constants, mbarrier and the TMEM address; plus
+// 1024 bytes of alignment slack in the dynamic allocation.
+struct MlpTcSmem {
+  uint4 a[MLP_TILE * 8];   // 128 rows x 128 B
+  uint4 b[512];            // 64 rows x 128 B
+  float4 w1[64];
+  float b2[64];
+  float w3[64];
+  float b3;
+  unsigned tmem;
+  unsigned long long mbar;
+  int staged;              // shape whose weights are in b / w1 / b2 / w3 (-1: none)
+  int phase;               // parity of the next mbarrier completion
+};
+constexpr size_t MLP_TC_SMEM = sizeof(MlpTcSmem) + 1024;
 
 #ifdef __CUDACC__
 
@@ -65,110 +92,162 @@ __device__ __forceinline__ unsigned silu_bf16x2(unsigned x) {
   return r;
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// The aligned shared-memory block of an inference CTA inside the dynamic allocation.
+__device__ __forceinline__ MlpTcSmem* mlp_tc_smem(unsigned char* dyn) {
+  const unsigned a = smem_u32(dyn);
+  return reinterpret_cast<MlpTcSmem*>(dyn + ((1024u - (a & 1023u)) & 1023u));
 }
 
-__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const void* smem_row) {
-  const unsigned addr = (unsigned)__cvta_generic_to_shared(smem_row);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(addr));
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile whose 8-row
+// groups are 1024 bytes apart (start address and stride in 16-byte units, version 1,
+// layout type 2 = 128-byte swizzle).
+__device__ __forceinline__ unsigned long long mlp_desc(unsigned saddr) {
+  const unsigned long long start = (saddr & 0x3FFFFu) >> 4;
+  const unsigned long long lbo = 1ull, sbo = 1024ull >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
 }
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major,
+// N = 64, M = 128.
+constexpr unsigned MLP_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
-// Copies one shape's W2 (64 x 72 BF16) into this warp's shared staging area.
-__device__ __forceinline__ void mlp_stage_w2(const MlpInfer& M, __nv_bfloat16* sw2) {
-  const int lane = threadIdx.x & 31;
-  const uint4* src = reinterpret_cast<const uint4*>(M.w2);
-  uint4* dst = reinterpret_cast<uint4*>(sw2);
-  for (int k = lane; k < 64 * 72 / 8; k += 32) dst[k] = src[k];
-  __syncwarp();
-}
-
-// phi / R of the network at this lane's point u (all 32 lanes call it; the
-// result of an inactive lane is meaningless). sw2: this warp's staged W2.
-// w1b: this lane's 8 layer-1 B fragments (M.w1b[nt * 32 + lane]).
-__device__ __forceinline__ float mlp_eval_warp(const MlpInfer& M, const unsigned (&w1b)[8],
-                                               const __nv_bfloat16* sw2, float ux, float uy, float uz) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  // layer-1 A fragments: rows = points, columns (u.x, u.y, u.z, 1, 0 ...)
-  unsigned a1[2][4];
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int r0 = mt * 16 + g, r1 = r0 + 8;
-    const float x0 = __shfl_sync(0xffffffffu, ux, r0), y0 = __shfl_sync(0xffffffffu, uy, r0);
-    const float z0 = __shfl_sync(0xffffffffu, uz, r0);
-    const float x1 = __shfl_sync(0xffffffffu, ux, r1), y1 = __shfl_sync(0xffffffffu, uy, r1);
-    const float z1 = __shfl_sync(0xffffffffu, uz, r1);
-    a1[mt][0] = t == 0 ? pack_bf16x2(x0, y0) : (t == 1 ? pack_bf16x2(z0, 1.f) : 0u);
-    a1[mt][1] = t == 0 ? pack_bf16x2(x1, y1) : (t == 1 ? pack_bf16x2(z1, 1.f) : 0u);
-    a1[mt][2] = 0u;
-    a1[mt][3] = 0u;
+// One warp allocates the CTA's tensor-memory columns; thread 0 sets up the mbarrier.
+__device__ __forceinline__ void mlp_tc_setup(MlpTcSmem* S) {
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S->tmem)),
+                 "r"(MLP_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // layer 1 (+ SiLU) straight into the layer-2 A fragments: the accumulators of
-  // n-tiles 2k and 2k+1 are the A fragment of k-step k
-  unsigned a2[2][4][4];
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S->mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    S->staged = -1;
+    S->phase = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+}
+
+// Releases the tensor memory. ok = false (a wait gave up): first waits once more, again
+// bounded, for the outstanding MMA before the columns are freed.
+__device__ __forceinline__ void mlp_tc_teardown(MlpTcSmem* S, bool ok = true) {
+  if (!ok) {
+    const unsigned mb = smem_u32(&S->mbar), par = (unsigned)S->phase;
+    unsigned done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it)
+      asm volatile(
+          "{\n\t.reg .pred q;\n\tmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+          : "=r"(done)
+          : "r"(mb), "r"(par));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S->tmem), "r"(MLP_TMEM_COLS));
+}
+
+// Copies one shape's inference tables into the CTA's tiles (all threads).
+__device__ __forceinline__ void mlp_tc_stage(MlpTcSmem* S, const MlpInfer& M, int shape) {
+  __syncthreads();  // the previous tile's MMA has completed and every thread has read it
+  for (int k = threadIdx.x; k < 512; k += blockDim.x) S->b[k] = __ldg(&M.w2[k]);
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+    S->w1[k] = __ldg(&M.w1[k]);
+    S->b2[k] = __ldg(&M.b2[k]);
+    S->w3[k] = __ldg(&M.w3[k]);
+  }
+  if (threadIdx.x == 0) {
+    S->b3 = __ldg(&M.b3);
+    S->staged = shape;
+  }
+  asm volatile("fence.proxy.async.shared::cta;");
+  __syncthreads();
+}
+
+// Layer 1 of this thread's point (row threadIdx.x of the tile) into the A tile:
+// 64 hidden units in FP32, SiLU in BF16, 8 chunks of 8 units, swizzled.
+__device__ __forceinline__ void mlp_tc_layer1(MlpTcSmem* S, float ux, float uy, float uz) {
+  const int r = threadIdx.x;
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int c = 0; c < 8; ++c) {
+    unsigned w[4];
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      float d[4] = {0.f, 0.f, 0.f, 0.f};
-      mma_bf16(d, a1[mt], w1b[nt], 0u);
-      const int ks = nt >> 1, hi = nt & 1;
-      a2[mt][ks][hi * 2 + 0] = silu_bf16x2(pack_bf16x2(d[0], d[1]));
-      a2[mt][ks][hi * 2 + 1] = silu_bf16x2(pack_bf16x2(d[2], d[3]));
+    for (int q = 0; q < 4; ++q) {
+      const float4 a = S->w1[8 * c + 2 * q], b = S->w1[8 * c + 2 * q + 1];
+      const float h0 = fmaf(a.x, ux, fmaf(a.y, uy, fmaf(a.z, uz, a.w)));
+      const float h1 = fmaf(b.x, ux, fmaf(b.y, uy, fmaf(b.z, uz, b.w)));
+      w[q] = silu_bf16x2(pack_bf16x2(h0, h1));
     }
-  // layer 2 + SiLU + output layer, accumulated per row
-  float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    S->a[r * 8 + (c ^ (r & 7))] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Layer 2 of the tile: makes the A tile visible to the tensor core, thread 0 issues
+// the four K = 16 steps of the 128 x 64 x 64 MMA and commits them to the mbarrier,
+// and every thread waits for the completion (bounded). Returns false when the wait
+// gave up (the accumulators are then not valid; the caller sets its error flag).
+__device__ __forceinline__ bool mlp_tc_mma(MlpTcSmem* S) {
+  asm volatile("fence.proxy.async.shared::cta;");
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const unsigned a0 = smem_u32(S->a), b0 = smem_u32(S->b);
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    // B fragments of the 4 k-steps: rows nt*8 .. +7 of W2 (outputs), 16 inputs each
-    unsigned b[8];
-    {
-      const int row = nt * 8 + (lane & 7);
-      const int col = (lane >> 3) * 8;  // lanes 0-7: k 0-7, 8-15: k 8-15, 16-23: k 16-23, 24-31: k 24-31
-      unsigned r[4];
-      ldmatrix_x4(r, sw2 + row * 72 + col);
-      b[0] = r[0]; b[1] = r[1]; b[2] = r[2]; b[3] = r[3];
-      ldmatrix_x4(r, sw2 + row * 72 + 32 + col);
-      b[4] = r[0]; b[5] = r[1]; b[6] = r[2]; b[7] = r[3];
+    for (int k = 0; k < 4; ++k) {
+      const unsigned long long da = mlp_desc(a0 + 32 * k), db = mlp_desc(b0 + 32 * k);
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(S->tmem),
+          "l"(da), "l"(db), "r"(MLP_IDESC), "r"(k));
     }
-    const int c0 = nt * 8 + 2 * t;
-    const float bb0 = M.b2[c0], bb1 = M.b2[c0 + 1], w0 = M.w3[c0], w1 = M.w3[c0 + 1];
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        smem_u32(&S->mbar)));
+  }
+  const unsigned mb = smem_u32(&S->mbar);
+  const unsigned par = (unsigned)S->phase;
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 22) && !done; ++it) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(done)
+        : "r"(mb), "r"(par));
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const bool all = __syncthreads_and(done) != 0;
+  if (threadIdx.x == 0 && all) S->phase ^= 1;  // a wait that gave up keeps the parity it waits for
+  __syncthreads();
+  return all;
+}
+
+// Read-back of this thread's row: bias, SiLU and the output dot product; then the
+// tile is released for the next one (every thread's loads have completed).
+__device__ __forceinline__ float mlp_tc_output(MlpTcSmem* S) {
+  const unsigned warp = threadIdx.x >> 5;
+  const unsigned taddr = S->tmem + ((warp * 32u) << 16);
+  float y = S->b3;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-      float d[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int q = 0; q < 4; ++q) {
+    unsigned v[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr + 16u * q));
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-      for (int ks = 0; ks < 4; ++ks) {
-        const unsigned a[4] = {a2[mt][ks][0], a2[mt][ks][1], a2[mt][ks][2], a2[mt][ks][3]};
-        mma_bf16(d, a, b[2 * ks], b[2 * ks + 1]);
-      }
-      const unsigned s0 = silu_bf16x2(pack_bf16x2(d[0] + bb0, d[1] + bb1));
-      const unsigned s1 = silu_bf16x2(pack_bf16x2(d[2] + bb0, d[3] + bb1));
-      const __nv_bfloat162 v0 = *reinterpret_cast<const __nv_bfloat162*>(&s0);
-      const __nv_bfloat162 v1 = *reinterpret_cast<const __nv_bfloat162*>(&s1);
-      y[mt][0] = fmaf(w0, __low2float(v0), fmaf(w1, __high2float(v0), y[mt][0]));
-      y[mt][1] = fmaf(w0, __low2float(v1), fmaf(w1, __high2float(v1), y[mt][1]));
+    for (int j = 0; j < 16; j += 2) {
+      const int n = 16 * q + j;
+      const unsigned s = silu_bf16x2(pack_bf16x2(__uint_as_float(v[j]) + S->b2[n], __uint_as_float(v[j + 1]) + S->b2[n + 1]));
+      const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&s);
+      y = fmaf(S->w3[n], __low2float(h), fmaf(S->w3[n + 1], __high2float(h), y));
     }
   }
-  // row sums over the 4 lanes of a group, then to the lane that owns the row
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 1);
-      y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 2);
-    }
-  const int mt = lane >> 4, rr = lane & 15, src = (rr & 7) * 4, h = rr >> 3;
-  const float v00 = __shfl_sync(0xffffffffu, y[0][0], src), v01 = __shfl_sync(0xffffffffu, y[0][1], src);
-  const float v10 = __shfl_sync(0xffffffffu, y[1][0], src), v11 = __shfl_sync(0xffffffffu, y[1][1], src);
-  const float v = mt == 0 ? (h == 0 ? v00 : v01) : (h == 0 ? v10 : v11);
-  return v + M.b3;
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  return y;
 }
 
 #endif  // __CUDACC__

@@ -269,7 +269,7 @@ void build_clusters(ShapeHost& s) {
 }
 
 struct BodyHost {
-  std::vector<double> pos, vel, angvel, quat, invm, invI, radius, kn, ks, mu, res, scale, origin, invh;
+  std::vector<double> pos, vel, angvel, quat, force, torque, invm, invI, radius, kn, ks, mu, res, scale, origin, invh;
   std::vector<int> shape;
   std::vector<long long> node_base;
   int n() const { return (int)shape.size(); }
@@ -368,6 +368,16 @@ struct lsdem_solver {
   bool mlp_trained = false, mlp_on = false;
   DArr<int4> mb_pair;
   long long mb_cap = 0, mb_pcap = 0;
+  // learned form: network queues and pending nodes, per narrowphase launch
+  struct NetDev {
+    DArr<float4> row, pend_g;
+    DArr<int> cnt, pend_n, ctr;
+    DArr<unsigned char> pend_v;
+    DArr<int4> pair;
+    int qcap = 0, pcap = 0, paircap = 0;
+  } net[2];
+  long long cap_netq = 0, cap_pend = 0;  // rows per shape, pending nodes per launch (0: not sized yet)
+  bool net_dirty = true;                 // the buffers must be (re)allocated before the next step
   std::vector<int> h_node_off, h_cl_off;
   GridP pg{}, wg{};
   DArr<int> cell_idx, cell_start, cell_end, sorted_key;
@@ -426,6 +436,13 @@ struct lsdem_solver {
   DArr<double3> bk_cspring;
   int bk_cap[3] = {0, 0, 0};
   long long hist_count = 0;  // contacts in the history buffer hp
+  // host copies of the device state: stale after steps until pulled (pull_host); the
+  // body and node counts the device arrays were built for
+  bool host_stale = false;
+  int dev_np = -1, dev_nw = -1;
+  long long dev_nodes = -1;
+  int dev_nsets = -1;
+  size_t dev_nb = 0;
   bool grow_contacts = false;
   long long steps = 0, reruns = 0, launches = 0;
   double time = 0.0;
@@ -529,6 +546,8 @@ void push_body(lsdem_solver* s, BodyHost& B, int shape, double scale, const doub
     B.vel.push_back(vel ? vel[a] : 0.);
     B.angvel.push_back(angvel ? angvel[a] : 0.);
     B.origin.push_back(scale == 1.0 ? sh.origin[a] : scale * sh.origin[a]);
+    B.force.push_back(0.);
+    B.torque.push_back(0.);
   }
   double q[4];
   qnormalize(quat, q);
@@ -596,6 +615,39 @@ void alloc_contacts(lsdem_solver* s, ContactsDev& c, long long cap) {
   c.geom = false;
 }
 
+// Learned form: the network queues (rows per shape), the pending nodes and the pair
+// records of both narrowphase launches. Per-step scratch: contents are not kept.
+void alloc_net(lsdem_solver* s) {
+  const int n = std::max(s->P.n(), 1);
+  const int ns = std::max((int)s->shapes.size(), 1);
+  if (s->cap_pend <= 0) s->cap_pend = std::max<long long>(1 << 20, (long long)n * 8);
+  if (s->cap_netq <= 0) s->cap_netq = std::max<long long>(1 << 14, s->cap_pend / ns * 2);
+  s->cap_pend = std::min<long long>(s->cap_pend, 0x7fffffffLL);
+  s->cap_netq = std::min<long long>(s->cap_netq, 0x7fffffffLL / ns);
+  for (int l = 0; l < 2; ++l) {
+    auto& N = s->net[l];
+    const long long pairs = l == 0 ? (long long)n * (s->slots[0][0].cap + s->slots[0][1].cap)
+                                   : (long long)n * s->slots[0][2].cap;
+    if (l == 1 && s->nsets == 0) {
+      N.qcap = N.pcap = N.paircap = 0;
+      N.row.release(); N.pend_g.release(); N.cnt.release(); N.pend_n.release(); N.ctr.release();
+      N.pend_v.release(); N.pair.release();
+      continue;
+    }
+    N.qcap = (int)s->cap_netq;
+    N.pcap = (int)s->cap_pend;
+    N.paircap = (int)std::min<long long>(std::max<long long>(pairs, 1), 0x7fffffffLL);
+    CK(N.row.alloc((size_t)ns * N.qcap));
+    CK(N.cnt.alloc(ns)); CK(N.cnt.zero(s->stream));
+    CK(N.pend_g.alloc(N.pcap));
+    CK(N.pend_n.alloc(N.pcap));
+    CK(N.pend_v.alloc(N.pcap));
+    CK(N.pair.alloc(N.paircap));
+    CK(N.ctr.alloc(2)); CK(N.ctr.zero(s->stream));
+  }
+  s->net_dirty = false;
+}
+
 // Scratch of the precision form, sized with the contact capacity.
 void alloc_maybe(lsdem_solver* s) {
   if (s->precision == PREC_FP64) return;
@@ -626,8 +678,10 @@ void upload_bodies(lsdem_solver* s, BodyHost& H, BodyDev& D) {
   CK(D.pos.upload((const double3*)H.pos.data(), n, st));
   CK(D.vel.upload((const double3*)H.vel.data(), n, st));
   CK(D.angvel.upload((const double3*)H.angvel.data(), n, st));
-  CK(D.force.alloc(n)); CK(D.force.zero(st));
-  CK(D.torque.alloc(n)); CK(D.torque.zero(st));
+  // forces of the last step (zero before the first): the first half kick of a new
+  // phase uses them, as the reference's upload of its host copy does (LSParticle.h:700-710)
+  CK(D.force.upload((const double3*)H.force.data(), n, st));
+  CK(D.torque.upload((const double3*)H.torque.data(), n, st));
   CK(D.origin.upload((const double3*)H.origin.data(), n, st));
   CK(D.quat.upload((const Quat*)H.quat.data(), n, st));
   CK(D.invm.upload(H.invm.data(), n, st));
@@ -644,6 +698,35 @@ void upload_bodies(lsdem_solver* s, BodyHost& H, BodyDev& D) {
   if (!H.node_base.empty()) CK(D.node_base.upload(H.node_base.data(), n, st));
   if (&D == &s->dP && s->precision != PREC_FP64) CK(D.rotm.alloc(3 * std::max<size_t>(n, 1)));
   else D.rotm.release();
+}
+
+// Brings the host copies of the bodies' state up to date with the device after steps:
+// particle position, velocity, angular velocity, orientation, force and torque, wall
+// position and orientation, bond flags and state (the reference downloads them at every
+// output, LSSolver.h:625-635, so that its host-side edits and the next phase's upload start
+// from the last step). Called before every host-side read or edit of that state.
+void pull_host(lsdem_solver* s) {
+  if (!s->host_stale) return;
+  cudaStream_t st = s->stream;
+  const size_t n = (size_t)std::min(s->dev_np, s->P.n()), nw = (size_t)std::min(s->dev_nw, s->W.n());
+  auto dl = [&](std::vector<double>& h, const void* d, size_t bytes) {
+    if (bytes) CK(cudaMemcpyAsync(h.data(), d, bytes, cudaMemcpyDeviceToHost, st));
+  };
+  dl(s->P.pos, s->dP.pos.p, 24 * n);
+  dl(s->P.vel, s->dP.vel.p, 24 * n);
+  dl(s->P.angvel, s->dP.angvel.p, 24 * n);
+  dl(s->P.quat, s->dP.quat.p, 32 * n);
+  dl(s->P.force, s->dP.force.p, 24 * n);
+  dl(s->P.torque, s->dP.torque.p, 24 * n);
+  dl(s->W.pos, s->dW.pos.p, 24 * nw);
+  dl(s->W.quat, s->dW.quat.p, 32 * nw);
+  const size_t nb = std::min(s->dev_nb, s->bonds.bonded.size());
+  if (nb) {
+    CK(cudaMemcpyAsync(s->bonds.bonded.data(), s->b_bonded.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(s->bonds.state.data(), s->b_state.p, sizeof(double) * 9 * nb, cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  s->host_stale = false;
 }
 
 void set_grid(GridP& g, const double* mn, const double* mx_in, double cell) {  // spatialGrid::set
@@ -684,7 +767,27 @@ void alloc_bucket(lsdem_solver* s, int n, int ncells, bool second = false) {
   CK(t.alloc((size_t)std::max(n, 1)));
 }
 
+void backup_history(lsdem_solver* s);
+void restore_history(lsdem_solver* s, int hp0);
+
 void initialize(lsdem_solver* s) {
+  // A new phase of the same bodies keeps the contact history of the last step, as the
+  // reference keeps its contact arrays when their size is unchanged (SolidInteraction.h:24-27,
+  // PeriodicBoundary.h:23-39): saved here, put back after the buffers are rebuilt.
+  pull_host(s);
+  long long nodes_now = 0;
+  for (int i = 0; i < s->P.n(); ++i) nodes_now += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3);
+  int nsets_now = 0;
+  {
+    const int ax = s->periodic & 7;
+    for (int m = 1; m < 8; ++m)
+      if ((m & ax) == m) ++nsets_now;
+    if (s->periodic & 8) nsets_now = 3;
+  }
+  const bool carry = s->hist_count > 0 && s->dev_np == s->P.n() && s->dev_nw == s->W.n() &&
+                     s->dev_nodes == nodes_now && s->dev_nsets == nsets_now;
+  const long long carried = carry ? s->hist_count : 0;
+  if (carry) backup_history(s);
   CK(cudaSetDevice(s->device));
   cudaStream_t st = s->stream;
   // shapes
@@ -938,6 +1041,26 @@ void initialize(lsdem_solver* s) {
   alloc_maybe(s);
   s->hp = 0;
   s->hist_count = 0;
+  if (carry) {
+    if (carried > s->con[0].cap) {
+      s->cap_c = std::max<long long>(s->cap_c, carried + carried / 2);
+      alloc_contacts(s, s->con[0], s->cap_c);
+      alloc_contacts(s, s->con[1], s->cap_c);
+      alloc_maybe(s);
+    }
+    s->hist_count = carried;
+    restore_history(s, 0);
+    const int c32 = (int)carried;
+    CK(cudaMemcpyAsync(s->con[0].count.p, &c32, sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    s->force_reuse = true;
+  }
+  s->net_dirty = true;
+  s->dev_np = s->P.n();
+  s->dev_nw = s->W.n();
+  s->dev_nodes = nodes_now;
+  s->dev_nsets = s->nsets;
+  s->dev_nb = s->bonds.bonded.size();
   // bonds
   const size_t nbnd = s->bonds.bonded.size();
   if (nbnd) {
@@ -1041,6 +1164,16 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.mlp_inf = learned ? s->mlp_inf.p : nullptr;
   a.mlp_norm = s->mlp_norm.p;
   a.mlp_band = s->mlp_band.p;
+  a.nshapes = (int)s->shapes.size();
+  for (int l = 0; l < 2; ++l) {
+    auto& N = s->net[l];
+    NetView& v = a.net[l];
+    v = NetView{};
+    if (!learned || !N.ctr.p) continue;
+    v.row = N.row.p; v.cnt = N.cnt.p; v.qcap = N.qcap;
+    v.pend_g = N.pend_g.p; v.pend_n = N.pend_n.p; v.pend_v = N.pend_v.p; v.pcap = N.pcap;
+    v.pair = N.pair.p; v.paircap = N.paircap; v.ctr = N.ctr.p;
+  }
   return a;
 }
 
@@ -1180,7 +1313,14 @@ void step_once(lsdem_solver* s, double dt, bool record, lsdem_hook hook, void* u
 }
 
 // Snapshot of everything a batch may change, taken at the batch start.
+void backup_state(lsdem_solver* s);
 void backup(lsdem_solver* s) {
+  backup_state(s);
+  backup_history(s);
+}
+
+// Body state and bond flags (what one step changes besides the new contact list).
+void backup_state(lsdem_solver* s) {
   cudaStream_t st = s->stream;
   const size_t n = (size_t)s->P.n(), nw = (size_t)s->W.n();
   // backup buffers grow geometrically (never per batch: a free synchronises the device)
@@ -1192,6 +1332,17 @@ void backup(lsdem_solver* s) {
   cp(s->bk_quat, s->dP.quat, n); cp(s->bk_force, s->dP.force, n); cp(s->bk_torque, s->dP.torque, n);
   cp(s->bk_wpos, s->dW.pos, nw); cp(s->bk_wquat, s->dW.quat, nw);
   cp(s->bk_bonded, s->b_bonded, s->bonds.bonded.size());
+}
+
+// The contact history of the last step (candidate slots with their contact segments,
+// contact nodes and springs) into the backup buffers.
+void backup_history(lsdem_solver* s) {
+  cudaStream_t st = s->stream;
+  const size_t n = (size_t)s->P.n();
+  auto cp = [&](auto& dst, auto& src, size_t m) {
+    if (dst.n < m) CK(dst.alloc(std::max(m + m / 2, (size_t)1024)));
+    if (m) CK(cudaMemcpyAsync(dst.p, src.p, m * sizeof(*src.p), cudaMemcpyDeviceToDevice, st));
+  };
   for (int k = 0; k < 3; ++k) {
     SlotsDev& sl = s->slots[s->hp][k];
     s->bk_cap[k] = sl.cap;
@@ -1206,7 +1357,13 @@ void backup(lsdem_solver* s) {
   cp(s->bk_cspring, s->con[s->hp].spring, nc);
 }
 
+void restore_state(lsdem_solver* s, int hp0);
 void restore(lsdem_solver* s, int hp0) {
+  restore_state(s, hp0);
+  restore_history(s, hp0);
+}
+
+void restore_state(lsdem_solver* s, int hp0) {
   s->force_reuse = true;
   cudaStream_t st = s->stream;
   s->hp = hp0;
@@ -1218,6 +1375,16 @@ void restore(lsdem_solver* s, int hp0) {
   cp(s->dP.quat, s->bk_quat, n); cp(s->dP.force, s->bk_force, n); cp(s->dP.torque, s->bk_torque, n);
   cp(s->dW.pos, s->bk_wpos, nw); cp(s->dW.quat, s->bk_wquat, nw);
   cp(s->b_bonded, s->bk_bonded, s->bonds.bonded.size());
+}
+
+// The backed-up contact history into the buffers of parity hp0 (capacities may have
+// grown since the backup: slots are copied row by row).
+void restore_history(lsdem_solver* s, int hp0) {
+  cudaStream_t st = s->stream;
+  const size_t n = (size_t)s->P.n();
+  auto cp = [&](auto& dst, auto& src, size_t m) {
+    if (m) CK(cudaMemcpyAsync(dst.p, src.p, m * sizeof(*src.p), cudaMemcpyDeviceToDevice, st));
+  };
   for (int k = 0; k < 3; ++k) {
     SlotsDev& sl = s->slots[hp0][k];
     if (!sl.cnt.p) continue;
@@ -1261,6 +1428,24 @@ bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
     changed = true;
     s->grow_contacts = true;
   }
+  if (changed) s->net_dirty = true;  // pair records are sized with the candidate slots
+  // learned form: network rows per shape and pending nodes
+  auto up64 = [&](long long& cap, long long need) {
+    if (need * 5 > cap * 4) {
+      cap = std::max<long long>(cap * 2, need + need / 2 + 1024);
+      changed = true;
+      s->net_dirty = true;
+    }
+  };
+  if (s->net[0].ctr.p) {
+    up64(s->cap_netq, st.need_netq);
+    up64(s->cap_pend, st.need_pend);
+    if ((st.flags & OVF_NET) && !s->net_dirty) {  // overflowed without a recorded demand: double both
+      s->cap_netq *= 2;
+      s->cap_pend *= 2;
+      s->net_dirty = changed = true;
+    }
+  }
   return changed;
 }
 
@@ -1269,6 +1454,7 @@ bool plan_growth(lsdem_solver* s, const Status& st, long long last_contacts) {
 void grow(lsdem_solver* s) {
   ++s->graph_gen;
   s->force_reuse = true;
+  if (s->net_dirty && s->net[0].ctr.p) alloc_net(s);
   if (s->grow_nbr) {
     CK(s->nbr.alloc((size_t)std::max(s->P.n(), 1) * s->nbr_cap));
     s->grow_nbr = false;
@@ -1300,7 +1486,7 @@ cudaEvent_t step_start(lsdem_solver* s) {
 // cannot be captured) the graph runs on a private blocking stream: the legacy stream
 // and blocking streams are ordered with each other both ways, so the copies, events
 // and app kernels on the legacy stream keep their order around the step.
-static void step_graph(lsdem_solver* s, double dt, lsdem_hook hook, void* user, double t) {
+static void step_graph_pre(lsdem_solver* s, double dt) {
   const int hp = s->hp;
   uint64_t key = 1469598103934665603ull;
   auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
@@ -1311,6 +1497,7 @@ static void step_graph(lsdem_solver* s, double dt, lsdem_hook hook, void* user, 
   mix((uint64_t)s->flags); mix((uint64_t)s->mb_cap); mix((uint64_t)s->mb_pcap);
   mix((uint64_t)s->cap_pp); mix((uint64_t)s->cap_w); mix((uint64_t)s->cap_g); mix((uint64_t)s->cap_c);
   mix((uint64_t)s->mlp_on); mix((uint64_t)(s->scr_stats.p != nullptr)); mix((uint64_t)s->periodic);
+  mix((uint64_t)s->cap_netq); mix((uint64_t)s->cap_pend); mix((uint64_t)(uintptr_t)s->net[0].row.p);
   if (!s->stream && !s->gstream) CK(cudaStreamCreate(&s->gstream));
   cudaStream_t gs = s->stream ? s->stream : s->gstream;
   lsdem_solver::StepGraph& G = s->sgraph[hp];
@@ -1342,13 +1529,85 @@ static void step_graph(lsdem_solver* s, double dt, lsdem_hook hook, void* user, 
   }
   CK(cudaGraphLaunch(G.exec, gs));
   s->launches += G.launches;
+}
+
+static void step_graph(lsdem_solver* s, double dt, lsdem_hook hook, void* user, double t) {
+  step_graph_pre(s, dt);
   if (hook) hook(user, t);
   step_post(s, dt);
+}
+
+// Steps with an external-force hook: each step's capacity status is read before its hook
+// runs (one host synchronisation per step, as the reference's per-step count reads), and a
+// step that overflowed is re-run with grown capacities first, so the hook runs exactly once
+// per step, after the step's complete contact and bond forces (LSSolver.h:1000-1011).
+static int run_steps_hooked(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
+  cudaStream_t st = s->stream;
+  for (long long k = 0; k < nsteps; ++k) {
+    const bool rec = s->record && (k == nsteps - 1);
+    const int hp0 = s->hp;
+    cudaEvent_t ea = s->step_timing ? step_start(s) : nullptr;
+    // the step leaves the history of parity hp0 untouched until step_post: only the body
+    // state is saved per step, the history only before a re-allocation
+    backup_state(s);
+    Status stat{};
+    for (int attempt = 0;; ++attempt) {
+      CK(cudaMemsetAsync(s->status.p, 0, sizeof(Status), st));
+      if (s->force_reuse && s->reuse.p) {  // sort and rebuild in this step
+        CK(cudaMemsetAsync(s->reuse.p, 0xff, sizeof(int), st));
+        s->force_reuse = false;
+      }
+      if (s->graphs && !rec && !s->profiling && s->P.n() > 0) step_graph_pre(s, dt);
+      else step_pre(s, dt, rec);
+      // this step's contacts are in the buffer of the other parity until step_post
+      CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(Status), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(s->h_count, s->con[1 - s->hp].count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      stat = *s->h_status;
+      if (stat.errors) throw Fail{LSDEM_ERR_CUDA, "a tensor-core wait in the network pass gave up"};
+      resolve_profile(s, stat.flags == 0);  // every pending event has completed
+      if (stat.flags == 0) break;
+      if (attempt > 8) throw Fail{LSDEM_ERR_NOMEM, "capacity growth did not converge"};
+      plan_growth(s, stat, *s->h_count);
+      backup_history(s);
+      grow(s);
+      restore(s, hp0);
+      s->reruns++;
+    }
+    const long long count = *s->h_count;
+    hook(user, s->time);
+    step_post(s, dt);
+    if (ea) {
+      cudaEvent_t eb = pool_event(s);
+      CK(cudaEventRecord(eb, st));
+      s->prof_pending.push_back({9, {ea, eb}});  // resolved after the next synchronisation
+    }
+    s->hist_count = count;
+    s->steps += 1;
+    s->time += dt;
+    s->builds += stat.builds;
+    if (plan_growth(s, stat, s->hist_count)) {
+      const int hp1 = s->hp;
+      backup(s);
+      grow(s);
+      restore(s, hp1);
+    }
+  }
+  CK(cudaStreamSynchronize(st));
+  resolve_profile(s, true);
+  s->host_stale = true;
+  return LSDEM_OK;
 }
 
 int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, void* user) {
   if (!s->ready) throw Fail{LSDEM_ERR_STATE, "lsdem_step before lsdem_initialize"};
   if (!(dt > 0.)) throw Fail{LSDEM_ERR_ARG, "Invalid timeStep"};
+  const bool learned = s->mlp_on && s->mlp_trained && s->precision != PREC_FP64;
+  if (learned && (s->net_dirty || !s->net[0].ctr.p)) {
+    alloc_net(s);
+    ++s->graph_gen;
+  }
+  if (hook) return run_steps_hooked(s, dt, nsteps, hook, user);
   cudaStream_t st = s->stream;
   long long done = 0;
   while (done < nsteps) {
@@ -1384,6 +1643,7 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
       CK(cudaMemcpyAsync(s->h_count, s->con[s->hp].count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       stat = *s->h_status;
+      if (stat.errors) throw Fail{LSDEM_ERR_CUDA, "a tensor-core wait in the network pass gave up"};
       resolve_profile(s, stat.flags == 0);
       if (stat.flags == 0) {
         s->hist_count = *s->h_count;
@@ -1410,6 +1670,7 @@ int run_steps(lsdem_solver* s, double dt, long long nsteps, lsdem_hook hook, voi
       s->cur_batch = std::min(s->batch, s->cur_batch * 2);
     }
   }
+  s->host_stale = true;
   return LSDEM_OK;
 }
 
@@ -1505,6 +1766,7 @@ int lsdem_add_particles(lsdem_solver* s, int n, const int* shape, const double* 
   if (!s || n < 0 || !shape || !pos || !quat || !inv_mass || !kn || !ks || !mu || !e)
     return fail(s, LSDEM_ERR_ARG, "null argument");
   return guard(s, [&] {
+    pull_host(s);
     for (int i = 0; i < n; ++i)
       if (shape[i] < 0 || shape[i] >= (int)s->shapes.size()) throw Fail{LSDEM_ERR_ARG, "unknown shape id"};
     if (first_index) *first_index = s->P.n();
@@ -1526,6 +1788,7 @@ int lsdem_add_ls_particle(lsdem_solver* s, const double* nodes, int n_nodes, con
                           double density, int* index) {
   if (!s || !sdf || !size3 || !origin3 || !pos || !quat) return fail(s, LSDEM_ERR_ARG, "null argument");
   return guard(s, [&] {
+    pull_host(s);
     if (size3[0] < 2 || size3[1] < 2 || size3[2] < 2) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid size"};
     if (!(spacing > 0.)) throw Fail{LSDEM_ERR_ARG, "Invalid level-set grid spacing"};
     double mp[16];
@@ -1555,6 +1818,7 @@ int lsdem_add_wall(lsdem_solver* s, const double* verts, int n_verts, const doub
   if (!s || !sdf || !size3 || !origin3 || !pos || !quat || (n_verts > 0 && !verts))
     return fail(s, LSDEM_ERR_ARG, "null argument");
   return guard(s, [&] {
+    pull_host(s);
     // walls keep their vertices as nodes (LSSolver.h:255-271); only the radius uses them
     const int sh = add_shape_impl(s, verts, 0, sdf, size3, origin3, spacing);
     double r = 0.;
@@ -1570,6 +1834,7 @@ int lsdem_add_wall(lsdem_solver* s, const double* verts, int n_verts, const doub
 static int set_vec(lsdem_solver* s, std::vector<double>& v, int n, int index, const double* x, bool add) {
   if (!s || !x) return LSDEM_ERR_ARG;
   if (index < 0 || index >= n) return LSDEM_OK;  // reference: silently ignored
+  if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
   for (int a = 0; a < 3; ++a) v[3 * (size_t)index + a] = add ? v[3 * (size_t)index + a] + x[a] : x[a];
   s->ready = false;
   return LSDEM_OK;
@@ -1625,6 +1890,7 @@ int lsdem_add_bond(lsdem_solver* s, int master, int slave, const double* point3,
                    double initial_length, double youngs, double poisson, double tensile, double cohesion, double mu) {
   if (!s || !point3 || !normal3) return LSDEM_ERR_ARG;
   if (master >= s->P.n() || slave >= s->P.n() || master < 0 || slave < 0) return LSDEM_OK;  // reference: ignored
+  if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
   return add_bond_impl(s, master, slave, &s->P.pos[3 * (size_t)master], &s->P.quat[4 * (size_t)master],
                        &s->P.pos[3 * (size_t)slave], &s->P.quat[4 * (size_t)slave], point3, normal3, radius,
                        initial_length, youngs, poisson, tensile, cohesion, mu);
@@ -1663,6 +1929,7 @@ int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samp
       nm.cy = (float)(sh.origin[1] + 0.5 * (sh.size[1] - 1) * sh.h);
       nm.cz = (float)(sh.origin[2] + 0.5 * (sh.size[2] - 1) * sh.h);
       nm.R = (float)(0.5 * ext);
+      nm.r_over_h = (float)(0.5 * ext / sh.h);
       org[k] = make_double3(sh.origin[0], sh.origin[1], sh.origin[2]);
       hh[k] = sh.h;
     }
@@ -1716,9 +1983,14 @@ int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samp
     DArr<float> ddelta;
     CK(ddelta.upload(delta.data(), ns, st));
     CK(s->mlp_err.alloc(2 * (size_t)ns)); CK(s->mlp_err.zero(st));
-    mlp_validate(D, ns, s->mlp_inf.p, samples, seed ^ 0x5eedf00dull, ddelta.p, s->mlp_err.p, st);
+    DArr<int> dfail;
+    CK(dfail.alloc(1)); CK(dfail.zero(st));
+    mlp_validate(D, ns, s->mlp_inf.p, samples, seed ^ 0x5eedf00dull, ddelta.p, s->mlp_err.p, dfail.p, st);
+    CK(cudaGetLastError());
     std::vector<unsigned> eb = dl(s->mlp_err, 2 * (size_t)ns, st);
+    std::vector<int> hf = dl(dfail, 1, st);
     CK(cudaStreamSynchronize(st));
+    if (hf[0]) throw Fail{LSDEM_ERR_CUDA, "tensor-core wait gave up in the network validation"};
     s->h_mlp_band.assign(ns, 0.f);
     for (int k = 0; k < ns; ++k) {
       float e, ein;
@@ -1775,10 +2047,14 @@ int lsdem_mlp_eval(lsdem_solver* s, int shape, int n, const double* pts, float* 
     DArr<float> dphi;
     CK(dp.upload((const double3*)pts, (size_t)n, s->stream));
     CK(dphi.alloc((size_t)std::max(n, 1)));
-    mlp_infer(s->mlp_inf.p + shape, s->h_mlp_norm[shape], dp.p, n, dphi.p, s->stream);
+    DArr<int> dfail;
+    CK(dfail.alloc(1)); CK(dfail.zero(s->stream));
+    mlp_infer(s->mlp_inf.p + shape, s->h_mlp_norm[shape], dp.p, n, dphi.p, dfail.p, s->stream);
     CK(cudaGetLastError());
     if (n) CK(cudaMemcpyAsync(phi, dphi.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<int> hf = dl(dfail, 1, s->stream);
     CK(cudaStreamSynchronize(s->stream));
+    if (hf[0]) throw Fail{LSDEM_ERR_CUDA, "tensor-core wait gave up in the network evaluation"};
     return LSDEM_OK;
   });
 }
@@ -1869,6 +2145,7 @@ int lsdem_initialize(lsdem_solver* s, const double* min3, const double* max3, co
   }
   ++s->vtu_layout;
   ++s->graph_gen;
+  s->time = 0.0;  // each phase starts at time 0, as the reference's compute loop (LSSolver.h:994-996)
   return guard(s, [&] {
     initialize(s);
     return LSDEM_OK;
@@ -1908,13 +2185,14 @@ int lsdem_get_state(lsdem_solver* s, double* pos, double* vel, double* angvel, d
                     double* torque) {
   if (!s) return LSDEM_ERR_ARG;
   if (!s->ready) {
+    if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
     const size_t n = (size_t)s->P.n();
     if (pos) std::memcpy(pos, s->P.pos.data(), 24 * n);
     if (vel) std::memcpy(vel, s->P.vel.data(), 24 * n);
     if (angvel) std::memcpy(angvel, s->P.angvel.data(), 24 * n);
     if (quat) std::memcpy(quat, s->P.quat.data(), 32 * n);
-    if (force) std::memset(force, 0, 24 * n);
-    if (torque) std::memset(torque, 0, 24 * n);
+    if (force) std::memcpy(force, s->P.force.data(), 24 * n);
+    if (torque) std::memcpy(torque, s->P.torque.data(), 24 * n);
     return LSDEM_OK;
   }
   return guard(s, [&] {
@@ -1935,6 +2213,7 @@ int lsdem_get_wall_state(lsdem_solver* s, double* pos, double* vel, double* angv
   if (!s) return LSDEM_ERR_ARG;
   const size_t n = (size_t)s->W.n();
   if (!s->ready) {
+    if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
     if (pos) std::memcpy(pos, s->W.pos.data(), 24 * n);
     if (vel) std::memcpy(vel, s->W.vel.data(), 24 * n);
     if (angvel) std::memcpy(angvel, s->W.angvel.data(), 24 * n);
@@ -1956,6 +2235,7 @@ int lsdem_set_state(lsdem_solver* s, const double* pos, const double* vel, const
   if (!s) return LSDEM_ERR_ARG;
   const size_t n = (size_t)s->P.n();
   if (!s->ready) {
+    if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
     if (pos) std::memcpy(s->P.pos.data(), pos, 24 * n);
     if (vel) std::memcpy(s->P.vel.data(), vel, 24 * n);
     if (angvel) std::memcpy(s->P.angvel.data(), angvel, 24 * n);
@@ -1969,6 +2249,7 @@ int lsdem_set_state(lsdem_solver* s, const double* pos, const double* vel, const
     if (angvel && n) CK(cudaMemcpyAsync(s->dP.angvel.p, angvel, 24 * n, cudaMemcpyHostToDevice, st));
     if (quat && n) CK(cudaMemcpyAsync(s->dP.quat.p, quat, 32 * n, cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
+    s->host_stale = true;
     return LSDEM_OK;
   });
 }
@@ -2161,6 +2442,7 @@ int lsdem_get_bonds(lsdem_solver* s, int* ids2, int* bonded, double* state9) {
   const size_t nb = s->bonds.bonded.size();
   if (ids2) std::memcpy(ids2, s->bonds.ids.data(), 8 * nb);
   if (!s->ready || nb == 0) {
+    if (const int rc = guard(s, [&] { pull_host(s); return LSDEM_OK; })) return rc;
     if (bonded) std::memcpy(bonded, s->bonds.bonded.data(), 4 * nb);
     if (state9) std::memcpy(state9, s->bonds.state.data(), 72 * nb);
     return LSDEM_OK;
@@ -2463,6 +2745,178 @@ int lsdem_pack_rsa(int n, const double* radius, const double* lo, const double* 
     if (!placed) return LSDEM_ERR_ARG;
   }
   return LSDEM_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Snapshots: the dynamic state of a running solver in one binary file (no counterpart
+// in the reference, whose host mirrors are written only as VTU frames). Layout, little
+// endian: "LSDEMSNP", u32 version 1; i32 particles, walls, image sets, 0; i64 surface
+// nodes, bonds, steps; f64 time; particles: position, velocity, angular velocity (3 f64
+// each), orientation (4), force, torque (3); walls: position, velocity, angular velocity
+// (3), orientation (4); bonds: flag (i32), state (9 f64); contact history: i64 contacts,
+// per partner kind (particles, walls, images) i32 slot capacity and, when > 0, i32 per
+// particle slot count, then per particle and slot partner id, segment start and segment
+// length (i32); per contact i32 node and 3 f64 spring.
+
+}  // extern "C"
+
+namespace {
+struct SnapIO {
+  FILE* f;
+  bool ok = true;
+  void w(const void* p, size_t b) { if (b && std::fwrite(p, 1, b, f) != b) ok = false; }
+  void r(void* p, size_t b) { if (b && std::fread(p, 1, b, f) != b) ok = false; }
+};
+constexpr char kSnapMagic[8] = {'L', 'S', 'D', 'E', 'M', 'S', 'N', 'P'};
+
+template <class T>
+void snap_dl(SnapIO& io, const DArr<T>& d, size_t n, cudaStream_t st) {
+  std::vector<T> h(n);
+  if (n) CK(cudaMemcpyAsync(h.data(), d.p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  io.w(h.data(), n * sizeof(T));
+}
+template <class T>
+void snap_ul(SnapIO& io, DArr<T>& d, size_t n, cudaStream_t st) {
+  std::vector<T> h(n);
+  io.r(h.data(), n * sizeof(T));
+  if (!io.ok) throw Fail{LSDEM_ERR_ARG, "snapshot file truncated"};
+  if (n) CK(cudaMemcpyAsync(d.p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+}
+}  // namespace
+
+extern "C" {
+
+int lsdem_snapshot_save(lsdem_solver* s, const char* path) {
+  if (!s || !path) return LSDEM_ERR_ARG;
+  if (!s->ready) return fail(s, LSDEM_ERR_STATE, "lsdem_snapshot_save before lsdem_initialize");
+  return guard(s, [&] {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) throw Fail{LSDEM_ERR_ARG, std::string("cannot open ") + path};
+    SnapIO io{f};
+    cudaStream_t st = s->stream;
+    CK(cudaStreamSynchronize(st));
+    const int np = s->P.n(), nw = s->W.n();
+    const uint32_t ver = 1;
+    const int32_t hdr[4] = {np, nw, s->nsets, 0};
+    const long long nb = (long long)s->bonds.bonded.size();
+    const long long h64[3] = {s->dev_nodes, nb, s->steps};
+    io.w(kSnapMagic, 8); io.w(&ver, 4); io.w(hdr, 16); io.w(h64, 24); io.w(&s->time, 8);
+    snap_dl(io, s->dP.pos, np, st); snap_dl(io, s->dP.vel, np, st); snap_dl(io, s->dP.angvel, np, st);
+    snap_dl(io, s->dP.quat, np, st); snap_dl(io, s->dP.force, np, st); snap_dl(io, s->dP.torque, np, st);
+    snap_dl(io, s->dW.pos, nw, st); snap_dl(io, s->dW.vel, nw, st); snap_dl(io, s->dW.angvel, nw, st);
+    snap_dl(io, s->dW.quat, nw, st);
+    snap_dl(io, s->b_bonded, (size_t)nb, st); snap_dl(io, s->b_state, (size_t)nb * 9, st);
+    io.w(&s->hist_count, 8);
+    for (int k = 0; k < 3; ++k) {
+      SlotsDev& sl = s->slots[s->hp][k];
+      const int32_t cap = sl.cnt.p ? sl.cap : 0;
+      io.w(&cap, 4);
+      if (cap <= 0) continue;
+      const size_t m = (size_t)np * cap;
+      snap_dl(io, sl.cnt, np, st); snap_dl(io, sl.id, m, st); snap_dl(io, sl.seg_start, m, st);
+      snap_dl(io, sl.seg_cnt, m, st);
+    }
+    snap_dl(io, s->con[s->hp].node, (size_t)s->hist_count, st);
+    snap_dl(io, s->con[s->hp].spring, (size_t)s->hist_count, st);
+    const bool ok = io.ok;
+    if (std::fclose(f) != 0 || !ok) throw Fail{LSDEM_ERR_ARG, std::string("cannot write ") + path};
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_snapshot_load(lsdem_solver* s, const char* path) {
+  if (!s || !path) return LSDEM_ERR_ARG;
+  if (!s->ready) return fail(s, LSDEM_ERR_STATE, "lsdem_snapshot_load before lsdem_initialize");
+  return guard(s, [&] {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) throw Fail{LSDEM_ERR_ARG, std::string("cannot open ") + path};
+    struct Closer { FILE* f; ~Closer() { std::fclose(f); } } closer{f};
+    SnapIO io{f};
+    cudaStream_t st = s->stream;
+    char magic[8];
+    uint32_t ver = 0;
+    int32_t hdr[4];
+    long long h64[3];
+    double t = 0.;
+    io.r(magic, 8); io.r(&ver, 4); io.r(hdr, 16); io.r(h64, 24); io.r(&t, 8);
+    if (!io.ok || std::memcmp(magic, kSnapMagic, 8) != 0 || ver != 1) throw Fail{LSDEM_ERR_ARG, "not a snapshot file"};
+    const int np = s->P.n(), nw = s->W.n();
+    const long long nb = (long long)s->bonds.bonded.size();
+    if (hdr[0] != np || hdr[1] != nw || hdr[2] != s->nsets || h64[0] != s->dev_nodes || h64[1] != nb)
+      throw Fail{LSDEM_ERR_ARG, "snapshot does not match the solver's bodies, nodes, bonds or image sets"};
+    CK(cudaStreamSynchronize(st));
+    snap_ul(io, s->dP.pos, np, st); snap_ul(io, s->dP.vel, np, st); snap_ul(io, s->dP.angvel, np, st);
+    snap_ul(io, s->dP.quat, np, st); snap_ul(io, s->dP.force, np, st); snap_ul(io, s->dP.torque, np, st);
+    snap_ul(io, s->dW.pos, nw, st); snap_ul(io, s->dW.vel, nw, st); snap_ul(io, s->dW.angvel, nw, st);
+    snap_ul(io, s->dW.quat, nw, st);
+    snap_ul(io, s->b_bonded, (size_t)nb, st); snap_ul(io, s->b_state, (size_t)nb * 9, st);
+    // walls' prescribed velocities are host settings too
+    if (nw) {
+      CK(cudaMemcpy(s->W.vel.data(), s->dW.vel.p, 24 * (size_t)nw, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(s->W.angvel.data(), s->dW.angvel.p, 24 * (size_t)nw, cudaMemcpyDeviceToHost));
+    }
+    long long hc = 0;
+    io.r(&hc, 8);
+    int32_t caps[3] = {0, 0, 0};
+    std::vector<std::vector<int>> slot_data[3];
+    for (int k = 0; k < 3; ++k) {
+      io.r(&caps[k], 4);
+      if (!io.ok || caps[k] < 0) throw Fail{LSDEM_ERR_ARG, "snapshot file truncated"};
+      if (caps[k] == 0) continue;
+      const size_t m = (size_t)np * caps[k];
+      slot_data[k].resize(4);
+      slot_data[k][0].resize(np);
+      for (int a = 1; a < 4; ++a) slot_data[k][a].resize(m);
+      io.r(slot_data[k][0].data(), 4 * (size_t)np);
+      for (int a = 1; a < 4; ++a) io.r(slot_data[k][a].data(), 4 * m);
+    }
+    std::vector<int> node((size_t)hc);
+    std::vector<double3> spring((size_t)hc);
+    io.r(node.data(), 4 * (size_t)hc);
+    io.r(spring.data(), 24 * (size_t)hc);
+    if (!io.ok) throw Fail{LSDEM_ERR_ARG, "snapshot file truncated"};
+    // capacities at least those of the file
+    bool realloc = false;
+    int* capv[3] = {&s->cap_pp, &s->cap_w, &s->cap_g};
+    for (int k = 0; k < 3; ++k)
+      if (caps[k] > *capv[k]) { *capv[k] = caps[k]; realloc = true; }
+    if (realloc) alloc_slots(s);
+    if (hc > s->con[0].cap) {
+      s->cap_c = std::max<long long>(s->cap_c, hc + hc / 2);
+      alloc_contacts(s, s->con[0], s->cap_c);
+      alloc_contacts(s, s->con[1], s->cap_c);
+      alloc_maybe(s);
+    }
+    for (int k = 0; k < 3; ++k) {
+      SlotsDev& sl = s->slots[s->hp][k];
+      if (!sl.cnt.p) continue;
+      CK(cudaMemset(sl.cnt.p, 0, 4 * (size_t)std::max(np, 1)));
+      if (caps[k] == 0 || np == 0) continue;
+      CK(cudaMemcpy(sl.cnt.p, slot_data[k][0].data(), 4 * (size_t)np, cudaMemcpyHostToDevice));
+      for (int a = 1; a < 4; ++a) {
+        DArr<int>& dst = a == 1 ? sl.id : (a == 2 ? sl.seg_start : sl.seg_cnt);
+        CK(cudaMemcpy2D(dst.p, sizeof(int) * sl.cap, slot_data[k][a].data(), sizeof(int) * caps[k],
+                        sizeof(int) * caps[k], np, cudaMemcpyHostToDevice));
+      }
+    }
+    if (hc) {
+      CK(cudaMemcpy(s->con[s->hp].node.p, node.data(), 4 * (size_t)hc, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(s->con[s->hp].spring.p, spring.data(), 24 * (size_t)hc, cudaMemcpyHostToDevice));
+    }
+    const int c32 = (int)hc;
+    CK(cudaMemcpy(s->con[s->hp].count.p, &c32, sizeof(int), cudaMemcpyHostToDevice));
+    s->con[s->hp].geom = false;
+    s->hist_count = hc;
+    s->time = t;
+    s->steps = h64[2];
+    s->host_stale = true;
+    s->force_reuse = true;
+    ++s->graph_gen;
+    return LSDEM_OK;
+  });
 }
 
 }  // extern "C"

@@ -59,6 +59,11 @@ __global__ void k_integrate_first(StepArgs a) {
     if (a.G.count) *a.G.count = 0;
     if (a.mb.ctr) a.mb.ctr[0] = a.mb.ctr[1] = a.mb.ctr[2] = 0;
     if (a.pl.ctr) a.pl.ctr[0] = a.pl.ctr[1] = a.pl.ctr[2] = 0;
+    for (int l = 0; l < 2; ++l)
+      if (a.net[l].ctr) {
+        a.net[l].ctr[0] = a.net[l].ctr[1] = 0;
+        for (int k = 0; k < a.nshapes; ++k) a.net[l].cnt[k] = 0;
+      }
   }
   if (i < a.P.n) {
     const BodyView& P = a.P;
@@ -1144,16 +1149,20 @@ LD float2 unpack16(unsigned w) {
   return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
 template <int SDFK>
-LD float phi16(const PairF& F, float gx, float gy, float gz) {
+LD float phi16_at(const uint4* cells, int sy, int sz, float gx, float gy, float gz) {
   const int i0 = __float2int_rd(gx), j0 = __float2int_rd(gy), k0 = __float2int_rd(gz);
   const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
-  const uint4 w = __ldg(F.cells + (k0 * F.sz + j0 * F.sy + i0));
+  const uint4 w = __ldg(cells + (k0 * sz + j0 * sy + i0));
   const float2 c01 = unpack16<SDFK>(w.x), c23 = unpack16<SDFK>(w.y);
   const float2 c45 = unpack16<SDFK>(w.z), c67 = unpack16<SDFK>(w.w);
   const float x0 = fmaf(fx, c01.y - c01.x, c01.x), x1 = fmaf(fx, c23.y - c23.x, c23.x);
   const float x2 = fmaf(fx, c45.y - c45.x, c45.x), x3 = fmaf(fx, c67.y - c67.x, c67.x);
   const float y0 = fmaf(fy, x1 - x0, x0), y1 = fmaf(fy, x3 - x2, x2);
   return fmaf(fz, y1 - y0, y0);
+}
+template <int SDFK>
+LD float phi16(const PairF& F, float gx, float gy, float gz) {
+  return phi16_at<SDFK>(F.cells, F.sy, F.sz, gx, gy, gz);
 }
 
 // Cell-window admission of walls and images from the FP32 world node offset ra
@@ -1247,8 +1256,7 @@ LD int partner_shape(const StepArgs& a, int pid) {
 // k_contacts_f; a pair without such nodes gets its empty contact segment here.
 template <int KIND, int SDFK, bool LRN>
 LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* s_cl, unsigned short* s_sub,
-                      unsigned* s_mask,
-                      unsigned (&cnt)[8], __nv_bfloat16* sw2, int& staged) {
+                      unsigned* s_mask, unsigned (&cnt)[8]) {
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous pair's write pass may still read s_cl / s_mask
   const int shA = a.P.shape[A];
@@ -1302,41 +1310,87 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   };
   int total = 0;
   if (LRN) {
-    if (nch > 0 && staged != F.pshape) {  // this warp's copy of the partner network's W2
-      mlp_stage_w2(a.mlp_inf[F.pshape], sw2);
-      staged = F.pshape;
-    }
-    const MlpInfer& M = a.mlp_inf[F.pshape];
-    unsigned w1b[8];
-    if (nch > 0)
-      for (int nt = 0; nt < 8; ++nt) w1b[nt] = M.w1b[nt * 32 + lane];
+    // Learned form: every node the partner's bounds cannot reject goes to the network of
+    // the partner's shape (k_net_screen, tensor cores), which decides with the grid
+    // test of the nodes it keeps; here the nodes awaiting that verdict are recorded in
+    // node order for the pair (k_net_compact queues the survivors for the FP64 pass).
+    const NetView& Q = a.net[li];
     for (int k = 0; k < nch; ++k) {
       const int ni = node_of(k);
       cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
-      const float4 nd = __ldg(a.S.node_pos_f + n0 + min(ni, nn - 1));
-      const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
-      bool adm;
-      if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
-      else adm = window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) != 0;
-      const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
-      const float lo = fminf(gx, fminf(gy, gz));
-      const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
-      const bool need = ni < nn && adm && !(lo < -F.eg || hi >= F.eg);
-      const bool edge = lo < F.eg || hi >= -F.eg;
-      bool may = false;
-      if (__any_sync(FULL, need)) {
-        // the network for the chunk (tensor cores); nodes it cannot reject go to the grid screen
-        const float y = mlp_eval_warp(M, w1b, sw2, fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y),
-                                      fmaf(l.z, F.ms, -F.mc.z));
-        const bool keep = need && !(y * F.mtoh > F.Tn);
-        cnt[6] += __popc(__ballot_sync(FULL, need));
-        cnt[3] += __popc(__ballot_sync(FULL, keep && !edge));
-        may = keep && (edge || !(phi16<SDFK>(F, gx, gy, gz) > F.T));
+      bool need = false;
+      if (ni < nn) {
+        const float4 nd = __ldg(a.S.node_pos_f + n0 + ni);
+        const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
+        bool adm;
+        if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
+        else adm = window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) != 0;
+        const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+        const float lo = fminf(gx, fminf(gy, gz));
+        const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+        need = adm && !(lo < -F.eg || hi >= F.eg);
       }
-      const unsigned m = __ballot_sync(FULL, may);
+      const unsigned m = __ballot_sync(FULL, need);
       if (lane == 0) s_mask[k] = m;
       total += __popc(m);
     }
+    __syncwarp();
+    const SlotView& cur = slots_of<KIND>(a, false);
+    const size_t sidx = (size_t)A * cur.cap + slot;
+    if (lane == 0) {  // set here; k_contacts_f writes the segment of a pair with contacts
+      cur.seg_start[sidx] = 0;
+      cur.seg_cnt[sidx] = 0;
+    }
+    if (total == 0) return;
+    int pstart = 0, pi = 0;
+    bool ok = false;
+    if (lane == 0) {
+      pstart = atomicAdd(&Q.ctr[0], total);
+      pi = atomicAdd(&Q.ctr[1], 1);
+      ok = pstart + total <= Q.pcap && pi < Q.paircap;
+      if (!ok) {
+        atomicOr(&a.status->flags, OVF_NET);
+        const long long need = (long long)pstart + total;
+        atomicMax(&a.status->need_pend, (int)(need < 0x7fffffff ? need : 0x7fffffff));
+      }
+    }
+    pstart = __shfl_sync(FULL, pstart, 0);
+    pi = __shfl_sync(FULL, pi, 0);
+    ok = __shfl_sync(FULL, ok, 0);
+    if (!ok) return;
+    const int sh = F.pshape;
+    int off = 0;
+    for (int k = 0; k < nch; ++k) {
+      const unsigned m = s_mask[k];
+      if (m == 0u) continue;
+      const int ni = node_of(k);
+      const float4 nd = __ldg(a.S.node_pos_f + n0 + min(ni, nn - 1));
+      const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
+      const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+      const float lo = fminf(gx, fminf(gy, gz));
+      const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+      const bool edge = lo < F.eg || hi >= -F.eg;
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&Q.cnt[sh], __popc(m));
+      base = __shfl_sync(FULL, base, 0);
+      if ((m >> lane) & 1u) {
+        const int rank = __popc(m & lanemask_lt());
+        const int idx = pstart + off + rank;
+        Q.pend_g[idx] = make_float4(gx, gy, gz, F.T);
+        Q.pend_n[idx] = ni | (edge ? (int)0x80000000u : 0);
+        const int r = base + rank;
+        if (r < Q.qcap) {
+          Q.row[(size_t)sh * Q.qcap + r] =
+              make_float4(fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y), fmaf(l.z, F.ms, -F.mc.z), __int_as_float(idx));
+        } else {
+          atomicOr(&a.status->flags, OVF_NET);
+          atomicMax(&a.status->need_netq, r + 1);
+        }
+      }
+      off += __popc(m);
+    }
+    if (lane == 0) Q.pair[pi] = make_int4(A, (KIND << 24) | slot, pstart, total);
+    return;
   } else {
     for (int k = 0; k < nch; ++k) {
       const int ni = node_of(k);
@@ -1393,16 +1447,13 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
 // One warp per listed pair: the flat pair lists of the kinds in KINDS, in
 // particle, wall, image order.
 // Particle-only screens fit 64 registers (8 blocks per SM); walls and images
-// need the window test's FP64 registers, the learned screen the network's.
+// need the window test's FP64 registers.
 template <int KINDS, int SDFK, bool LRN>
-__global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5)) k_screen_f(StepArgs a, int li) {
+__global__ void __launch_bounds__(NP_WARPS * 32, KINDS == 1 ? 8 : 5) k_screen_f(StepArgs a, int li) {
   __shared__ int s_cl[NP_WARPS][MAXCL];
   __shared__ unsigned short s_sub[NP_WARPS][4 * MAXCL];
   __shared__ unsigned s_mask[NP_WARPS][MAXCL];
-  extern __shared__ __align__(16) unsigned char s_dyn[];  // learned screen: W2 of each warp
   const int warp = threadIdx.x >> 5;
-  int staged = -1;
-  __nv_bfloat16* sw2 = reinterpret_cast<__nv_bfloat16*>(s_dyn) + (LRN ? warp * 64 * 72 : 0);
   const int n0 = (KINDS & 1) ? min(a.pl.ctr[0], a.P.n * a.pp.cap) : 0;
   const int n1 = (KINDS & 2) && a.pw.cap > 0 ? min(a.pl.ctr[1], a.P.n * a.pw.cap) : 0;
   const int n2 = (KINDS & 4) ? min(a.pl.ctr[2], a.P.n * a.pgh.cap) : 0;
@@ -1412,18 +1463,18 @@ __global__ void __launch_bounds__(NP_WARPS * 32, LRN ? 3 : (KINDS == 1 ? 8 : 5))
     if ((KINDS & 1) && e < n0) {
       const int idx = __ldg(a.pl.list[0] + e);
       const int A = idx / a.pp.cap;
-      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, __ldg(a.pp.id + idx), li, s_cl[warp], s_sub[warp], s_mask[warp],
-                                        cnt, sw2, staged);
+      screen_pair_f<KIND_PP, SDFK, LRN>(a, A, idx - A * a.pp.cap, __ldg(a.pp.id + idx), li, s_cl[warp], s_sub[warp],
+                                        s_mask[warp], cnt);
     } else if ((KINDS & 2) && e < n0 + n1) {
       const int idx = a.pl.list[1][e - n0];
       const int A = idx / a.pw.cap;
-      screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_sub[warp], s_mask[warp],
-                                          cnt, sw2, staged);
+      screen_pair_f<KIND_WALL, SDFK, LRN>(a, A, idx - A * a.pw.cap, a.pw.id[idx], li, s_cl[warp], s_sub[warp],
+                                          s_mask[warp], cnt);
     } else if (KINDS & 4) {
       const int idx = __ldg(a.pl.list[2] + e - n0 - n1);
       const int A = idx / a.pgh.cap;
       screen_pair_f<KIND_GHOST, SDFK, LRN>(a, A, idx - A * a.pgh.cap, __ldg(a.pgh.id + idx), li, s_cl[warp], s_sub[warp],
-                                           s_mask[warp], cnt, sw2, staged);
+                                           s_mask[warp], cnt);
     }
   }
   if (a.screen_stats && (threadIdx.x & 31) == 0)
@@ -1477,6 +1528,134 @@ __global__ void __launch_bounds__(NP_WARPS * 32) k_contacts_f(StepArgs a, int li
   }
 }
 
+// Learned form, the network pass of launch li: the queued nodes of each partner shape
+// in 128-row tiles on the tensor cores (mlp.cuh), one tile per CTA at a time over a
+// persistent grid. A node is kept when phi_net does not exceed the shape's network
+// threshold (trust band plus the measured one-sided error, in spacings); a kept node
+// then takes the 16-bit grid test of the plain screen (skipped within the error of the
+// grid boundary), and its verdict goes to the pair's pending list. If a tensor-core wait
+// gives up, the tile's nodes are passed on (no rejection) and the batch reports an error.
+template <int SDFK>
+__global__ void __launch_bounds__(MLP_TILE) k_net_screen(StepArgs a, int li) {
+  extern __shared__ unsigned char dyn[];
+  MlpTcSmem* T = mlp_tc_smem(dyn);
+  int* s_pre = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(T) + sizeof(MlpTcSmem));
+  const NetView& Q = a.net[li];
+  const int ns = a.nshapes;
+  if (threadIdx.x == 0) {
+    int t = 0, mx = 0;
+    for (int s = 0; s < ns; ++s) {
+      const int c = Q.cnt[s];
+      mx = max(mx, c);
+      s_pre[s] = t;
+      t += (min(c, Q.qcap) + MLP_TILE - 1) / MLP_TILE;
+    }
+    s_pre[ns] = t;
+    if (blockIdx.x == 0) {  // this step's demands, for the capacity planning
+      atomicMax(&a.status->need_netq, mx);
+      atomicMax(&a.status->need_pend, Q.ctr[0]);
+    }
+  }
+  __syncthreads();
+  const int tiles = s_pre[ns];
+  if ((int)blockIdx.x >= tiles) return;  // no tensor memory taken
+  mlp_tc_setup(T);
+  unsigned evals = 0, looks = 0;
+  bool ok = true;
+  for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+    int sh = 0;
+    while (s_pre[sh + 1] <= t) ++sh;
+    if (T->staged != sh) mlp_tc_stage(T, a.mlp_inf[sh], sh);
+    const int rows = min(Q.cnt[sh], Q.qcap);
+    const int r = (t - s_pre[sh]) * MLP_TILE + threadIdx.x;
+    const bool act = r < rows;
+    const float4 u = act ? Q.row[(size_t)sh * Q.qcap + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+    mlp_tc_layer1(T, u.x, u.y, u.z);
+    ok = mlp_tc_mma(T);
+    const float y = mlp_tc_output(T);
+    if (act) {
+      const int idx = __float_as_int(u.w);
+      unsigned char may = 1;
+      if (ok && !(y * __ldg(&a.mlp_norm[sh].r_over_h) > __ldg(&a.mlp_band[sh]))) {
+        // kept by the network: the plain screen's grid test decides
+        if (Q.pend_n[idx] >= 0) {
+          const float4 g = Q.pend_g[idx];
+          const int3 gs = a.S.gsize[sh];
+          may = !(phi16_at<SDFK>(a.S.cell16 + a.S.cell_off[sh], gs.x - 1, (gs.x - 1) * (gs.y - 1), g.x, g.y, g.z) > g.w);
+          ++looks;
+        }
+      } else if (ok) {
+        may = 0;
+      }
+      Q.pend_v[idx] = may;
+      ++evals;
+    }
+  }
+  if (!ok && threadIdx.x == 0) atomicAdd(&a.status->errors, 1);
+  if (a.screen_stats) {
+    evals = __reduce_add_sync(FULL, evals);
+    looks = __reduce_add_sync(FULL, looks);
+    if ((threadIdx.x & 31) == 0) {
+      if (evals) atomicAdd(&a.screen_stats[6], (unsigned long long)evals);
+      if (looks) atomicAdd(&a.screen_stats[3], (unsigned long long)looks);
+    }
+  }
+  mlp_tc_teardown(T, ok);
+}
+
+// Learned form, after the network pass of launch li: one warp per pair record, its
+// pending nodes with a passing verdict compacted in node order into the FP64 pass's
+// node queue, and the pair queued for k_contacts_f (the screen's tail for the plain
+// screen).
+__global__ void __launch_bounds__(NP_WARPS * 32) k_net_compact(StepArgs a, int li) {
+  __shared__ unsigned s_mask[NP_WARPS][MAXCL];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const NetView& Q = a.net[li];
+  const int np = min(Q.ctr[1], Q.paircap);
+  unsigned queued = 0;
+  for (int p = blockIdx.x * NP_WARPS + warp; p < np; p += gridDim.x * NP_WARPS) {
+    const int4 e = Q.pair[p];
+    const int nch = (e.w + 31) >> 5;
+    __syncwarp();  // the previous pair may still read s_mask
+    int total = 0;
+    for (int k = 0; k < nch; ++k) {
+      const int j = k * 32 + lane;
+      const bool may = j < e.w && Q.pend_v[e.z + j] != 0;
+      const unsigned m = __ballot_sync(FULL, may);
+      if (lane == 0) s_mask[warp][k] = m;
+      total += __popc(m);
+    }
+    __syncwarp();
+    if (total == 0) continue;
+    queued += total;
+    int start = 0;
+    bool ok = false;
+    if (lane == 0) {
+      start = atomicAdd(&a.mb.ctr[0], total);
+      const int pi = atomicAdd(&a.mb.ctr[1 + li], 1);
+      ok = start + total <= a.mb.cap && pi < a.mb.pcap;
+      if (ok) {
+        a.mb.pair[(size_t)li * a.mb.pcap + pi] = make_int4(e.x, e.y, start, total);
+      } else {
+        if (pi < a.mb.pcap) a.mb.pair[(size_t)li * a.mb.pcap + pi] = make_int4(-1, 0, 0, 0);
+        atomicOr(&a.status->flags, OVF_CONTACT);
+        const long long need = start + total > 2LL * (pi + 1) ? start + total : 2LL * (pi + 1);
+        atomicMax(&a.status->need_contact, (int)(need < 0x7fffffff ? need : 0x7fffffff));
+      }
+    }
+    start = __shfl_sync(FULL, start, 0);
+    ok = __shfl_sync(FULL, ok, 0);
+    if (!ok) continue;
+    int off = 0;
+    for (int k = 0; k < nch; ++k) {
+      const unsigned m = s_mask[warp][k];
+      if ((m >> lane) & 1u) a.mb.node[start + off + __popc(m & lanemask_lt())] = Q.pend_n[e.z + k * 32 + lane] & 0x7fffffff;
+      off += __popc(m);
+    }
+  }
+  if (a.screen_stats && lane == 0 && queued) atomicAdd(&a.screen_stats[5], (unsigned long long)queued);
+}
+
 static int g_num_sms = 0;
 static int num_sms() {
   if (g_num_sms == 0) {
@@ -1490,15 +1669,25 @@ static int num_sms() {
 
 template <int KINDS, int SDFK, bool LRN>
 void launch_screen_k(const StepArgs& a, int li, dim3 g, dim3 b, cudaStream_t s) {
-  const int dyn = LRN ? NP_WARPS * 64 * 72 * (int)sizeof(__nv_bfloat16) : 0;
-  if (LRN) {
-    static bool attr = false;  // per kernel instance
-    if (!attr) {
-      cudaFuncSetAttribute(k_screen_f<KINDS, SDFK, LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-      attr = true;
-    }
+  k_screen_f<KINDS, SDFK, LRN><<<g, b, 0, s>>>(a, li);
+}
+
+// Learned form: the network pass and the compaction after the screen of launch li.
+template <int SDFK>
+void launch_net_k(const StepArgs& a, int li, cudaStream_t s) {
+  const int smem = (int)(MLP_TC_SMEM + sizeof(int) * (a.nshapes + 1));
+  static int attr = 0;  // per kernel instance: the largest dynamic shared memory set so far
+  if (smem > attr) {
+    cudaFuncSetAttribute(k_net_screen<SDFK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = smem;
   }
-  k_screen_f<KINDS, SDFK, LRN><<<g, b, dyn, s>>>(a, li);
+  // four CTAs per SM: 4 x 64 tensor-memory columns, the other launch's pass fits beside it
+  k_net_screen<SDFK><<<num_sms() * 4, MLP_TILE, smem, s>>>(a, li);
+  k_net_compact<<<num_sms() * 16, NP_WARPS * 32, 0, s>>>(a, li);
+}
+void launch_net(const StepArgs& a, int li, cudaStream_t s) {
+  if (a.precision == PREC_FP32_FP16) launch_net_k<PREC_FP32_FP16>(a, li, s);
+  else launch_net_k<PREC_FP32_BF16>(a, li, s);
 }
 
 template <bool LRN>
@@ -1532,8 +1721,12 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   // precision form: the screen over the flat pair lists (launch_contact_pass
   // follows it); the grid is sized for the device, the list length is on it
   const int li = kinds == 4 ? 1 : 0;
-  if (a.mlp_inf) launch_screen<true>(a, kinds, li, g, b, s);
-  else launch_screen<false>(a, kinds, li, g, b, s);
+  if (a.mlp_inf) {
+    launch_screen<true>(a, kinds, li, g, b, s);
+    launch_net(a, li, s);
+  } else {
+    launch_screen<false>(a, kinds, li, g, b, s);
+  }
 }
 
 void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s) {

@@ -929,13 +929,15 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
             "solid_fraction": solid_fraction, "raw_templates": T}
 
 
-def write_c0_app_scene(path, sc, nsteps, k0, k1):
+def write_c0_app_scene(path, sc, nsteps, k0, k1, nsteps2=0, floor_wz=0.0):
     """Scene file of the config-0 app (tests/apps/c0_bench.cpp, written against the LSSolver
     API only, so the same source builds against the reference and against the drop-in):
     magic "LSDEMC0", shape (node count, grid size, spacing, origin, nodes, SDF), particles
     (count, positions, quaternions, velocities), material (kn, ks, mu, e, density), the floor
     wall (grid, spacing, origin, SDF, position, quaternion, mu, e, vertices, two triangles),
-    dt, domain, gravity, and the step count with the timed window (k0, k1]."""
+    dt, domain, gravity, and the step count with the timed window (k0, k1], counted in
+    hook calls; optionally a second phase of nsteps2 steps after the floor's angular velocity
+    about z is set to floor_wz."""
     s, f = sc["shape"], sc["floor"]
     n = len(sc["pos"])
     d = lambda a: np.ascontiguousarray(a, np.float64).tobytes()
@@ -953,6 +955,8 @@ def write_c0_app_scene(path, sc, nsteps, k0, k1):
         fh.write(i32(len(f["verts"]), len(tris)) + d(f["verts"]) + tris.tobytes())
         fh.write(d([sc["dt"]]) + d(sc["min"]) + d(sc["max"]) + d(sc["gravity"]))
         fh.write(i32(nsteps, k0, k1))
+        if nsteps2 > 0:
+            fh.write(i32(nsteps2) + d([floor_wz]))
 
 
 def read_c0_app_result(path):

@@ -115,6 +115,13 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "truncated scene file\n");
     return 2;
   }
+  // optional second phase: its step count and the floor's angular velocity about z
+  // (set between the phases with setFixedAngularVelocityToWall, as tutorial 2 does)
+  int32_t nsteps2 = 0;
+  double floor_w = 0.;
+  f.read(reinterpret_cast<char*>(&nsteps2), 4);
+  if (f) f.read(reinterpret_cast<char*>(&floor_w), 8);
+  if (!f) nsteps2 = 0;
 
   Bench s(argv[2], k0, k1);
   for (int i = 0; i < np; ++i)
@@ -126,6 +133,11 @@ int main(int argc, char** argv) {
   // numStep = floor(T / dt) + 1 and numStep + 1 steps: T = (nsteps - 1.5) dt gives nsteps steps
   s.solve(make_double3(dmin[0], dmin[1], dmin[2]), make_double3(dmax[0], dmax[1], dmax[2]),
           make_double3(g[0], g[1], g[2]), dt, (nsteps - 1.5) * dt, 1, argc, argv);
+  if (nsteps2 > 0) {
+    s.setFixedAngularVelocityToWall(0, make_double3(0., 0., floor_w));
+    s.solve(make_double3(dmin[0], dmin[1], dmin[2]), make_double3(dmax[0], dmax[1], dmax[2]),
+            make_double3(g[0], g[1], g[2]), dt, (nsteps2 - 1.5) * dt, 1, argc, argv);
+  }
   cudaDeviceSynchronize();
   float ms = -1.f;
   if (s.k_ >= k1) cudaEventElapsedTime(&ms, s.a_, s.b_);

@@ -193,3 +193,31 @@ def test_config2_bonded_same_gpu(lsdem, tmp_path):
     print(f"config 2 (bonded, {len(sc['pos'])} ellipsoids, {len(sc['bonds']['master'])} bonds), steps {k0}..{k1}: "
           f"reference build {ms0 / w0:.4f} ms/step, this solver (FP64) {ms1 / w1:.4f} ms/step, "
           f"ratio {ms0 / ms1:.2f}x, velocity difference {err:.2e} of the largest")
+
+
+@pytest.mark.skipif(not FUNDEM.exists(), reason="oracle/_ref/c0_bench_fundem not built (needs the reference tree)")
+@pytest.mark.skipif(shutil.which("nvcc") is None and not OURS.exists(), reason="nvcc not available")
+def test_two_phases_same_gpu(lsdem, tmp_path):
+    """Two solve() phases, the floor's angular velocity set between them (as tutorial 2
+    does), on a dense scene whose contacts persist across the phase boundary: the
+    reference keeps its state, forces and contact history between phases; the velocities
+    after 30 steps of the second phase agree with the reference build's to FP64 round-off."""
+    from helpers import dense_ellipsoid_scene
+    from lsdem_b200 import scenes
+    build_ours()
+    sc = dense_ellipsoid_scene(scenes, n=64, seed=23, vel_sigma=0.2)
+    n1, n2 = 40, 40
+    k0, k1 = 5, n1 + 30
+    scene = tmp_path / "c0p.bin"
+    scenes.write_c0_app_scene(scene, sc, n1, k0, k1, nsteps2=n2, floor_wz=20.0)
+    res = {}
+    for name, binary in (("fundem", FUNDEM), ("b200", OURS)):
+        out = tmp_path / name
+        out.mkdir()
+        res[name] = run(binary, scene, out, tmp_path / f"{name}.res")
+    (s0, w0, ms0, v0), (s1, w1, ms1, v1) = res["fundem"], res["b200"]
+    assert s0 == s1 == n1 + n2 and w0 == w1 == k1 - k0
+    vmax = np.abs(v0).max()
+    err = np.abs(v1 - v0).max() / vmax
+    assert err <= 1e-9, err
+    print(f"two phases: velocity difference {err:.2e} of the largest")

@@ -1,7 +1,8 @@
 """V-bonds on the GPU against the FP64 oracle, from identical state.
 
 Bonds are created from the contacts of a dense ellipsoid scene (createBondsFromContacts,
-LSSolver.h:385-418: one bond per particle-particle contact), then the scene is stepped.
+LSSolver.h:385-418: one bond per particle-particle contact), then the scene is stepped in
+a new phase, which keeps the contact history of the step before.
 Before each step the bond flags and state are read; the external-force hook captures the
 state the step's forces were computed from; the oracle recomputes contacts (with the
 GPU's previous contact list as history) and contact + bond forces from it
@@ -28,11 +29,12 @@ def test_bond_step_parity(lsdem, prec, strength):
     sv = load_scene(lsdem, scenes, sc, precision=prec)
     dt = 1e-6
     sv.step(dt, 1)
+    # the next phase keeps this step's contact history (as the reference's contact arrays)
+    prev = {"pp": sv.contacts(lsdem.CONTACT_PARTICLE), "pw": sv.contacts(lsdem.CONTACT_WALL)}
     sv.create_bonds_from_contacts(1.0e-3, 1.0e-4, 1e8, 0.3, strength, strength, 0.3)
     nb = sv.num(2)
     assert nb > 20, "the scene must produce bonds"
     sv.initialize(sc["min"], sc["max"], sc["gravity"])
-    prev = None
     broken = 0
     for step in range(3):
         before = sv.bonds()
