@@ -80,6 +80,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _bf16_peak():
+    """Dense BF16 tensor throughput (TFLOP/s): the measured burst figure (the network pass
+    is timed on its own launches), else the fallback."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+# FLOP per network evaluation: layer 1 (3 x 64 multiply-adds + bias), the layer-2 MMA
+# (64 x 64 multiply-adds), the output layer (64 multiply-adds): 2 x (192 + 4096 + 64) = 8704.
+NET_FLOP = 8704
+
+
 # Algorithmic bytes of the narrowphase kernel of each form.
 # FP64 form, k_narrowphase (detection and forces fused): per owner particle (pose,
 # velocities, slot counts, force/torque write: 208 B), per candidate pair (partner id,
@@ -100,6 +114,9 @@ B_PAIR_SCREEN = 120
 SCREEN_TRAFFIC_DEFAULT = (22.89e6 + 0.22e6 + 11.57e6) / 2
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
+# What bounds the screen, from an ncu capture of k_screen_f (particle pairs, FP32/BF16 form)
+# on the 200,000-particle settling box (the recipe and figures are in profiles/).
+SCREEN_LIMITER = None
 
 
 class Clocks:
@@ -295,7 +312,20 @@ def force_error(lsdem, sc, workload, device, prec, warm=20, learned=False):
 SAMPLE_PARTICLES = 4000  # host sample of the large-scale workload (CPU baseline, reference arm)
 
 
+ORACLE_BUILD = {"flags": "-O3 -fopenmp -ffp-contract=off (portable x86-64 build)"}
+
+
 def _oracle():
+    """The FP64 oracle for the CPU timing, built here with -march=native for this host's cores
+    (the checker's portable build when that fails)."""
+    if "oracle" not in sys.modules and not os.environ.get("LSDEM_ORACLE_LIB"):
+        import tempfile
+        out = Path(tempfile.mkdtemp(prefix="lsdem_oracle_")) / "liboracle_native.so"
+        r = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "native", f"NATIVE_OUT={out}"],
+                           capture_output=True, text=True)
+        if r.returncode == 0 and out.exists():
+            os.environ["LSDEM_ORACLE_LIB"] = str(out)
+            ORACLE_BUILD["flags"] = "-O3 -march=native -fopenmp -ffp-contract=off (built on this host)"
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as ora  # the checker, timed as the CPU baseline / reference arm only
     return ora
@@ -350,7 +380,7 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_second
         done, t, threads = time_oracle(ora, model, sc["dt"], steps, min_seconds, max_steps)
         m = len(smp["pos"])
         return {"value": m * done / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                "sample": (f"{m} particles of the same 16 superquadrics in a box periodic in x and y with floor and "
+                "build": ORACLE_BUILD["flags"], "sample": (f"{m} particles of the same 16 superquadrics in a box periodic in x and y with floor and "
                            f"ceiling at the same solid fraction ({smp['max'][0]:.4f} m side), random sequential "
                            f"addition, {done} steps of the FP64 oracle (reference per-node 27-cell algorithm)")}
 
@@ -400,7 +430,7 @@ def cpu_baseline(lsdem, sc, workload, target_particles=3000, steps=2, min_second
     steps, t, threads = time_oracle(ora, model, sc["dt"], steps, min_seconds, max_steps)
     m = len(idx)
     return {"value": m * steps / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": (f"{m} particles of the same scene in a {frac:.3f}-scaled corner sub-box, {steps} steps "
+            "build": ORACLE_BUILD["flags"], "sample": (f"{m} particles of the same scene in a {frac:.3f}-scaled corner sub-box, {steps} steps "
                        f"of the FP64 oracle (reference per-node 27-cell algorithm)") if workload in ("small", "polydisperse")
             else (f"{m} particles of the same scene (the cluster nearest its median position, with the bonds among "
                   f"them), {steps} steps of the FP64 oracle (reference per-node 27-cell algorithm)")}
@@ -449,7 +479,7 @@ def run_reference(args, rank, world):
                "nodes_per_particle": 1500, "sdf_grid": "48 nodes on the longest axis", "periodic": "xy",
                "walls": "z", "solid_fraction": 0.25, "dt_s": 5e-7}
         cb = {"value": m * steps / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-              "sample": (f"{m} particles of the same 16 superquadrics (grids from the oracle's host generator, "
+              "build": ORACLE_BUILD["flags"], "sample": (f"{m} particles of the same 16 superquadrics (grids from the oracle's host generator, "
                          f"{t_prep:.0f} s) in a box periodic in x and y with floor and ceiling at the same solid "
                          f"fraction ({smp['max'][0]:.4f} m side), {steps} steps of the FP64 oracle "
                          f"(reference per-node 27-cell algorithm)")}
@@ -475,6 +505,22 @@ def run_reference(args, rank, world):
 
 
 L2_FLUSH_BYTES = 256 << 20  # > the 126 MB L2
+
+
+def tensor_roofline(head, scr):
+    """The learned form's network pass (k_net_screen, tcgen05): network evaluations per step
+    x NET_FLOP over the pass's per-step time (its own profile phase), against the dense BF16
+    peak."""
+    ms, calls = head["profile"].get("network", (0.0, 0))
+    rows = (scr or {}).get("net_evals", 0.0)
+    if not calls or not rows:
+        return None
+    t = ms / head["profile_steps"] * 1e-3
+    achieved = rows * NET_FLOP / t / 1e12
+    peak, kind = _bf16_peak()
+    return {"bound": "tensor", "kernel": "k_net_screen", "achieved": achieved, "peak": peak, "peak_kind": kind,
+            "unit": "TFLOP/s", "frac": achieved / peak, "rows_per_step": rows, "flop_per_row": NET_FLOP,
+            "ms_per_step": t * 1e3}
 
 
 def build_c0_app():
@@ -702,10 +748,17 @@ def main():
             "headline_over_plain_grid": (value / plain) if plain else None,
             "contacts_per_s": stats["contacts"] * per_s,
             "node_tests_per_s": scr.get("node_tests", 0.0) * per_s if scr else None,
-            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+            # The screen is bound by load latency and instruction issue, not by DRAM: its
+            # algorithmic bytes over its launch time are a few percent of HBM bandwidth
+            # (reported as such), the issue and warp figures come from ncu.
+            "roofline": {"bound": "latency/issue", "kernel": kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
+                         "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+                         "hbm_is_limiter": False, "limiter": SCREEN_LIMITER if prec != 0 else None,
+                         "node_tests_per_s_in_screen": (scr.get("node_tests", 0.0) * head["profile_steps"] /
+                                                        ((np_ms + g_ms) * 1e-3)) if scr else None},
             "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_step * 1e-3) / 1e9},
+            "tensor_roofline": tensor_roofline(head, scr),
             "phases_ms_per_step": {k: v[0] / head["profile_steps"] for k, v in prof.items()},
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": n * (3 * 24 + 32),
                     "d2h_bytes_per_step": n * (5 * 24 + 32)},

@@ -232,10 +232,11 @@ void* lsdem_stream(const lsdem_solver* s);
  * 1 cell sort, 2 candidates, 3 particle/wall narrowphase + forces (precision forms:
  * the FP32 screen), 4 periodic wrap + ghost images + ghost candidates, 5 ghost
  * narrowphase + forces (precision forms: the screen), 6 bonds, 7 second half kick,
- * 8 precision forms: FP64 contact pass of both narrowphases, 9 whole steps (step
- * timing, below). ms and calls hold LSDEM_NUM_PHASES entries. Enabling resets the
- * totals of phases 0-8. */
-#define LSDEM_NUM_PHASES 10
+ * 8 precision forms: FP64 contact pass of both narrowphases (learned form: with the
+ * compaction of the network's survivors), 9 whole steps (step timing, below), 10
+ * learned form: the network passes on the tensor cores. ms and calls hold
+ * LSDEM_NUM_PHASES entries. Enabling resets the totals of every phase but 9. */
+#define LSDEM_NUM_PHASES 11
 int lsdem_set_profiling(lsdem_solver* s, int on);
 int lsdem_get_profile(const lsdem_solver* s, double* ms, long long* calls);
 /* Benchmark support (no counterpart in the reference): when on, every step is

@@ -472,7 +472,7 @@ class Solver:
         return {"ids": ids, "bonded": bonded, "state": state}
 
     PHASES = ("kick_drift_keys", "cell_sort", "candidates", "narrowphase", "periodic", "ghost_narrowphase", "bonds",
-              "kick", "contact_pass", "step")
+              "kick", "contact_pass", "step", "network")
 
     def set_step_timing(self, on=True, l2_flush_bytes=0):
         """Per-step CUDA events (profile()["step"]), optionally with an L2 flush before each step."""

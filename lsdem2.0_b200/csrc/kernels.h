@@ -139,13 +139,17 @@ struct GhostView {
   int* count;          // number of entries in list
 };
 
+// Scratch of the bucket sort: counts, fill and offsets of cells + 3 buckets each,
+// scan partial sums (scan_temp_elems), the list of buckets over 64 members (n / 65 + 1),
+// two counters (buckets over 64, buckets of 9 to 64 members), and n entries that hold
+// the list of 9-to-64-member buckets and then the large buckets' copies.
 struct BucketScratch {
   int* counts;
   int* fill;
   int* offs;
   int* scan_tmp;
   int* big_list;
-  int* big_count;
+  int* big_count;  // 2 entries
   int* tmp;
 };
 
@@ -273,6 +277,10 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s);
 // precision form: FP64 contact pass over the pairs queued by the screen of
 // launch li (0: particles and walls, 1: periodic images)
 void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s);
+// learned form, after the screen of launch li: the network pass (tensor cores) and the
+// compaction of the surviving nodes for the contact pass (no-ops without the network)
+void launch_net_screen(const StepArgs& a, int li, cudaStream_t s);
+void launch_net_compact(const StepArgs& a, int li, cudaStream_t s);
 void launch_kick(const StepArgs& a, cudaStream_t s);
 void launch_periodic(const StepArgs& a, int axes, double3* out, cudaStream_t s);
 // g2_off: bucket offsets of the image search's cell sort (cell k at [k + 1])

@@ -763,7 +763,7 @@ void alloc_bucket(lsdem_solver* s, int n, int ncells, bool second = false) {
   CK(o.alloc(nb + 1));
   CK(sc.alloc(scan_temp_elems(nb + 1)));
   CK(b.alloc((size_t)n / 65 + 1));
-  CK(bc.alloc(1));
+  CK(bc.alloc(2));
   CK(t.alloc((size_t)std::max(n, 1)));
 }
 
@@ -1259,17 +1259,26 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
     bucket_sort(s->key2.p, a.P.n, s->pg.ncells, w2, s->g2_idx.p, nullptr, s->g2_start.p, s->g2_end.p, s2);
     launch_ghost_candidates(a2, s->g2_idx.p, w2.offs, s2);
     launch_narrowphase(a2, 4, s2);
+    launch_net_screen(a2, 1, s2);
+    launch_net_compact(a2, 1, s2);
     if (s->precision != PREC_FP64) launch_contact_pass(a2, 1, s2);
     CK(cudaEventRecord(s->ev_join, s2));
     launch_candidates(a, st);
     launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st);
+    launch_net_screen(a, 0, st);
+    launch_net_compact(a, 0, st);
     if (s->precision != PREC_FP64) launch_contact_pass(a, 0, st);
     CK(cudaStreamWaitEvent(st, s->ev_join, 0));
     if (a.P.n > 0) CK(cudaMemcpyAsync(a.P.pos, s->pos_w.p, sizeof(double3) * a.P.n, cudaMemcpyDeviceToDevice, st));
   } else {
     { PhaseTimer pt(s, 2); launch_candidates(a, st); }
     { PhaseTimer pt(s, 3); launch_narrowphase(a, s->W.n() > 0 ? 3 : 1, st); }
-    if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 0, st); }
+    if (a.mlp_inf) { PhaseTimer pt(s, 10); launch_net_screen(a, 0, st); }
+    if (s->precision != PREC_FP64) {
+      PhaseTimer pt(s, 8);
+      launch_net_compact(a, 0, st);
+      launch_contact_pass(a, 0, st);
+    }
     if (s->nsets > 0) {
       {
         PhaseTimer pt(s, 4);
@@ -1279,7 +1288,12 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
         launch_ghost_candidates(a, s->g2_idx.p, w2.offs, st);
       }
       { PhaseTimer pt(s, 5); launch_narrowphase(a, 4, st); }
-      if (s->precision != PREC_FP64) { PhaseTimer pt(s, 8); launch_contact_pass(a, 1, st); }
+      if (a.mlp_inf) { PhaseTimer pt(s, 10); launch_net_screen(a, 1, st); }
+      if (s->precision != PREC_FP64) {
+        PhaseTimer pt(s, 8);
+        launch_net_compact(a, 1, st);
+        launch_contact_pass(a, 1, st);
+      }
     }
   }
   if (!s->bonds.bonded.empty()) {
@@ -1291,9 +1305,14 @@ void step_pre(lsdem_solver* s, double dt, bool record) {
   // kernels launched up to here: kick/drift/keys, cell sort (10; with neighbour lists
   // they return at once between rebuilds), packing + candidates, narrowphase; periodic:
   // wrap/images, clamped keys, cell sort (9), image compaction + packing + candidates,
-  // ghost narrowphase; bonds (the precision form adds one contact pass per narrowphase)
-  const int nf = s->precision == PREC_FP64 ? 0 : 1;
-  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 15 + nf : 0) + (s->bonds.bonded.empty() ? 0 : 1);
+  // ghost narrowphase; bonds. The precision forms add one contact pass per narrowphase
+  // and a separate wall screen; the learned form the network pass and the compaction
+  // after each screen.
+  const bool fp32 = s->precision != PREC_FP64;
+  const int lrn = a.mlp_inf ? 2 : 0;
+  const int nf = fp32 ? 1 + (s->W.n() > 0 ? 1 : 0) + lrn : 0;
+  const int ng = fp32 ? 1 + lrn : 0;
+  if (a.P.n > 0) s->launches += 14 + nf + (s->nsets > 0 ? 15 + ng : 0) + (s->bonds.bonded.empty() ? 0 : 1);
   CK(cudaGetLastError());
 }
 
@@ -2499,7 +2518,8 @@ int lsdem_set_neighbour_lists(lsdem_solver* s, int on) {
 int lsdem_set_profiling(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   s->profiling = on != 0;
-  for (int k = 0; k < 9; ++k) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
+  for (int k = 0; k < LSDEM_NUM_PHASES; ++k)
+    if (k != 9) { s->prof_ms[k] = 0.; s->prof_calls[k] = 0; }
   return LSDEM_OK;
 }
 

@@ -7,6 +7,8 @@
 // and each bucket is put back into ascending particle order, which yields
 // exactly the order of a stable sort by key. Memory traffic per particle:
 // key read three times, index written twice, plus 8 B per cell.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace lsdem {
@@ -142,7 +144,7 @@ __global__ void k_bucket_clear(int* __restrict__ counts, int* __restrict__ fill,
   if (idle(gate)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) { counts[i] = 0; fill[i] = 0; }
-  if (i == 0) *big_count = 0;
+  if (i == 0) big_count[0] = big_count[1] = 0;  // buckets for k_bucket_big, for k_bucket_mid
 }
 
 __global__ void k_bucket_hist(const int* __restrict__ key, int n, int ncells, int* __restrict__ counts, const int* gate) {
@@ -196,31 +198,75 @@ __global__ void k_special_buckets(const int* __restrict__ key, int n, int ncells
 // share the last bucket, in ascending key and then index order.
 __device__ __forceinline__ bool key_idx_less(int ka, int a, int kb, int b) { return ka < kb || (ka == kb && a < b); }
 
+// Compare-exchange of two (key, index) entries.
+__device__ __forceinline__ void cx(int& ka, int& a, int& kb, int& b) {
+  if (key_idx_less(kb, b, ka, a)) {
+    const int t = a, tk = ka;
+    a = b; ka = kb;
+    b = t; kb = tk;
+  }
+}
+
 // Cell ranges [start, end) of every cell (-1 when empty; findStartAndEnd,
 // buildHashStartEnd.cu:47-67) and the stable order inside each bucket (the
-// scatter leaves members in arbitrary order): one warp per bucket, members of
-// buckets up to 64 long are ranked by particle index in registers (the last
-// bucket by key, then index); longer buckets go to k_bucket_big, except the -1
-// bucket, which k_special_buckets has put in index order.
+// scatter leaves members in arbitrary order), one thread per bucket: a bucket of up
+// to 8 members is put in order in registers by an odd-even transposition network
+// (by particle index; the last bucket, whose keys differ, by key, then index);
+// buckets of 9 to 64 members are listed for k_bucket_mid (in tmp, which k_bucket_big
+// uses only after it), longer ones for k_bucket_big, except the -1 bucket, which
+// k_special_buckets has put in index order.
 __global__ void k_bucket_fix(const int* __restrict__ key, const int* __restrict__ offs, int nbuckets, int ncells,
                              int* __restrict__ sorted_idx, int* __restrict__ start, int* __restrict__ end,
-                             int* __restrict__ big_list, int* __restrict__ big_count, const int* gate) {
+                             int* __restrict__ big_list, int* __restrict__ big_count, int* __restrict__ mid_list,
+                             const int* gate) {
+  if (idle(gate)) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbuckets) return;
+  const int s = offs[b], e = offs[b + 1], L = e - s;
+  if (b > 0 && b <= ncells) {
+    start[b - 1] = L > 0 ? s : -1;
+    end[b - 1] = L > 0 ? e : -1;
+  }
+  if (L <= 1) return;
+  if (b == 0 && L > 64) return;  // placed in index order by k_special_buckets
+  if (L > 64) {
+    // the last bucket was put in index order by k_special_buckets; k_bucket_big
+    // re-ranks it by key
+    big_list[atomicAdd(&big_count[0], 1)] = b;
+    return;
+  }
+  if (L > 8) {
+    mid_list[atomicAdd(&big_count[1], 1)] = b;
+    return;
+  }
+  const bool bykey = b == ncells + 1;
+  int v[8], k[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    v[j] = j < L ? sorted_idx[s + j] : 0x7fffffff;
+    k[j] = (j < L && bykey) ? key[v[j]] : (j < L ? 0 : 0x7fffffff);
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+#pragma unroll
+    for (int j = r & 1; j + 1 < 8; j += 2) cx(k[j], v[j], k[j + 1], v[j + 1]);
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (j < L) sorted_idx[s + j] = v[j];
+}
+
+// One warp per listed bucket of 9 to 64 members: ranked by particle index in registers
+// (the last bucket by key, then index).
+__global__ void k_bucket_mid(const int* __restrict__ key, const int* __restrict__ offs, int ncells,
+                             const int* __restrict__ mid_list, const int* __restrict__ big_count,
+                             int* __restrict__ sorted_idx, const int* gate) {
   if (idle(gate)) return;
   const int lane = threadIdx.x & 31;
-  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbuckets; b += (gridDim.x * blockDim.x) >> 5) {
-    const int s = offs[b], e = offs[b + 1], L = e - s;
-    if (lane == 0 && b > 0 && b <= ncells) {
-      start[b - 1] = L > 0 ? s : -1;
-      end[b - 1] = L > 0 ? e : -1;
-    }
-    if (L <= 1) continue;
-    if (b == 0 && L > 64) continue;  // placed in index order by k_special_buckets
-    if (L > 64) {
-      // the last bucket was put in index order by k_special_buckets; k_bucket_big
-      // re-ranks it by key
-      if (lane == 0) big_list[atomicAdd(big_count, 1)] = b;
-      continue;
-    }
+  const int nmid = big_count[1];
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nmid; q += (gridDim.x * blockDim.x) >> 5) {
+    const int b = mid_list[q];
+    const int s = offs[b], L = offs[b + 1] - s;
     const int v0 = lane < L ? sorted_idx[s + lane] : 0x7fffffff;
     const int v1 = lane + 32 < L ? sorted_idx[s + 32 + lane] : 0x7fffffff;
     int r0 = 0, r1 = 0;
@@ -292,8 +338,12 @@ void bucket_sort(const int* key, int n, int ncells, BucketScratch& w, int* sorte
     k_bucket_scatter<<<(n + 255) / 256, 256, 0, s>>>(key, n, ncells, w.offs, w.fill, sorted_idx, gate);
     k_special_buckets<<<1, 1024, 0, s>>>(key, n, ncells, w.offs, sorted_idx, gate);
   }
-  k_bucket_fix<<<(unsigned)((nb + 7) / 8), 256, 0, s>>>(key, w.offs, nb, ncells, sorted_idx, start, end, w.big_list,
-                                                        w.big_count, gate);
+  k_bucket_fix<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(key, w.offs, nb, ncells, sorted_idx, start, end,
+                                                            w.big_list, w.big_count, w.tmp, gate);
+  // at most n / 9 buckets have 9 to 64 members: one warp each, grid-stride
+  const int max_mid = n / 9 + 1;
+  const int mid_blocks = std::min((max_mid + 7) / 8, 148 * 16);
+  if (n > 8) k_bucket_mid<<<mid_blocks, 256, 0, s>>>(key, w.offs, ncells, w.tmp, w.big_count, sorted_idx, gate);
   // at most n / 65 buckets can exceed 64 members
   int max_big = n / 65 + 1;
   k_bucket_big<<<max_big, 256, 0, s>>>(key, w.offs, ncells, w.big_list, w.big_count, sorted_idx, w.tmp, gate);

@@ -1683,25 +1683,29 @@ void launch_net_k(const StepArgs& a, int li, cudaStream_t s) {
   }
   // four CTAs per SM: 4 x 64 tensor-memory columns, the other launch's pass fits beside it
   k_net_screen<SDFK><<<num_sms() * 4, MLP_TILE, smem, s>>>(a, li);
-  k_net_compact<<<num_sms() * 16, NP_WARPS * 32, 0, s>>>(a, li);
 }
-void launch_net(const StepArgs& a, int li, cudaStream_t s) {
+void launch_net_screen(const StepArgs& a, int li, cudaStream_t s) {
+  if (!a.mlp_inf || a.P.n <= 0) return;
   if (a.precision == PREC_FP32_FP16) launch_net_k<PREC_FP32_FP16>(a, li, s);
   else launch_net_k<PREC_FP32_BF16>(a, li, s);
 }
+void launch_net_compact(const StepArgs& a, int li, cudaStream_t s) {
+  if (!a.mlp_inf || a.P.n <= 0) return;
+  k_net_compact<<<num_sms() * 16, NP_WARPS * 32, 0, s>>>(a, li);
+}
 
 template <bool LRN>
+// Particle and wall pairs in two launches: the particle-only screen fits 64 registers
+// (8 blocks per SM); the wall pairs (few) take the window test's FP64 registers.
 void launch_screen(const StepArgs& a, int kinds, int li, dim3 g, dim3 b, cudaStream_t s) {
   if (a.precision == PREC_FP32_FP16) {
-    if (kinds == 3) launch_screen_k<3, PREC_FP32_FP16, LRN>(a, li, g, b, s);
-    else if (kinds == 1) launch_screen_k<1, PREC_FP32_FP16, LRN>(a, li, g, b, s);
-    else if (kinds == 4) launch_screen_k<4, PREC_FP32_FP16, LRN>(a, li, g, b, s);
-    else launch_screen_k<7, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    if (kinds & 1) launch_screen_k<1, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    if (kinds & 2) launch_screen_k<2, PREC_FP32_FP16, LRN>(a, li, g, b, s);
+    if (kinds & 4) launch_screen_k<4, PREC_FP32_FP16, LRN>(a, li, g, b, s);
   } else {
-    if (kinds == 3) launch_screen_k<3, PREC_FP32_BF16, LRN>(a, li, g, b, s);
-    else if (kinds == 1) launch_screen_k<1, PREC_FP32_BF16, LRN>(a, li, g, b, s);
-    else if (kinds == 4) launch_screen_k<4, PREC_FP32_BF16, LRN>(a, li, g, b, s);
-    else launch_screen_k<7, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    if (kinds & 1) launch_screen_k<1, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    if (kinds & 2) launch_screen_k<2, PREC_FP32_BF16, LRN>(a, li, g, b, s);
+    if (kinds & 4) launch_screen_k<4, PREC_FP32_BF16, LRN>(a, li, g, b, s);
   }
 }
 
@@ -1721,12 +1725,8 @@ void launch_narrowphase(const StepArgs& a, int kinds, cudaStream_t s) {
   // precision form: the screen over the flat pair lists (launch_contact_pass
   // follows it); the grid is sized for the device, the list length is on it
   const int li = kinds == 4 ? 1 : 0;
-  if (a.mlp_inf) {
-    launch_screen<true>(a, kinds, li, g, b, s);
-    launch_net(a, li, s);
-  } else {
-    launch_screen<false>(a, kinds, li, g, b, s);
-  }
+  if (a.mlp_inf) launch_screen<true>(a, kinds, li, g, b, s);  // launch_net_screen and _compact follow
+  else launch_screen<false>(a, kinds, li, g, b, s);
 }
 
 void launch_contact_pass(const StepArgs& a, int li, cudaStream_t s) {

@@ -16,13 +16,16 @@ kernels is pinned by the golden vectors under tests/golden/.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB = HERE / "liboracle.so"
+# LSDEM_ORACLE_LIB: another build of the same source (the benchmark's CPU baseline builds
+# one with -march=native for the host it runs on)
+LIB = Path(os.environ["LSDEM_ORACLE_LIB"]) if os.environ.get("LSDEM_ORACLE_LIB") else HERE / "liboracle.so"
 
 FIX_GRADIENT = 1
 FIX_SQRTF = 2

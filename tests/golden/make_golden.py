@@ -292,4 +292,6 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else str(ROOT / "gpurun_out" / "golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py OUTPUT_DIR  (the fixtures are then copied into tests/golden/)")
+    main(sys.argv[1])

@@ -102,3 +102,13 @@ def test_bond_stiffness_from_beam_theory(lsdem):
     assert sv.num(2) == 1
     b = sv.bonds()
     assert b["ids"].tolist() == [[0, 1]] and b["bonded"].tolist() == [1]
+
+
+def test_compat_launchers_exported(lsdem):
+    """Every launcher include/lsdem_compat.h declares (the reference's extern "C" names) is
+    exported by the library."""
+    txt = (ROOT / "include" / "lsdem_compat.h").read_text()
+    names = sorted(set(re.findall(r"^void\s+(launch\w+)\s*\(", txt, flags=re.M)))
+    assert len(names) == 5
+    for n in names:
+        assert hasattr(lsdem.lib, n), f"{n} declared in include/lsdem_compat.h but not exported"

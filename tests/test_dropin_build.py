@@ -6,6 +6,7 @@ repository's include/ first on the include path they build against
 include/kernel/LSSolver.h and link liblsdem_b200.so. Needs the reference tree
 (present where the repository is developed, absent on GPU hosts).
 """
+import os
 import shutil
 import subprocess
 from pathlib import Path
@@ -14,7 +15,7 @@ import pytest
 
 from conftest import ROOT
 
-REF = Path("/root/reference/FunDEM")
+REF = Path(os.environ.get("REF", "/root/reference")) / "FunDEM"  # the reference tree, where it is present
 APPS = ["tutorial1-LSParticleFalling", "tutorial2-LSParticleRolling", "tutorial3-bondedLSParticleBeam",
         "tutorial4-PeriodicBoundary"]
 
