@@ -22,9 +22,10 @@ LIB = HERE / "liblsdem_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-I", str(ROOT / "include")]
-# Per-file flags: the mesh grid builder and the frame writer round every product and sum
-# separately, as the reference's host code does (no fused multiply-add contraction).
-FILE_FLAGS = {"sdfgen.cu": ["--fmad=false"], "vtu.cu": ["--fmad=false"]}
+# Per-file flags: the mesh grid builder, the frame writer and the bond builder round every
+# product and sum separately, as the host code they match does (no fused multiply-add
+# contraction).
+FILE_FLAGS = {"sdfgen.cu": ["--fmad=false"], "vtu.cu": ["--fmad=false"], "bonds.cu": ["--fmad=false"]}
 
 
 def _nvcc() -> str:

@@ -298,6 +298,12 @@ struct BondView {
   double* state;         // 9 per bond: Un, Us, Ub, Ut, sigma_max, tau_max, point xyz
 };
 void launch_bonds(const StepArgs& a, const BondView& b, cudaStream_t s);
+// Bonds from the recorded particle-particle contacts (bonds.cu): contacts per owner, then
+// one bond per contact at offs[owner] + k: ids (2), frames (8 vectors), point.
+void bonds_from_contacts_count(const SlotView& pp, int n, int* cnt, cudaStream_t s);
+void bonds_from_contacts_make(const SlotView& pp, int n, const int* offs, const double3* point, const double3* normal,
+                              const double3* pos, const Quat* quat, double Lb, int* ids, double3* frames,
+                              double3* bpoint, int* bad, cudaStream_t s);
 
 
 // ---------------------------------------------------------------------------

@@ -2431,25 +2431,54 @@ int lsdem_create_bonds_from_contacts(lsdem_solver* s, double radius, double L0, 
     lsdem_count_contacts(s, LSDEM_CONTACT_PARTICLE, &n);
     if (n == 0) return LSDEM_OK;
     if (!s->con[s->hp].geom) throw Fail{LSDEM_ERR_STATE, "contact geometry not recorded (lsdem_set_record_contacts)"};
-    std::vector<long long> node(n);
-    std::vector<int> partner(n);
-    std::vector<double> point(3 * n), normal(3 * n);
-    int rc = lsdem_get_contacts(s, LSDEM_CONTACT_PARTICLE, n, node.data(), partner.data(), nullptr, nullptr,
-                                point.data(), normal.data(), nullptr, nullptr, nullptr);
-    if (rc) return rc;
-    // host copy of particle state, as the reference reads its host mirrors
-    std::vector<double> pos(3 * (size_t)s->P.n()), quat(4 * (size_t)s->P.n());
-    rc = lsdem_get_state(s, pos.data(), nullptr, nullptr, quat.data(), nullptr, nullptr);
-    if (rc) return rc;
-    std::vector<long long> nbase(s->P.n() + 1);
-    long long nb = 0;
-    for (int i = 0; i < s->P.n(); ++i) { nbase[i] = nb; nb += (long long)(s->shapes[s->P.shape[i]].nodes.size() / 3); }
-    nbase[s->P.n()] = nb;
-    for (long long k = 0; k < n; ++k) {
-      const int i = (int)(std::upper_bound(nbase.begin(), nbase.end(), node[k]) - nbase.begin()) - 1;
-      const int j = partner[k];
-      add_bond_impl(s, i, j, &pos[3 * (size_t)i], &quat[4 * (size_t)i], &pos[3 * (size_t)j], &quat[4 * (size_t)j],
-                    &point[3 * k], &normal[3 * k], radius, L0, E, nu, ten, coh, mu);
+    // the bond constants are the same for every bond: checked once, as add_bond_impl does
+    if (radius <= 0.) throw Fail{LSDEM_ERR_ARG, "Invalid bond radius"};
+    if (L0 <= 0.) throw Fail{LSDEM_ERR_ARG, "Invalid bond length"};
+    if (E <= 0.) throw Fail{LSDEM_ERR_ARG, "Invalid Young's modulus"};
+    if (nu <= -1.0 || nu >= 0.5) throw Fail{LSDEM_ERR_ARG, "Invalid Poisson ratio"};
+    pull_host(s);
+    cudaStream_t st = s->stream;
+    const int np = s->P.n();
+    SlotsDev& sl = s->slots[s->hp][LSDEM_CONTACT_PARTICLE];
+    const SlotView v{sl.cap, sl.cnt.p, sl.id.p, sl.seg_start.p, sl.seg_cnt.p};
+    // contacts per owner, their offsets, then one bond per contact in list order, on the device
+    DArr<int> cnt, offs, tmp;
+    CK(cnt.alloc(np)); CK(offs.alloc(np)); CK(tmp.alloc(scan_temp_elems(np)));
+    bonds_from_contacts_count(v, np, cnt.p, st);
+    scan_i32(cnt.p, offs.p, np, tmp.p, false, st);
+    int last[2] = {0, 0};
+    CK(cudaMemcpyAsync(&last[0], offs.p + np - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], cnt.p + np - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const size_t nb = (size_t)last[0] + last[1];
+    if (nb == 0) return LSDEM_OK;
+    DArr<int> ids, bad;
+    DArr<double3> frames, bpt;
+    CK(ids.alloc(2 * nb)); CK(bad.alloc(1)); CK(bad.zero(st));
+    CK(frames.alloc(8 * nb)); CK(bpt.alloc(nb));
+    ContactsDev& c = s->con[s->hp];
+    bonds_from_contacts_make(v, np, offs.p, c.point.p, c.normal.p, s->dP.pos.p, s->dP.quat.p, L0, ids.p, frames.p,
+                             bpt.p, bad.p, st);
+    CK(cudaGetLastError());
+    std::vector<int> hid = dl(ids, 2 * nb, st), hbad = dl(bad, 1, st);
+    std::vector<double3> hfr = dl(frames, 8 * nb, st), hpt = dl(bpt, nb, st);
+    CK(cudaStreamSynchronize(st));
+    if (hbad[0]) throw Fail{LSDEM_ERR_ARG, "Invalid bond normal"};
+    // constants of add_bond_impl (VBondedInteraction.h:74-195)
+    const double Gb = E / (2. * (1. + nu));
+    const double Ab = M_PI * radius * radius;
+    const double Ib = Ab * radius * radius / 4.;
+    const double Jb = 2. * Ib;
+    const double Kn = E * Ab / L0, Kt = Gb * Jb / L0, Ks = 12. * E * Ib / (L0 * L0 * L0), Kb = E * Ib / L0;
+    const double B1 = Kn, B2 = L0 * L0 * Ks, B4 = Kt, B3 = Kb - B2 / 4. - B4 / 2.;
+    BondHost& b = s->bonds;
+    for (size_t k = 0; k < nb; ++k) {
+      b.ids.push_back(hid[2 * k]); b.ids.push_back(hid[2 * k + 1]);
+      b.bonded.push_back(1);
+      b.B.insert(b.B.end(), {B1, B2, B3, B4});
+      b.geo.insert(b.geo.end(), {radius, L0, ten, coh, mu});
+      for (int f = 0; f < 8; ++f) b.frames.insert(b.frames.end(), {hfr[8 * k + f].x, hfr[8 * k + f].y, hfr[8 * k + f].z});
+      b.state.insert(b.state.end(), {0., 0., 0., 0., 0., 0., hpt[k].x, hpt[k].y, hpt[k].z});
     }
     s->ready = false;
     return LSDEM_OK;

@@ -1149,16 +1149,24 @@ LD float2 unpack16(unsigned w) {
   return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
 template <int SDFK>
-LD float phi16_at(const uint4* cells, int sy, int sz, float gx, float gy, float gz) {
-  const int i0 = __float2int_rd(gx), j0 = __float2int_rd(gy), k0 = __float2int_rd(gz);
-  const float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
-  const uint4 w = __ldg(cells + (k0 * sz + j0 * sy + i0));
+LD float phi16_interp(uint4 w, float gx, float gy, float gz) {
+  const float fx = gx - floorf(gx), fy = gy - floorf(gy), fz = gz - floorf(gz);
   const float2 c01 = unpack16<SDFK>(w.x), c23 = unpack16<SDFK>(w.y);
   const float2 c45 = unpack16<SDFK>(w.z), c67 = unpack16<SDFK>(w.w);
   const float x0 = fmaf(fx, c01.y - c01.x, c01.x), x1 = fmaf(fx, c23.y - c23.x, c23.x);
   const float x2 = fmaf(fx, c45.y - c45.x, c45.x), x3 = fmaf(fx, c67.y - c67.x, c67.x);
   const float y0 = fmaf(fy, x1 - x0, x0), y1 = fmaf(fy, x3 - x2, x2);
   return fmaf(fz, y1 - y0, y0);
+}
+// The cell's corners (one 16-byte load) and the interpolation, split so that the load
+// can be issued early.
+LD uint4 phi16_cell(const uint4* cells, int sy, int sz, float gx, float gy, float gz) {
+  const int i0 = __float2int_rd(gx), j0 = __float2int_rd(gy), k0 = __float2int_rd(gz);
+  return __ldg(cells + (k0 * sz + j0 * sy + i0));
+}
+template <int SDFK>
+LD float phi16_at(const uint4* cells, int sy, int sz, float gx, float gy, float gz) {
+  return phi16_interp<SDFK>(phi16_cell(cells, sy, sz, gx, gy, gz), gx, gy, gz);
 }
 template <int SDFK>
 LD float phi16(const PairF& F, float gx, float gy, float gz) {
@@ -1570,18 +1578,28 @@ __global__ void __launch_bounds__(MLP_TILE) k_net_screen(StepArgs a, int li) {
     const int r = (t - s_pre[sh]) * MLP_TILE + threadIdx.x;
     const bool act = r < rows;
     const float4 u = act ? Q.row[(size_t)sh * Q.qcap + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int idx = __float_as_int(u.w);
+    // the grid test's operands are fetched before the network runs (its 16-byte cell load
+    // is then in flight during layer 1 and the MMA); the test is applied only to the
+    // nodes the network keeps
+    const int nflag = act ? Q.pend_n[idx] : -1;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint4 cell = make_uint4(0u, 0u, 0u, 0u);
+    if (nflag >= 0) {
+      g = Q.pend_g[idx];
+      const int3 gs = a.S.gsize[sh];
+      cell = phi16_cell(a.S.cell16 + a.S.cell_off[sh], gs.x - 1, (gs.x - 1) * (gs.y - 1), g.x, g.y, g.z);
+    }
     mlp_tc_layer1(T, u.x, u.y, u.z);
     ok = mlp_tc_mma(T);
     const float y = mlp_tc_output(T);
     if (act) {
-      const int idx = __float_as_int(u.w);
       unsigned char may = 1;
       if (ok && !(y * __ldg(&a.mlp_norm[sh].r_over_h) > __ldg(&a.mlp_band[sh]))) {
-        // kept by the network: the plain screen's grid test decides
-        if (Q.pend_n[idx] >= 0) {
-          const float4 g = Q.pend_g[idx];
-          const int3 gs = a.S.gsize[sh];
-          may = !(phi16_at<SDFK>(a.S.cell16 + a.S.cell_off[sh], gs.x - 1, (gs.x - 1) * (gs.y - 1), g.x, g.y, g.z) > g.w);
+        // kept by the network: the plain screen's grid test decides (not within the error
+        // of the grid boundary, where the FP64 test decides)
+        if (nflag >= 0) {
+          may = !(phi16_interp<SDFK>(cell, g.x, g.y, g.z) > g.w);
           ++looks;
         }
       } else if (ok) {

@@ -594,12 +594,14 @@ def load_polydisperse(solver, sc):
 # Bonded, drum and large-scale workloads
 
 
-def _unit_density_templates(lsdem, T):
+def _unit_density_templates(lsdem, T, gpu=False):
     """Mass (= volume at density 1), inverse inertia and the frame moved to the centroid, from
-    each template's grid by the reference's smoothed-Heaviside integration (LSSolver.h:66-135)."""
+    each template's grid by the reference's smoothed-Heaviside integration (LSSolver.h:66-135),
+    on the host or (gpu=True, for the large template sets) on the GPU."""
     out = []
+    mp_fn = lsdem.mass_properties_gpu if gpu else lsdem.mass_properties
     for t in T:
-        mp = lsdem.mass_properties(t["sdf"], t["size"], t["origin"], t["spacing"], 1.0)
+        mp = mp_fn(t["sdf"], t["size"], t["origin"], t["spacing"], 1.0)
         c = mp["centroid"]
         out.append({"nodes": t["nodes"] - c, "sdf": t["sdf"], "size": t["size"], "origin": t["origin"] - c,
                     "spacing": t["spacing"], "mass": mp["mass"], "inv_inertia": mp["inv_inertia"],
@@ -865,7 +867,7 @@ def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-
     the empty upper part of the drum."""
     rng = np.random.default_rng(seed_for(3) if seed is None else seed)
     T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
-    tm = _unit_density_templates(lsdem, T)
+    tm = _unit_density_templates(lsdem, T, gpu=True)
     shape = rng.integers(0, len(tm), size=n).astype(np.int32)
     vol = np.array([t["mass"] for t in tm])[shape].sum()
     lo = np.array([-0.5 * length + 5e-3, -0.7 * radius, -math.sqrt(radius ** 2 - (0.7 * radius) ** 2)])
@@ -908,7 +910,7 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
     fraction, no overlaps), which raises the ceiling accordingly."""
     rng = np.random.default_rng(seed_for(4) if seed is None else seed)
     T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
-    tm = _unit_density_templates(lsdem, T)
+    tm = _unit_density_templates(lsdem, T, gpu=True)
     shape = rng.integers(0, len(tm), size=n).astype(np.int32)
     vol = np.array([t["mass"] for t in tm])[shape].sum()
     L = (vol / solid_fraction) ** (1.0 / 3.0)

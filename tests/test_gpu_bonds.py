@@ -75,3 +75,33 @@ def test_bond_step_parity(lsdem, prec, strength):
         assert broken == 0 and (sv.bonds()["bonded"] == 1).all(), "unbreakable bonds must survive"
     else:
         assert broken > 0, "weak bonds must break"
+
+
+def test_bonds_from_contacts_built_on_device_equal_host_routine(lsdem):
+    """lsdem_create_bonds_from_contacts builds the bonds on the device (bonds.cu). The same
+    contacts added one by one through lsdem_add_bond (the host routine, VBondedInteraction::add,
+    VBondedInteraction.h:74-195), in the contact list's order, give the same bonds bit for bit:
+    topology, stiffness constants, local frames and points."""
+    from lsdem_b200 import scenes
+    sc = dense_ellipsoid_scene(scenes, n=64, seed=19)
+    args = (1.0e-3, 1.0e-4, 1e8, 0.3, 2e6, 2e6, 0.3)
+    dev = load_scene(lsdem, scenes, sc)
+    dev.step(1e-6, 2)
+    c = dev.contacts(lsdem.CONTACT_PARTICLE, geometry=True)
+    st = dev.state()
+    nb = dev.particle_params()["node_base"]
+    owner = np.searchsorted(nb, c["node"], side="right") - 1
+    dev.create_bonds_from_contacts(*args)
+    host = load_scene(lsdem, scenes, sc)
+    host.set_state(pos=st["pos"], vel=st["vel"], angvel=st["angvel"], quat=st["quat"])
+    for k in range(len(owner)):
+        host.add_bond(int(owner[k]), int(c["partner"][k]), c["point"][k], c["normal"][k], *args)
+    assert dev.num(2) == host.num(2) == len(owner) > 50
+    bd, bh = dev.bonds(), host.bonds()
+    assert np.array_equal(bd["ids"], bh["ids"])
+    assert np.array_equal(bd["state"], bh["state"])
+    pd, ph = dev.bond_params(), host.bond_params()
+    for k in ("B", "geo", "frames"):
+        assert np.array_equal(pd[k], ph[k]), k
+    dev.close()
+    host.close()

@@ -95,13 +95,15 @@ def test_integration_launchers(lsdem):
     g = gold("integration.npz")
     n = len(g["vel"])
     v, w = _dev(g["vel"]), _dev(g["angvel"])
-    kick(_p(v), _p(w), _p(_dev(g["force"])), _p(_dev(g["torque"])), _p(_dev(g["invm"])), _p(_dev(g["quat"])),
-         _p(_dev(g["invI"])), _d3(g["g"]), float(g["h"]), n, 1, 64, None)
+    keep = {k: _dev(g[k]) for k in ("force", "torque", "invm", "quat", "invI")}  # alive until the kernel ran
+    kick(_p(v), _p(w), _p(keep["force"]), _p(keep["torque"]), _p(keep["invm"]), _p(keep["quat"]), _p(keep["invI"]),
+         _d3(g["g"]), float(g["h"]), n, 1, 64, None)
     torch.cuda.synchronize()
     assert _close(v.cpu().numpy(), g["vel_out"], 1e-14)
     assert _close(w.cpu().numpy(), g["angvel_out"], 1e-13)
     p, q = _dev(g["pos"]), _dev(g["quat"])
-    drift(_p(p), _p(q), _p(_dev(g["vel_out"])), _p(_dev(g["angvel_out"])), float(g["dt"]), n, 1, 64, None)
+    vo, wo = _dev(g["vel_out"]), _dev(g["angvel_out"])
+    drift(_p(p), _p(q), _p(vo), _p(wo), float(g["dt"]), n, 1, 64, None)
     torch.cuda.synchronize()
     assert _close(p.cpu().numpy(), g["pos_out"], 1e-15)
     assert _close(q.cpu().numpy(), g["quat_out"], 1e-15, scale=1.0)
