@@ -187,11 +187,12 @@ struct PairLists {
 // network pass writes each verdict (after the grid test of the nodes it keeps) and
 // the compaction pass queues the surviving nodes of each pair for the FP64 pass.
 struct NetView {
-  float4* row;            // nshapes * qcap: (u.x, u.y, u.z, pending index bits)
+  float4* row;            // nshapes * qcap rows of two float4: (u.x, u.y, u.z, pending index bits;
+                          //   bit 31 set: within the error of the grid boundary) and (grid point
+                          //   in the partner's grid x, y, z, the pair's threshold T)
   int* cnt;               // nshapes: rows appended this step
   int qcap;               // rows per shape
-  float4* pend_g;         // pcap: grid point in the partner's grid (x, y, z), the pair's threshold T
-  int* pend_n;            // pcap: node index; bit 31 set: within the error of the grid boundary
+  int* pend_n;            // pcap: node index
   unsigned char* pend_v;  // pcap: 1 when the node goes on to the FP64 test
   int pcap;
   int4* pair;             // paircap: {A, kind << 24 | slot, pending start, pending count}

@@ -370,7 +370,7 @@ struct lsdem_solver {
   long long mb_cap = 0, mb_pcap = 0;
   // learned form: network queues and pending nodes, per narrowphase launch
   struct NetDev {
-    DArr<float4> row, pend_g;
+    DArr<float4> row;
     DArr<int> cnt, pend_n, ctr;
     DArr<unsigned char> pend_v;
     DArr<int4> pair;
@@ -630,16 +630,15 @@ void alloc_net(lsdem_solver* s) {
                                    : (long long)n * s->slots[0][2].cap;
     if (l == 1 && s->nsets == 0) {
       N.qcap = N.pcap = N.paircap = 0;
-      N.row.release(); N.pend_g.release(); N.cnt.release(); N.pend_n.release(); N.ctr.release();
+      N.row.release(); N.cnt.release(); N.pend_n.release(); N.ctr.release();
       N.pend_v.release(); N.pair.release();
       continue;
     }
     N.qcap = (int)s->cap_netq;
     N.pcap = (int)s->cap_pend;
     N.paircap = (int)std::min<long long>(std::max<long long>(pairs, 1), 0x7fffffffLL);
-    CK(N.row.alloc((size_t)ns * N.qcap));
+    CK(N.row.alloc((size_t)ns * N.qcap * 2));
     CK(N.cnt.alloc(ns)); CK(N.cnt.zero(s->stream));
-    CK(N.pend_g.alloc(N.pcap));
     CK(N.pend_n.alloc(N.pcap));
     CK(N.pend_v.alloc(N.pcap));
     CK(N.pair.alloc(N.paircap));
@@ -1171,7 +1170,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
     v = NetView{};
     if (!learned || !N.ctr.p) continue;
     v.row = N.row.p; v.cnt = N.cnt.p; v.qcap = N.qcap;
-    v.pend_g = N.pend_g.p; v.pend_n = N.pend_n.p; v.pend_v = N.pend_v.p; v.pcap = N.pcap;
+    v.pend_n = N.pend_n.p; v.pend_v = N.pend_v.p; v.pcap = N.pcap;
     v.pair = N.pair.p; v.paircap = N.paircap; v.ctr = N.ctr.p;
   }
   return a;

@@ -1384,12 +1384,13 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
       if ((m >> lane) & 1u) {
         const int rank = __popc(m & lanemask_lt());
         const int idx = pstart + off + rank;
-        Q.pend_g[idx] = make_float4(gx, gy, gz, F.T);
-        Q.pend_n[idx] = ni | (edge ? (int)0x80000000u : 0);
+        Q.pend_n[idx] = ni;
         const int r = base + rank;
         if (r < Q.qcap) {
-          Q.row[(size_t)sh * Q.qcap + r] =
-              make_float4(fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y), fmaf(l.z, F.ms, -F.mc.z), __int_as_float(idx));
+          float4* row = Q.row + 2 * ((size_t)sh * Q.qcap + r);
+          row[0] = make_float4(fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y), fmaf(l.z, F.ms, -F.mc.z),
+                               __int_as_float(idx | (edge ? (int)0x80000000u : 0)));
+          row[1] = make_float4(gx, gy, gz, F.T);
         } else {
           atomicOr(&a.status->flags, OVF_NET);
           atomicMax(&a.status->need_netq, r + 1);
@@ -1570,27 +1571,45 @@ __global__ void __launch_bounds__(MLP_TILE) k_net_screen(StepArgs a, int li) {
   mlp_tc_setup(T);
   unsigned evals = 0, looks = 0;
   bool ok = true;
-  for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+  // tile t's shape and this thread's row; the row of the CTA's next tile is loaded while
+  // the current one runs
+  auto shape_of = [&](int t) {
     int sh = 0;
     while (s_pre[sh + 1] <= t) ++sh;
-    if (T->staged != sh) mlp_tc_stage(T, a.mlp_inf[sh], sh);
-    const int rows = min(Q.cnt[sh], Q.qcap);
+    return sh;
+  };
+  auto load_row = [&](int t, int sh, float4& u, float4& g) {
     const int r = (t - s_pre[sh]) * MLP_TILE + threadIdx.x;
-    const bool act = r < rows;
-    const float4 u = act ? Q.row[(size_t)sh * Q.qcap + r] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const int idx = __float_as_int(u.w);
-    // the grid test's operands are fetched before the network runs (its 16-byte cell load
-    // is then in flight during layer 1 and the MMA); the test is applied only to the
-    // nodes the network keeps
-    const int nflag = act ? Q.pend_n[idx] : -1;
-    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t < tiles && r < min(Q.cnt[sh], Q.qcap)) {
+      const float4* row = Q.row + 2 * ((size_t)sh * Q.qcap + r);
+      u = row[0];
+      g = row[1];
+    } else {
+      u = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+      g = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  int t = blockIdx.x, sh = shape_of(t);
+  float4 u, g;
+  load_row(t, sh, u, g);
+  while (t < tiles && ok) {
+    if (T->staged != sh) mlp_tc_stage(T, a.mlp_inf[sh], sh);
+    const int tag = __float_as_int(u.w);
+    const bool act = tag != -1;
+    const bool edge = act && tag < 0;
+    const int idx = tag & 0x7fffffff;
+    // the grid test's 16-byte cell load is in flight during layer 1 and the MMA; the
+    // test is applied only to the nodes the network keeps
     uint4 cell = make_uint4(0u, 0u, 0u, 0u);
-    if (nflag >= 0) {
-      g = Q.pend_g[idx];
+    if (act && !edge) {
       const int3 gs = a.S.gsize[sh];
       cell = phi16_cell(a.S.cell16 + a.S.cell_off[sh], gs.x - 1, (gs.x - 1) * (gs.y - 1), g.x, g.y, g.z);
     }
     mlp_tc_layer1(T, u.x, u.y, u.z);
+    const float4 gc = g;
+    const int tn = t + gridDim.x;
+    const int shn = tn < tiles ? shape_of(tn) : sh;
+    load_row(tn, shn, u, g);
     ok = mlp_tc_mma(T);
     const float y = mlp_tc_output(T);
     if (act) {
@@ -1598,8 +1617,8 @@ __global__ void __launch_bounds__(MLP_TILE) k_net_screen(StepArgs a, int li) {
       if (ok && !(y * __ldg(&a.mlp_norm[sh].r_over_h) > __ldg(&a.mlp_band[sh]))) {
         // kept by the network: the plain screen's grid test decides (not within the error
         // of the grid boundary, where the FP64 test decides)
-        if (nflag >= 0) {
-          may = !(phi16_interp<SDFK>(cell, g.x, g.y, g.z) > g.w);
+        if (!edge) {
+          may = !(phi16_interp<SDFK>(cell, gc.x, gc.y, gc.z) > gc.w);
           ++looks;
         }
       } else if (ok) {
@@ -1608,6 +1627,8 @@ __global__ void __launch_bounds__(MLP_TILE) k_net_screen(StepArgs a, int li) {
       Q.pend_v[idx] = may;
       ++evals;
     }
+    t = tn;
+    sh = shn;
   }
   if (!ok && threadIdx.x == 0) atomicAdd(&a.status->errors, 1);
   if (a.screen_stats) {
@@ -1699,8 +1720,10 @@ void launch_net_k(const StepArgs& a, int li, cudaStream_t s) {
     cudaFuncSetAttribute(k_net_screen<SDFK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = smem;
   }
-  // four CTAs per SM: 4 x 64 tensor-memory columns, the other launch's pass fits beside it
-  k_net_screen<SDFK><<<num_sms() * 4, MLP_TILE, smem, s>>>(a, li);
+  // eight CTAs per SM (8 x 64 = all 512 tensor-memory columns, 8 x 27 KB of shared
+  // memory): a CTA that finds no free columns (the other launch's pass beside it) waits
+  // in tcgen05.alloc until a CTA on its SM has finished
+  k_net_screen<SDFK><<<num_sms() * 8, MLP_TILE, smem, s>>>(a, li);
 }
 void launch_net_screen(const StepArgs& a, int li, cudaStream_t s) {
   if (!a.mlp_inf || a.P.n <= 0) return;

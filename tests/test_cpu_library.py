@@ -112,3 +112,31 @@ def test_compat_launchers_exported(lsdem):
     assert len(names) == 5
     for n in names:
         assert hasattr(lsdem.lib, n), f"{n} declared in include/lsdem_compat.h but not exported"
+
+
+def test_host_model_of_a_scene_equals_the_solvers(lsdem):
+    """The oracle model built on the host from a scene dict (model_from_scene: the reference
+    arm of the benchmark prepares its sample without the CUDA library) holds the same
+    per-particle constants as the solver's set-up (lsdem_add_particles, LSParticle.h:115-212)."""
+    from lsdem_b200 import scenes
+    ora = load_oracle()
+    T = scenes.unit_templates(n_grid=12, n_nodes=60)
+    rng = np.random.default_rng(3)
+    n = 40
+    tm = []
+    for t in T:
+        mp = lsdem.mass_properties(t["sdf"], t["size"], t["origin"], t["spacing"], 1.0)
+        tm.append(dict(t, nodes=t["nodes"] - mp["centroid"], origin=t["origin"] - mp["centroid"]))
+    sc = {"templates": tm, "shape": rng.integers(0, 4, n).astype(np.int32), "scale": rng.uniform(1e-3, 3e-3, n),
+          "pos": rng.uniform(0, 0.05, (n, 3)), "quat": scenes.random_quaternions(rng, n), "vel": np.zeros((n, 3)),
+          "inv_mass": rng.uniform(1, 2, n), "inv_inertia": rng.uniform(1, 2, (n, 6)), "kn": 1e5, "ks": 8e4,
+          "mu": 0.5, "e": 0.6, "min": np.zeros(3), "max": np.full(3, 0.05), "gravity": np.zeros(3), "periodic": 0,
+          "walls": [scenes.plane_wall(0.05, [0.025, 0.025, 0.0])]}
+    sv = lsdem.Solver()
+    scenes.load_polydisperse(sv, sc)
+    pp = sv.particle_params()
+    m = ora.model_from_scene(sc)["particles"]
+    for k in ("radius", "origin", "invh", "scale", "kn", "ks", "mu", "e"):
+        assert np.array_equal(np.asarray(m[k]), pp[k]), k
+    assert np.allclose(m["quat"], sv.state()["quat"], rtol=0, atol=1e-15)
+    sv.close()
