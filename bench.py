@@ -59,7 +59,7 @@ ROOT = Path(__file__).resolve().parent
 FORMS = {"fp32-bf16": 2, "fp32-fp16": 1, "fp64": 0, "fp32-bf16-learned": 2}
 DTYPE = {"fp32-bf16": "f32 screen on bf16 SDF, f64 contacts", "fp32-fp16": "f32 screen on fp16 SDF, f64 contacts",
          "fp64": "f64", "fp32-bf16-learned": "bf16 network + f32 screen on bf16 SDF, f64 contacts"}
-LEARN = {"iterations": 4000, "batch": 4096, "samples": 1 << 17, "lr": 3e-3}
+LEARN = {"iterations": 12000, "batch": 4096, "samples": 1 << 17, "lr": 3e-3}
 
 
 def _package():
@@ -108,10 +108,6 @@ B_PAIR = 236
 B_CONTACT = 56
 B_PARTICLE_SCREEN = 72
 B_PAIR_SCREEN = 120
-# DRAM bytes (read + write) per k_screen_f launch, mean of the particle-pair and image
-# launches, from one ncu capture of the default workload in the FP32/BF16 form
-# (profiles/k_screen_f_polydisperse100k_dram.md); other workloads and forms report null.
-SCREEN_TRAFFIC_DEFAULT = (22.89e6 + 0.22e6 + 11.57e6) / 2
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
 # What bounds the screen, from an ncu capture of k_screen_f (particle pairs, FP32/BF16 form)
@@ -755,14 +751,15 @@ def main():
         else:
             kernel = "k_screen_f"
             bytes_launch = (B_PARTICLE_SCREEN * n * launches_per_step + B_PAIR_SCREEN * pairs) / launches_per_step
-        traffic = (SCREEN_TRAFFIC_DEFAULT if (args.workload == "polydisperse" and args.particles == 100_000
-                                              and args.form == "fp32-bf16") else None)
+        traffic = None
         achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
         b_step = B_STEP_PARTICLE * n + B_CONTACT * stats["contacts"] + 16 * pairs
         ms_step = head["ms"] / args.steps
         forms[args.form] = dict(forms.get(args.form, {}), value=value, ms_per_step=ms_step,
                                 warm_l2={"value": n * world * args.steps / (head["warm_ms"] * 1e-3),
                                          "ms_per_step": head["warm_ms"] / args.steps})
+        if "training" in head:
+            forms[args.form]["training"] = head["training"]
         per_s = world * args.steps / (head["ms"] * 1e-3)  # steps per second, all ranks
         scr = head.get("screen") or {}
         plain = forms.get("fp64", {}).get("value")

@@ -61,21 +61,24 @@ struct ShapeView {
   const float* lip;             // 2 per shape, in spacings: largest |phi| difference of grid
                                 //   neighbours; largest gradient-norm bound of a grid cell
   // support tables (cube map of SUP_M x SUP_M cells per face, per shape, template units,
-  // rounded up): nodes, and the grid points bounding the solid (cells with phi <= 0)
-  const float* sup_n;
-  const float* sup_s;
+  // rounded up): per cell the values at its four corner directions (p, q), (p + 1, q),
+  // (p, q + 1), (p + 1, q + 1) of the largest projection of the nodes (sup_n) and of the
+  // points bounding the solid (sup_s, where the trilinear phi can be <= 0)
+  const float4* sup_n;
+  const float4* sup_s;
   const float* sup_r;           // per shape: largest |p| over the sup_s points, rounded up
 };
 
 // Arithmetic form of the narrowphase and contact forces.
 enum { PREC_FP64 = 0, PREC_FP32_FP16 = 1, PREC_FP32_BF16 = 2 };
 
-// Support tables: cells per cube-map face side.
+// Support tables: cells per cube-map face side; corner directions of the cells.
 constexpr int SUP_M = 24;
 constexpr int SUP_CELLS = 6 * SUP_M * SUP_M;
+constexpr int SUP_VERTS = 6 * (SUP_M + 1) * (SUP_M + 1);
 void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
-                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, float* sup_r,
-                           cudaStream_t s);
+                           const double3* pts, const long long* pts_off, float* vtx, float4* sup_n, float4* sup_s,
+                           float* sup_r, cudaStream_t s);
 
 // A set of rigid bodies (particles or walls).
 struct BodyView {

@@ -54,7 +54,8 @@ __device__ __forceinline__ float dsilu_f(float x) {
 
 }  // namespace
 
-// Samples of all shapes: samples[s * S + k] = (u.x, u.y, u.z, phi / R).
+// Samples of all shapes: samples[s * S + k] = (u.x, u.y, u.z, phi / R clipped to
+// [MLP_CLIP_LO, MLP_CLIP_HI]).
 __global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, float4* samples) {
   const int s = blockIdx.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -82,7 +83,8 @@ __global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, fl
   }
   const double phi = grid_phi(D.sdf + D.sdf_off[s], gs, o, h, p);
   samples[(size_t)s * S + k] = make_float4((float)((p.x - nm.cx) / nm.R), (float)((p.y - nm.cy) / nm.R),
-                                           (float)((p.z - nm.cz) / nm.R), (float)(phi / nm.R));
+                                           (float)((p.z - nm.cz) / nm.R),
+                                           (float)fmin(fmax(phi / nm.R, (double)MLP_CLIP_LO), (double)MLP_CLIP_HI));
 }
 
 // Block-partial gradients of the mean squared error over points of the batch:
@@ -224,10 +226,11 @@ __global__ void k_mlp_pack(const float* __restrict__ params, MlpInfer* out) {
 // Error of each shape's network, with the inference code of the narrowphase,
 // over validation points: every grid node of the box, then S2 further points
 // drawn like the training data with another seed (template units).
-// err_bits[2 s]: largest |phi_net - phi_grid|; err_bits[2 s + 1]: largest
-// phi_net - phi_grid over the points with phi_grid <= delta[s] (the one-sided
-// bound that makes a rejection by the network safe). Float bits of running
-// maxima of non-negative values (which order as integers).
+// err_bits[2 s]: largest |phi_net - clip(phi_grid)|; err_bits[2 s + 1]: largest
+// phi_net - clip(phi_grid) over the points with phi_grid <= delta[s] (the one-sided
+// bound that makes a rejection by the network safe; clip as the training target, in
+// units of R). Float bits of running maxima of non-negative values (which order as
+// integers).
 __global__ void __launch_bounds__(MLP_TILE) k_mlp_validate(MlpShapeData D, const MlpInfer* __restrict__ inf, int S2,
                                                            unsigned long long seed, const float* __restrict__ delta,
                                                            unsigned* err_bits, int* fail) {
@@ -271,8 +274,9 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_validate(MlpShapeData D, const
     ok = mlp_tc_mma(T);
     const float net = mlp_tc_output(T) * nm.R;
     if (act && ok) {
-      emax = fmaxf(emax, fabsf(net - (float)phi));
-      if (phi <= (double)dlt) ein = fmaxf(ein, net - (float)phi);
+      const float tgt = (float)fmin(fmax(phi, (double)(MLP_CLIP_LO * nm.R)), (double)(MLP_CLIP_HI * nm.R));
+      emax = fmaxf(emax, fabsf(net - tgt));
+      if (phi <= (double)dlt) ein = fmaxf(ein, net - tgt);
     }
   }
   if (!ok && threadIdx.x == 0) atomicExch(fail, 1);

@@ -55,6 +55,14 @@ struct MlpNorm {
   float r_over_h;        // R / template grid spacing (phi / R -> phi / spacing)
 };
 
+// Training target: phi / R clipped to [MLP_CLIP_LO, MLP_CLIP_HI]. A rejection only needs
+// the network to tell phi > delta (a few per cent of R) apart, so the deep interior and the
+// far corners of the grid box are flattened; the one-sided error is measured against the
+// clipped value, and clip(phi) > delta implies phi > delta since delta lies inside the clip
+// range.
+constexpr float MLP_CLIP_LO = -0.25f;
+constexpr float MLP_CLIP_HI = 0.5f;
+
 // Points per tensor-core tile (= threads of an inference CTA) and TMEM columns.
 constexpr int MLP_TILE = 128;
 constexpr int MLP_TMEM_COLS = 64;

@@ -403,7 +403,8 @@ struct lsdem_solver {
   // support tables of the shapes (pair separation test of the candidate search)
   DArr<double3> sup_pts;
   DArr<long long> sup_off;
-  DArr<float> sup_n, sup_s, sup_r;
+  DArr<float4> sup_n, sup_s;
+  DArr<float> sup_r, sup_vtx;
   int nbr_cap = 24;
   float skin = 0.f;
   double move2 = 0.;
@@ -826,17 +827,50 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
   {
-    // support tables: per shape, the grid points that bound the cells with a corner
-    // phi <= 0 (those cells dilated by one point in every direction, then only the
-    // points with a 6-neighbour outside the set), template units
+    // support tables: per shape, points whose convex hull holds every point where the
+    // trilinear phi is <= 0, template units. The grid is refined by two (points at half
+    // spacings): phi restricted to one of the eight sub-cells of a cell is trilinear
+    // with the sub-cell's corner values, and a multilinear function takes its minimum
+    // over a box at a corner, so a point with phi <= 0 lies in a sub-cell with a corner
+    // phi <= 0. Those corners are marked (each with a tolerance above the rounding of
+    // its interpolation), the marks dilated by one refined point in every direction
+    // (the corners of every such sub-cell), and only the points with a 6-neighbour
+    // outside the set kept (the largest projection of a lattice set is reached there).
     std::vector<double3> pts;
     std::vector<long long> poff{0};
     for (const ShapeHost& sh : s->shapes) {
-      const int nx = sh.size[0], ny = sh.size[1], nz = sh.size[2];
+      const int gx = sh.size[0], gy = sh.size[1], gz = sh.size[2];
+      const int nx = 2 * gx - 1, ny = 2 * gy - 1, nz = 2 * gz - 1;
       const size_t N = (size_t)nx * ny * nz;
       auto id = [&](int x, int y, int z) { return (size_t)x + (size_t)nx * (y + (size_t)ny * z); };
-      std::vector<uint8_t> m(N), t(N);
-      for (size_t k = 0; k < N; ++k) m[k] = sh.sdf[k] <= 0.;
+      auto gv = [&](int x, int y, int z) { return sh.sdf[(size_t)x + (size_t)gx * (y + (size_t)gy * z)]; };
+      std::vector<uint8_t> m(N, 0), t(N);
+      for (int z = 0; z + 1 < gz; ++z)
+        for (int y = 0; y + 1 < gy; ++y)
+          for (int x = 0; x + 1 < gx; ++x) {
+            double c[8], lo = 1e300, hi = -1e300, mag = 0.;
+            for (int k = 0; k < 8; ++k) {
+              c[k] = gv(x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
+              lo = std::min(lo, c[k]);
+              hi = std::max(hi, c[k]);
+              mag = std::max(mag, std::fabs(c[k]));
+            }
+            const double tol = 1e-12 * mag;
+            if (lo > tol) continue;  // phi > 0 on the whole cell
+            for (int k = 0; k < 27; ++k) {
+              const int i = k % 3, j = (k / 3) % 3, l = k / 9;
+              double v;
+              if (hi <= tol) {
+                v = lo;  // phi <= 0 on the whole cell
+              } else {
+                const double fx = 0.5 * i, fy = 0.5 * j, fz = 0.5 * l;
+                const double c00 = c[0] * (1 - fx) + c[1] * fx, c10 = c[2] * (1 - fx) + c[3] * fx;
+                const double c01 = c[4] * (1 - fx) + c[5] * fx, c11 = c[6] * (1 - fx) + c[7] * fx;
+                v = (c00 * (1 - fy) + c10 * fy) * (1 - fz) + (c01 * (1 - fy) + c11 * fy) * fz;
+              }
+              if (v <= tol) m[id(2 * x + i, 2 * y + j, 2 * z + l)] = 1;
+            }
+          }
       // separable dilation by one point along x, y, z (the 27-neighbourhood)
       for (int ax = 0; ax < 3; ++ax) {
         for (int z = 0; z < nz; ++z)
@@ -858,7 +892,8 @@ void initialize(lsdem_solver* s) {
             if (!edge && m[id(x - 1, y, z)] && m[id(x + 1, y, z)] && m[id(x, y - 1, z)] && m[id(x, y + 1, z)] &&
                 m[id(x, y, z - 1)] && m[id(x, y, z + 1)])
               continue;
-            pts.push_back(make_double3(sh.origin[0] + sh.h * x, sh.origin[1] + sh.h * y, sh.origin[2] + sh.h * z));
+            pts.push_back(make_double3(sh.origin[0] + 0.5 * sh.h * x, sh.origin[1] + 0.5 * sh.h * y,
+                                       sh.origin[2] + 0.5 * sh.h * z));
           }
       poff.push_back((long long)pts.size());
     }
@@ -868,8 +903,9 @@ void initialize(lsdem_solver* s) {
     CK(s->sup_n.alloc((size_t)ns * SUP_CELLS));
     CK(s->sup_s.alloc((size_t)ns * SUP_CELLS));
     CK(s->sup_r.alloc((size_t)std::max(ns, 1)));
+    CK(s->sup_vtx.alloc((size_t)2 * ns * SUP_VERTS));
     launch_support_tables(ns, s->s_node_pos.p, s->s_node_off.p, s->s_node_cnt.p, s->sup_pts.p, s->sup_off.p,
-                          s->sup_n.p, s->sup_s.p, s->sup_r.p, st);
+                          s->sup_vtx.p, s->sup_n.p, s->sup_s.p, s->sup_r.p, st);
     CK(cudaGetLastError());
   }
   {

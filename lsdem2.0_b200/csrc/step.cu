@@ -219,83 +219,82 @@ __global__ void k_pack_cells(StepArgs a, const int* __restrict__ idx) {
 
 // ---------------------------------------------------------------------------
 // Support tables and the separation test of a candidate pair.
-// A direction u falls in one cell of a cube map (face of the largest |component|,
-// then SUP_M x SUP_M cells of the face's gnomonic square). For every direction v in
-// a cell, v . p <= c . p + delta |p|, where c is the cell's centre direction and
-// delta the largest distance from c to the cell (reached at a corner: v . c is
-// quasi-concave over the square). The tables hold, per shape and cell, the largest
-// c . p + delta |p| over the template's surface nodes (sup_n) and over the grid
-// points of every cell with a corner phi <= 0 (sup_s; the points where a trilinear
-// phi can be <= 0 lie in those cells, and the maximum of this convex function over
-// them is reached at points with a 6-neighbour outside the set). delta carries 1e-5
-// beyond its exact value for the FP32 rounding of the direction (pair_separated).
-// Unit direction of face f at gnomonic coordinates (p, q).
-LD double3 sup_dir(int f, double p, double q) {
+// The support of a point set P, h(w) = max over p in P of w . p, is convex and
+// positively homogeneous in w. A direction u falls on one face of a cube map (the axis
+// of its largest |component|, m = that |component|), where w = u / m = (+-1, p, q) in
+// the face's coordinates (gnomonic square [-1, 1]^2, SUP_M x SUP_M cells). Restricted
+// to the face's plane, h is convex in (p, q), so on each half of a cell (the triangles
+// below and above its (p + 1, q) - (p, q + 1) diagonal) it lies below the linear
+// interpolation of its values at the triangle's corners. The tables hold, per shape,
+// those values at the cube map's vertices (rounded up), packed four per cell; the
+// support along the unit direction u / |u| is h(w) m / |u|. Point sets: the template's
+// surface nodes (sup_n) and points whose convex hull holds every point where B's
+// trilinear phi can be <= 0 (sup_s; built by the host from the grid refined by two).
+
+// Face coordinates of vertex (i, j) of face f as an unnormalised direction.
+LD double3 sup_vertex(int f, int i, int j) {
   const double sg = (f & 1) ? -1.0 : 1.0;
-  double3 v = f < 2 ? d3(sg, p, q) : (f < 4 ? d3(q, sg, p) : d3(p, q, sg));
-  return (1.0 / sqrt(dot(v, v))) * v;
+  const double p = -1.0 + 2.0 * i / SUP_M, q = -1.0 + 2.0 * j / SUP_M;
+  return f < 2 ? d3(sg, p, q) : (f < 4 ? d3(q, sg, p) : d3(p, q, sg));
 }
 
-// One warp per (shape, cell): the two table entries.
-__global__ void k_support_tables(int nshapes, const double3* __restrict__ node_pos, const int* __restrict__ node_off,
-                                 const int* __restrict__ node_cnt, const double3* __restrict__ pts,
-                                 const long long* __restrict__ pts_off, float* __restrict__ sup_n,
-                                 float* __restrict__ sup_s, float* __restrict__ sup_r) {
+// One warp per (shape, table, vertex): the largest projection, rounded up.
+__global__ void k_support_vertices(int nshapes, const double3* __restrict__ node_pos, const int* __restrict__ node_off,
+                                   const int* __restrict__ node_cnt, const double3* __restrict__ pts,
+                                   const long long* __restrict__ pts_off, float* __restrict__ vtx,
+                                   float* __restrict__ sup_r) {
   const int lane = threadIdx.x & 31;
   const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= (long long)nshapes * SUP_CELLS) return;
-  const int sh = (int)(w / SUP_CELLS), cell = (int)(w % SUP_CELLS);
-  const int f = cell / (SUP_M * SUP_M), j = (cell / SUP_M) % SUP_M, i = cell % SUP_M;
-  const double h = 2.0 / SUP_M;
-  const double p0 = -1.0 + h * i, q0 = -1.0 + h * j;
-  const double3 c = sup_dir(f, p0 + 0.5 * h, q0 + 0.5 * h);
-  double delta = 0.;
-  for (int k = 0; k < 4; ++k) {
-    const double3 v = sup_dir(f, p0 + h * (k & 1), q0 + h * (k >> 1));
-    const double3 e = v - c;
-    delta = fmax(delta, sqrt(dot(e, e)));
+  if (w >= 2LL * nshapes * SUP_VERTS) return;
+  const int sh = (int)(w / (2 * SUP_VERTS)), tab = (int)((w / SUP_VERTS) & 1), v = (int)(w % SUP_VERTS);
+  const int f = v / ((SUP_M + 1) * (SUP_M + 1)), j = (v / (SUP_M + 1)) % (SUP_M + 1), i = v % (SUP_M + 1);
+  const double3 c = sup_vertex(f, i, j);
+  double mx = -1e300;
+  if (tab == 0) {
+    for (int k = lane; k < node_cnt[sh]; k += 32) mx = fmax(mx, dot(c, node_pos[node_off[sh] + k]));
+  } else {
+    for (long long k = pts_off[sh] + lane; k < pts_off[sh + 1]; k += 32) mx = fmax(mx, dot(c, pts[k]));
   }
-  delta = delta * (1.0 + 1e-9) + 1e-5;
-  double mn = -1e30, ms = -1e30;
-  for (int k = lane; k < node_cnt[sh]; k += 32) {
-    const double3 p = node_pos[node_off[sh] + k];
-    mn = fmax(mn, dot(c, p) + delta * sqrt(dot(p, p)));
-  }
-  for (long long k = pts_off[sh] + lane; k < pts_off[sh + 1]; k += 32) {
-    const double3 p = pts[k];
-    ms = fmax(ms, dot(c, p) + delta * sqrt(dot(p, p)));
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    mn = fmax(mn, __shfl_xor_sync(FULL, mn, o));
-    ms = fmax(ms, __shfl_xor_sync(FULL, ms, o));
-  }
-  if (cell == 0) {  // the largest |p| of the solid's points
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+  if (tab == 1 && v == 0) {  // the largest |p| of the solid's points
     double r = 0.;
     for (long long k = pts_off[sh] + lane; k < pts_off[sh + 1]; k += 32) r = fmax(r, sqrt(dot(pts[k], pts[k])));
     for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(FULL, r, o));
     if (lane == 0) sup_r[sh] = __double2float_ru(r * (1.0 + 1e-9));
   }
-  if (lane == 0) {
-    // relative 1e-9 covers the rounding of the sums above
-    sup_n[w] = mn > -1e29 ? __double2float_ru(mn + 1e-9 * fabs(mn) + 1e-30) : -1e30f;
-    sup_s[w] = ms > -1e29 ? __double2float_ru(ms + 1e-9 * fabs(ms) + 1e-30) : -1e30f;
-  }
+  // relative 1e-9 covers the rounding of the dot products and of the vertex coordinates
+  if (lane == 0) vtx[w] = mx > -1e299 ? __double2float_ru(mx + 1e-9 * fabs(mx) + 1e-30) : -1e30f;
+}
+
+// One thread per (shape, table, cell): its four corner values in one float4.
+__global__ void k_support_pack(int nshapes, const float* __restrict__ vtx, float4* __restrict__ sup_n,
+                               float4* __restrict__ sup_s) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2LL * nshapes * SUP_CELLS) return;
+  const int sh = (int)(t / (2 * SUP_CELLS)), tab = (int)((t / SUP_CELLS) & 1), cell = (int)(t % SUP_CELLS);
+  const int f = cell / (SUP_M * SUP_M), j = (cell / SUP_M) % SUP_M, i = cell % SUP_M;
+  const float* V = vtx + ((size_t)sh * 2 + tab) * SUP_VERTS + (size_t)f * (SUP_M + 1) * (SUP_M + 1);
+  const float4 c = make_float4(V[j * (SUP_M + 1) + i], V[j * (SUP_M + 1) + i + 1], V[(j + 1) * (SUP_M + 1) + i],
+                               V[(j + 1) * (SUP_M + 1) + i + 1]);
+  (tab == 0 ? sup_n : sup_s)[(size_t)sh * SUP_CELLS + cell] = c;
 }
 
 void launch_support_tables(int nshapes, const double3* node_pos, const int* node_off, const int* node_cnt,
-                           const double3* pts, const long long* pts_off, float* sup_n, float* sup_s, float* sup_r,
-                           cudaStream_t s) {
-  const long long warps = (long long)nshapes * SUP_CELLS;
+                           const double3* pts, const long long* pts_off, float* vtx, float4* sup_n, float4* sup_s,
+                           float* sup_r, cudaStream_t s) {
+  const long long warps = 2LL * nshapes * SUP_VERTS;
   if (warps <= 0) return;
-  k_support_tables<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(nshapes, node_pos, node_off, node_cnt, pts,
-                                                                       pts_off, sup_n, sup_s, sup_r);
+  k_support_vertices<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(nshapes, node_pos, node_off, node_cnt, pts,
+                                                                         pts_off, vtx, sup_r);
+  const long long cells = 2LL * nshapes * SUP_CELLS;
+  k_support_pack<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(nshapes, vtx, sup_n, sup_s);
 }
 
 // The separation test runs in FP32 on the packed records of the candidate search, with
 // explicitly rounded operations (the list filter and the walk of k_candidates inline it
-// at two places; explicit rounding keeps them deciding every pair alike). The cube-map
-// cell of a direction depends only on its ratios, so the unnormalised centre difference
-// is rotated into each body frame.
+// at two places; explicit rounding keeps them deciding every pair alike). Only the
+// direction of the centre difference matters, so it is rotated into each body frame
+// unnormalised.
 LD float3 rot_inv_f(float3 v, float4 q) {
   const float w = q.x, a = -q.y, b = -q.z, c = -q.w;
   const float tx = __fmul_rn(2.0f, __fmaf_rn(b, v.z, -__fmul_rn(c, v.y)));
@@ -305,31 +304,42 @@ LD float3 rot_inv_f(float3 v, float4 q) {
                      __fadd_rn(__fmaf_rn(w, ty, v.y), __fmaf_rn(c, tx, -__fmul_rn(a, tz))),
                      __fadd_rn(__fmaf_rn(w, tz, v.z), __fmaf_rn(a, ty, -__fmul_rn(b, tx))));
 }
-LD int sup_cell_f(float3 u) {
+// Upper bound of h(u / m) from the table tab of one shape; m = the largest |component|
+// of u (0 when u = 0).
+LD float sup_bound_f(const float4* __restrict__ tab, float3 u, float& m) {
   const float ax = fabsf(u.x), ay = fabsf(u.y), az = fabsf(u.z);
   int f;
-  float m, p, q;
+  float p, q;
   if (ax >= ay && ax >= az) { f = u.x >= 0.f ? 0 : 1; m = ax; p = u.y; q = u.z; }
   else if (ay >= az) { f = u.y >= 0.f ? 2 : 3; m = ay; p = u.z; q = u.x; }
   else { f = u.z >= 0.f ? 4 : 5; m = az; p = u.x; q = u.y; }
-  if (!(m > 0.f)) return 0;
+  if (!(m > 0.f)) {
+    m = 0.f;
+    return 0.f;
+  }
   const float r = __frcp_rn(m);
-  int i = (int)floorf(__fmul_rn(__fmaf_rn(p, r, 1.0f), 0.5f * SUP_M));
-  int j = (int)floorf(__fmul_rn(__fmaf_rn(q, r, 1.0f), 0.5f * SUP_M));
-  i = i < 0 ? 0 : (i > SUP_M - 1 ? SUP_M - 1 : i);
-  j = j < 0 ? 0 : (j > SUP_M - 1 ? SUP_M - 1 : j);
-  return (f * SUP_M + j) * SUP_M + i;
+  const float x = __fmul_rn(__fmaf_rn(p, r, 1.0f), 0.5f * SUP_M);
+  const float y = __fmul_rn(__fmaf_rn(q, r, 1.0f), 0.5f * SUP_M);
+  const int i = min(max((int)floorf(x), 0), SUP_M - 1), j = min(max((int)floorf(y), 0), SUP_M - 1);
+  const float s = fminf(fmaxf(__fsub_rn(x, (float)i), 0.f), 1.f), t = fminf(fmaxf(__fsub_rn(y, (float)j), 0.f), 1.f);
+  const float4 c = __ldg(tab + (f * SUP_M + j) * SUP_M + i);
+  if (__fadd_rn(s, t) <= 1.0f) return __fmaf_rn(s, __fsub_rn(c.y, c.x), __fmaf_rn(t, __fsub_rn(c.z, c.x), c.x));
+  return __fmaf_rn(__fsub_rn(1.0f, s), __fsub_rn(c.z, c.w), __fmaf_rn(__fsub_rn(1.0f, t), __fsub_rn(c.y, c.w), c.w));
 }
 
 // Separating-axis test of the pair (A, B) along the line of centres u: every node of
-// A projects onto u at most scale_A sup_n(A, R_A^T u) beyond x_A, and every point
-// where B's interpolated phi is <= 0 at least scale_B sup_s(B, -R_B^T u) before x_B;
-// if the two reaches sum to less than |x_B - x_A|, no node of A can be inside B and the
-// pair has no contact. Margins: the FP32 centres differ from the FP64 ones by at most
-// 2^-24 of each coordinate, so the distance by 1.2e-7 (n1 + D) and the direction by
-// 3e-7 (n1 + D) / D, plus 2e-6 for the FP32 orientation and rotation; a direction error
-// e moves a support by at most e times the set's largest |p| (the bounding radius for
-// A's nodes, scale_B sup_r for B's solid). Each margin is taken several times over.
+// A projects onto u at most scale_A h_n(A, R_A^T u) beyond x_A, and every point where
+// B's interpolated phi is <= 0 at least scale_B h_s(B, -R_B^T u) before x_B; if the two
+// reaches sum to less than |x_B - x_A|, no node of A can be inside B and the pair has no
+// contact. Margins: the FP32 centres differ from the FP64 ones by at most 2^-24 of each
+// coordinate, so the distance by 1.2e-7 (n1 + D) and the direction by 3e-7 (n1 + D) / D;
+// 2e-6 for the FP32 orientation and rotation, and 2e-6 for the rounding of the face
+// coordinates and of the interpolation (the interpolated plane point moves by a few
+// 1e-7, and the values, at most sqrt(3) times the set's largest |p|, round by a few
+// ulps); a direction error e moves a support by at most e times the set's largest |p|
+// (the bounding radius for A's nodes, scale_B sup_r for B's solid). The rotation keeps
+// |R^T u| = |u| within 1e-6, covered by the relative 1e-5. Each margin is taken several
+// times over.
 LD bool pair_separated(const StepArgs& a, float4 pa, float n1a, float4 qa, float scA, int shA, float4 pb, float4 qb,
                        float scB, int shB) {
   const float dx = __fsub_rn(pb.x, pa.x), dy = __fsub_rn(pb.y, pa.y), dz = __fsub_rn(pb.z, pa.z);
@@ -337,12 +347,13 @@ LD bool pair_separated(const StepArgs& a, float4 pa, float n1a, float4 qa, float
   if (!(D2 > 0.f)) return false;
   const float3 ua = rot_inv_f(make_float3(dx, dy, dz), qa);
   const float3 ub = rot_inv_f(make_float3(-dx, -dy, -dz), qb);
-  const float hA = __ldg(a.S.sup_n + (size_t)shA * SUP_CELLS + sup_cell_f(ua));
-  const float hB = __ldg(a.S.sup_s + (size_t)shB * SUP_CELLS + sup_cell_f(ub));
-  const float reach = __fmaf_rn(scA, hA, __fmul_rn(scB, hB));
+  float ma, mb;
+  const float hA = sup_bound_f(a.S.sup_n + (size_t)shA * SUP_CELLS, ua, ma);
+  const float hB = sup_bound_f(a.S.sup_s + (size_t)shB * SUP_CELLS, ub, mb);
   const float D = __fsqrt_rn(D2);
+  const float reach = __fdiv_rn(__fmaf_rn(__fmul_rn(scA, ma), hA, __fmul_rn(__fmul_rn(scB, mb), hB)), D);
   const float n1 = __fadd_rn(n1a, __fadd_rn(__fadd_rn(fabsf(pb.x), fabsf(pb.y)), fabsf(pb.z)));
-  const float eps = __fadd_rn(__fdiv_rn(__fmul_rn(4e-7f, __fadd_rn(n1, D)), D), 4e-6f);
+  const float eps = __fadd_rn(__fdiv_rn(__fmul_rn(4e-7f, __fadd_rn(n1, D)), D), 8e-6f);
   const float rho = __fadd_rn(pa.w, __fmul_rn(scB, __ldg(a.S.sup_r + shB)));
   const float slack = __fmaf_rn(eps, rho, __fmaf_rn(1e-6f, n1, __fmul_rn(1e-5f, D)));
   return __fmul_rn(__fadd_rn(reach, slack), 1.0f + 1e-5f) < D;
@@ -1220,8 +1231,14 @@ LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd,
 //    segment p-q lies in the box, and along it phi / h changes by at most gmax
 //    per grid unit, so phi(q) - gmax (rad + sqrt(3) m) > 0 proves phi > 0 at
 //    every node of the cluster.
+//  With up != nullptr (learned form), *up receives an estimate of the largest phi / h
+//  over the cluster's nodes (phi at q plus gmax times the reach; +inf when phi at q is
+//  not looked up): where it is below the network's rejection threshold the network
+//  cannot reject any of them (an efficiency choice only: every node the network does not
+//  see takes the grid test).
 template <int KIND, int SDFK>
-LD bool cluster_may_hit_f(const PairF& F, float4 cn, float scA) {
+LD bool cluster_may_hit_f(const PairF& F, float4 cn, float scA, float* up = nullptr) {
+  if (up) *up = INFINITY;
   const float3 l = mulf(F.M, cn.x, cn.y, cn.z) + F.dB;
   const float rad = cn.w * scA * (1.0f + 1e-6f);
   if (KIND == KIND_PP) {
@@ -1239,7 +1256,9 @@ LD bool cluster_may_hit_f(const PairF& F, float4 cn, float scA) {
   const float qx = fminf(fmaxf(gx, m), F.ux - m), qy = fminf(fmaxf(gy, m), F.uy - m),
               qz = fminf(fmaxf(gz, m), F.uz - m);
   const float reach = (F.gmax * (radh + 2.8f * m) + 1e-6f) * F.Tq * (1.0f + 1e-6f);
-  return !(phi16<SDFK>(F, qx, qy, qz) > F.T + reach);
+  const float ph = phi16<SDFK>(F, qx, qy, qz);
+  if (up) *up = ph + reach;
+  return !(ph > F.T + reach);
 }
 
 LD SelfCtx self_ctx(const StepArgs& a, int A) {
@@ -1291,7 +1310,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   }
   __syncwarp();
   // second level: sub-clusters of 8 nodes of the surviving clusters, compacted in
-  // ascending order; chunk k of the node loop is sub-clusters 4k .. 4k + 3
+  // ascending order; chunk k of the node loop is sub-clusters 4k .. 4k + 3. Learned
+  // form: bit 15 marks a sub-cluster whose nodes the network cannot reject (their phi / h
+  // estimate is below its threshold); they take the grid test here.
   int nsub = 0;
   for (int j0 = 0; j0 < 4 * nsurv; j0 += 32) {
     const int j = j0 + lane;
@@ -1300,7 +1321,9 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
     if (j < 4 * nsurv) {
       sid = s_cl[j >> 2] * 4 + (j & 3);
       const float4 sp = __ldg(a.S.sub_sphere + 4 * cl0 + sid);
-      keep = sp.w >= 0.f && cluster_may_hit_f<KIND, SDFK>(F, sp, scA);
+      float up = INFINITY;
+      keep = sp.w >= 0.f && cluster_may_hit_f<KIND, SDFK>(F, sp, scA, LRN ? &up : nullptr);
+      if (LRN && up <= F.Tn) sid |= 0x8000;
     }
     const unsigned m = __ballot_sync(FULL, keep);
     if (keep) s_sub[nsub + __popc(m & lanemask_lt())] = (unsigned short)sid;
@@ -1313,93 +1336,120 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   auto node_of = [&](int k) {
     const int j = 4 * k + (lane >> 3);
     if (j >= nsub) return nn;
-    const int ni = s_sub[j] * 8 + (lane & 7);
+    const int ni = (s_sub[j] & 0x7fff) * 8 + (lane & 7);
     return ni < nn ? ni : nn;
   };
   int total = 0;
   if (LRN) {
-    // Learned form: every node the partner's bounds cannot reject goes to the network of
-    // the partner's shape (k_net_screen, tensor cores), which decides with the grid
-    // test of the nodes it keeps; here the nodes awaiting that verdict are recorded in
-    // node order for the pair (k_net_compact queues the survivors for the FP64 pass).
+    // Learned form: the nodes the partner's bounds cannot reject go to the network of the
+    // partner's shape (k_net_screen, tensor cores), which decides with the grid test of
+    // the nodes it keeps, unless their sub-cluster is marked (then the grid test runs
+    // here). A pair with network nodes records all its remaining nodes in node order as
+    // pending (the marked ones with a passing verdict already; k_net_compact queues the
+    // survivors for the FP64 pass); a pair without takes the plain screen's tail.
     const NetView& Q = a.net[li];
+    unsigned* s_dir = reinterpret_cast<unsigned*>(s_cl);  // the cluster list is spent
+    int tnet = 0, tdir = 0;
     for (int k = 0; k < nch; ++k) {
       const int ni = node_of(k);
+      const int j = 4 * k + (lane >> 3);
+      const bool marked = j < nsub && (s_sub[j] & 0x8000);
       cnt[4] += __popc(__ballot_sync(FULL, ni < nn));
-      bool need = false;
+      bool need = false, may = false, looked = false;
       if (ni < nn) {
         const float4 nd = __ldg(a.S.node_pos_f + n0 + ni);
-        const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
-        bool adm;
-        if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
-        else adm = window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) != 0;
-        const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
-        const float lo = fminf(gx, fminf(gy, gz));
-        const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
-        need = adm && !(lo < -F.eg || hi >= F.eg);
-      }
-      const unsigned m = __ballot_sync(FULL, need);
-      if (lane == 0) s_mask[k] = m;
-      total += __popc(m);
-    }
-    __syncwarp();
-    const SlotView& cur = slots_of<KIND>(a, false);
-    const size_t sidx = (size_t)A * cur.cap + slot;
-    if (lane == 0) {  // set here; k_contacts_f writes the segment of a pair with contacts
-      cur.seg_start[sidx] = 0;
-      cur.seg_cnt[sidx] = 0;
-    }
-    if (total == 0) return;
-    int pstart = 0, pi = 0;
-    bool ok = false;
-    if (lane == 0) {
-      pstart = atomicAdd(&Q.ctr[0], total);
-      pi = atomicAdd(&Q.ctr[1], 1);
-      ok = pstart + total <= Q.pcap && pi < Q.paircap;
-      if (!ok) {
-        atomicOr(&a.status->flags, OVF_NET);
-        const long long need = (long long)pstart + total;
-        atomicMax(&a.status->need_pend, (int)(need < 0x7fffffff ? need : 0x7fffffff));
-      }
-    }
-    pstart = __shfl_sync(FULL, pstart, 0);
-    pi = __shfl_sync(FULL, pi, 0);
-    ok = __shfl_sync(FULL, ok, 0);
-    if (!ok) return;
-    const int sh = F.pshape;
-    int off = 0;
-    for (int k = 0; k < nch; ++k) {
-      const unsigned m = s_mask[k];
-      if (m == 0u) continue;
-      const int ni = node_of(k);
-      const float4 nd = __ldg(a.S.node_pos_f + n0 + min(ni, nn - 1));
-      const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
-      const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
-      const float lo = fminf(gx, fminf(gy, gz));
-      const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
-      const bool edge = lo < F.eg || hi >= -F.eg;
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&Q.cnt[sh], __popc(m));
-      base = __shfl_sync(FULL, base, 0);
-      if ((m >> lane) & 1u) {
-        const int rank = __popc(m & lanemask_lt());
-        const int idx = pstart + off + rank;
-        Q.pend_n[idx] = ni;
-        const int r = base + rank;
-        if (r < Q.qcap) {
-          float4* row = Q.row + 2 * ((size_t)sh * Q.qcap + r);
-          row[0] = make_float4(fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y), fmaf(l.z, F.ms, -F.mc.z),
-                               __int_as_float(idx | (edge ? (int)0x80000000u : 0)));
-          row[1] = make_float4(gx, gy, gz, F.T);
+        if (marked) {
+          may = node_may_hit_f<KIND, SDFK>(a, xA, F, nd, looked);
         } else {
-          atomicOr(&a.status->flags, OVF_NET);
-          atomicMax(&a.status->need_netq, r + 1);
+          const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
+          bool adm;
+          if (KIND == KIND_PP) adm = !(l.x * l.x + l.y * l.y + l.z * l.z > F.R2);
+          else adm = window_state<KIND>(a, xA, mulf(F.RA, nd.x, nd.y, nd.z), F.n1w, F.key) != 0;
+          const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y), gz = fmaf(l.z, F.invh, F.cg.z);
+          const float lo = fminf(gx, fminf(gy, gz));
+          const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+          need = adm && !(lo < -F.eg || hi >= F.eg);
         }
       }
-      off += __popc(m);
+      cnt[3] += __popc(__ballot_sync(FULL, looked));
+      const unsigned mn = __ballot_sync(FULL, need), md = __ballot_sync(FULL, may);
+      if (lane == 0) {
+        s_mask[k] = mn;
+        s_dir[k] = md;
+      }
+      tnet += __popc(mn);
+      tdir += __popc(md);
     }
-    if (lane == 0) Q.pair[pi] = make_int4(A, (KIND << 24) | slot, pstart, total);
-    return;
+    __syncwarp();
+    if (tnet == 0) {
+      // no node for the network: the marked nodes that passed go to the FP64 pass as in
+      // the plain screen
+      for (int k = lane; k < nch; k += 32) s_mask[k] = s_dir[k];
+      total = tdir;
+      __syncwarp();
+    } else {
+      const SlotView& cur = slots_of<KIND>(a, false);
+      const size_t sidx = (size_t)A * cur.cap + slot;
+      if (lane == 0) {  // set here; k_contacts_f writes the segment of a pair with contacts
+        cur.seg_start[sidx] = 0;
+        cur.seg_cnt[sidx] = 0;
+      }
+      const int tot = tnet + tdir;
+      int pstart = 0, pi = 0;
+      bool ok = false;
+      if (lane == 0) {
+        pstart = atomicAdd(&Q.ctr[0], tot);
+        pi = atomicAdd(&Q.ctr[1], 1);
+        ok = pstart + tot <= Q.pcap && pi < Q.paircap;
+        if (!ok) {
+          atomicOr(&a.status->flags, OVF_NET);
+          const long long need = (long long)pstart + tot;
+          atomicMax(&a.status->need_pend, (int)(need < 0x7fffffff ? need : 0x7fffffff));
+        }
+      }
+      pstart = __shfl_sync(FULL, pstart, 0);
+      pi = __shfl_sync(FULL, pi, 0);
+      ok = __shfl_sync(FULL, ok, 0);
+      if (!ok) return;
+      const int sh = F.pshape;
+      int off = 0;
+      for (int k = 0; k < nch; ++k) {
+        const unsigned mn = s_mask[k], md = s_dir[k], m = mn | md;
+        if (m == 0u) continue;
+        const int ni = node_of(k);
+        int base = 0;
+        if (lane == 0 && mn) base = atomicAdd(&Q.cnt[sh], __popc(mn));
+        base = __shfl_sync(FULL, base, 0);
+        if ((m >> lane) & 1u) {
+          const int idx = pstart + off + __popc(m & lanemask_lt());
+          Q.pend_n[idx] = ni;
+          if ((md >> lane) & 1u) {
+            Q.pend_v[idx] = 1;
+          } else {
+            const float4 nd = __ldg(a.S.node_pos_f + n0 + ni);
+            const float3 l = mulf(F.M, nd.x, nd.y, nd.z) + F.dB;
+            const float gx = fmaf(l.x, F.invh, F.cg.x), gy = fmaf(l.y, F.invh, F.cg.y),
+                        gz = fmaf(l.z, F.invh, F.cg.z);
+            const float lo = fminf(gx, fminf(gy, gz));
+            const float hi = fmaxf(gx - F.ux, fmaxf(gy - F.uy, gz - F.uz));
+            const bool edge = lo < F.eg || hi >= -F.eg;
+            const int r = base + __popc(mn & lanemask_lt());
+            if (r < Q.qcap) {
+              float4* row = Q.row + 2 * ((size_t)sh * Q.qcap + r);
+              row[0] = make_float4(fmaf(l.x, F.ms, -F.mc.x), fmaf(l.y, F.ms, -F.mc.y), fmaf(l.z, F.ms, -F.mc.z),
+                                   __int_as_float(idx | (edge ? (int)0x80000000u : 0)));
+              row[1] = make_float4(gx, gy, gz, F.T);
+            } else {
+              atomicOr(&a.status->flags, OVF_NET);
+              atomicMax(&a.status->need_netq, r + 1);
+            }
+          }
+        }
+        off += __popc(m);
+      }
+      if (lane == 0) Q.pair[pi] = make_int4(A, (KIND << 24) | slot, pstart, tot);
+      return;
+    }
   } else {
     for (int k = 0; k < nch; ++k) {
       const int ni = node_of(k);
@@ -1973,6 +2023,15 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
     const int z0 = axis_lo(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz), z1 = axis_hi(xg.z, g.mn.z, g.inv.z, g.size.z, reach, cz);
     const float3 xgf = make_float3((float)xg.x, (float)xg.y, (float)xg.z);
     const float Rgf = (float)Rg, n1g = fabsf(xgf.x) + fabsf(xgf.y) + fabsf(xgf.z);
+    // separation test of the pair (owner A, image) along the line of centres, as for
+    // particle pairs: a translated image has the particle's orientation, shape and scale
+    // (turned sector images are not tested)
+    const bool sep = a.S.sup_n != nullptr && !a.G.sector;
+    const Quat qi = a.P.quat[i];
+    const float4 qbf = make_float4((float)qi.q0, (float)qi.q1, (float)qi.q2, (float)qi.q3);
+    const float4 pbf = make_float4(xgf.x, xgf.y, xgf.z, 0.f);
+    const int shB = a.P.shape[i];
+    const float scB = (float)a.P.scale[i];
     for (int z = z0; z <= z1; ++z) {
       for (int y = y0; y <= y1; ++y) {
         // the cells x0..x1 of a row are contiguous in the sorted order
@@ -1987,8 +2046,15 @@ __global__ void k_ghost_candidates(StepArgs a, const int* __restrict__ g2_idx, c
               const float4 pa = __ldg(a.cell_pk + k);
               const float dx = pa.x - xgf.x, dy = pa.y - xgf.y, dz = pa.z - xgf.z;
               const float R = (pa.w + Rgf) * (1.0f + 1e-5f) + 1e-6f * (n1g + fabsf(pa.x) + fabsf(pa.y) + fabsf(pa.z));
-              if (!(dx * dx + dy * dy + dz * dz > R * R)) {
-                A = __ldg(g2_idx + k);
+              bool cand = !(dx * dx + dy * dy + dz * dz > R * R);
+              if (cand) A = __ldg(g2_idx + k);
+              if (cand && sep) {
+                const Quat qa = a.P.quat[A];
+                const float4 qaf = make_float4((float)qa.q0, (float)qa.q1, (float)qa.q2, (float)qa.q3);
+                const float n1a = __fadd_rn(__fadd_rn(fabsf(pa.x), fabsf(pa.y)), fabsf(pa.z));
+                cand = !pair_separated(a, pa, n1a, qaf, (float)a.P.scale[A], a.P.shape[A], pbf, qbf, scB, shB);
+              }
+              if (cand) {
                 slot = atomicAdd(&a.pgh.cnt[A], 1);
                 if (slot < a.pgh.cap) a.pgh.id[(size_t)A * a.pgh.cap + slot] = pid;
                 else atomicOr(&a.status->flags, OVF_GHOST);

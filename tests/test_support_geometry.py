@@ -1,91 +1,79 @@
 """The geometry behind the support tables of the candidate separation test (CPU).
 
-The tables (k_support_tables) bound, per cube-map cell of directions, v . p for every v in
-the cell by c . p + delta |p|, with c the cell's centre direction and delta the largest
-distance from c to the cell's four corner directions; and they take the maximum over the
-solid's dilated grid set from its points with a 6-neighbour outside the set. Both premises
-are checked here on a restatement of the mapping (same face order and gnomonic
-coordinates as sup_cell_f / sup_dir): sampled directions lie within delta of their cell's
-centre, and on a template's grid the boundary maximum equals the maximum over the whole
-dilated set, for many directions.
+The tables bound the support h(w) = max p . w of a point set along every direction from its
+values at the cube map's vertex directions (+-1, p, q): h is convex, so inside each half of a
+gnomonic cell it lies below the linear interpolation of its corner values. The solid's point
+set is built from the SDF grid refined by two: every point where the trilinear phi is <= 0
+must lie in the convex hull of the set, and the largest projection of the set must be reached
+on its boundary points (the ones the host uploads). Checked here on the restatement in
+support_restate.py: the interpolated bound is above the exact support for many directions and
+tight to a small fraction of the body size; sampled points with phi <= 0 never project beyond
+the set's support; and the boundary points reach the same support as the whole set.
 """
 import numpy as np
 
-M = 24
+import support_restate as sr
 
 
-def sup_dir(f, p, q):
-    sg = -1.0 if f & 1 else 1.0
-    v = np.array([sg, p, q]) if f < 2 else (np.array([q, sg, p]) if f < 4 else np.array([p, q, sg]))
-    return v / np.linalg.norm(v)
-
-
-def sup_cell(u):
-    a = np.abs(u)
-    if a[0] >= a[1] and a[0] >= a[2]:
-        f, m, p, q = (0 if u[0] >= 0 else 1), a[0], u[1], u[2]
-    elif a[1] >= a[2]:
-        f, m, p, q = (2 if u[1] >= 0 else 3), a[1], u[2], u[0]
-    else:
-        f, m, p, q = (4 if u[2] >= 0 else 5), a[2], u[0], u[1]
-    i = min(max(int(np.floor((p / m + 1.0) * 0.5 * M)), 0), M - 1)
-    j = min(max(int(np.floor((q / m + 1.0) * 0.5 * M)), 0), M - 1)
-    return f, i, j
-
-
-def cell_geometry(f, i, j):
-    h = 2.0 / M
-    p0, q0 = -1.0 + h * i, -1.0 + h * j
-    c = sup_dir(f, p0 + 0.5 * h, q0 + 0.5 * h)
-    delta = max(np.linalg.norm(sup_dir(f, p0 + h * (k & 1), q0 + h * (k >> 1)) - c) for k in range(4))
-    return c, delta
-
-
-def test_directions_lie_within_delta_of_their_cell_centre():
-    rng = np.random.default_rng(3)
-    worst = 0.0
-    for u in rng.normal(size=(20000, 3)):
-        u /= np.linalg.norm(u)
-        c, delta = cell_geometry(*sup_cell(u))
-        worst = max(worst, np.linalg.norm(u - c) / delta)
-        assert np.linalg.norm(u - c) <= delta * (1 + 1e-12)
-    assert worst > 0.9  # the bound is reached near the corners, so it is not loose
-
-
-def test_support_over_dilated_set_is_reached_on_its_boundary():
+def _template(k=3):
     from conftest import load_package
-    lsdem = load_package()
+    load_package()
     from lsdem_b200 import scenes
-    t = scenes.unit_templates(n_grid=16, n_nodes=200)[3]  # capsule
-    nx, ny, nz = t["size"]
-    phi = np.asarray(t["sdf"]).reshape(nz, ny, nx)
-    m = phi <= 0
-    for ax in range(3):  # dilation by one point along each axis: the 27-neighbourhood
-        d = m.copy()
-        a, b = [slice(None)] * 3, [slice(None)] * 3
-        a[ax], b[ax] = slice(1, None), slice(None, -1)
-        d[tuple(a)] |= m[tuple(b)]
-        d[tuple(b)] |= m[tuple(a)]
-        m = d
-    pad = np.pad(m, 1)
-    interior = m & pad[2:, 1:-1, 1:-1] & pad[:-2, 1:-1, 1:-1] & pad[1:-1, 2:, 1:-1] & pad[1:-1, :-2, 1:-1] \
-        & pad[1:-1, 1:-1, 2:] & pad[1:-1, 1:-1, :-2]
-    interior[[0, -1], :, :] = False
-    interior[:, [0, -1], :] = False
-    interior[:, :, [0, -1]] = False
-    boundary = m & ~interior
-    assert boundary.sum() < m.sum()
+    return scenes.unit_templates(n_grid=16, n_nodes=200)[k]
 
-    def points(mask):
-        z, y, x = np.nonzero(mask)
-        return np.stack([t["origin"][0] + t["spacing"] * x, t["origin"][1] + t["spacing"] * y,
-                         t["origin"][2] + t["spacing"] * z], 1)
 
-    pa, pb = points(m), points(boundary)
-    rng = np.random.default_rng(4)
-    for u in rng.normal(size=(500, 3)):
-        u /= np.linalg.norm(u)
-        c, delta = cell_geometry(*sup_cell(u))
-        full = (pa @ c + delta * np.linalg.norm(pa, axis=1)).max()
-        edge = (pb @ c + delta * np.linalg.norm(pb, axis=1)).max()
-        assert edge == full
+def _phi(t, x):
+    """Trilinear phi at points x (FP64, the reference's interpolation)."""
+    gx, gy, gz = (int(v) for v in t["size"])
+    phi = np.asarray(t["sdf"], np.float64).reshape(gz, gy, gx)
+    g = (x - np.asarray(t["origin"])) / t["spacing"]
+    i = np.clip(np.floor(g).astype(int), 0, [gx - 2, gy - 2, gz - 2])
+    f = g - i
+    out = 0.0
+    for k in range(8):
+        dx, dy, dz = k & 1, (k >> 1) & 1, k >> 2
+        w = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * (f[:, 2] if dz else 1 - f[:, 2])
+        out = out + w * phi[i[:, 2] + dz, i[:, 1] + dy, i[:, 0] + dx]
+    return out
+
+
+def test_interpolated_bound_is_above_the_support():
+    t = _template(0)
+    rng = np.random.default_rng(3)
+    for pts in (np.asarray(t["nodes"]), sr.solid_points(t)):
+        tab = sr.vertex_table(pts)
+        rad = np.linalg.norm(pts, axis=1).max()
+        worst = 0.0
+        for u in rng.normal(size=(4000, 3)):
+            H, m = sr.sup_bound_exact(tab, u)
+            bound = H * m / np.linalg.norm(u)
+            exact = (pts @ (u / np.linalg.norm(u))).max()
+            assert bound >= exact - 1e-15 * rad
+            worst = max(worst, (bound - exact) / rad)
+        assert worst < 2e-2  # second-order in the cell size: far tighter than a cone bound
+
+
+def test_points_with_nonpositive_phi_lie_within_the_solid_set():
+    for k in range(4):
+        t = _template(k)
+        P = sr.lattice_points(t, sr.refined_solid_mask(t))
+        o = np.asarray(t["origin"])
+        hi = o + t["spacing"] * (np.asarray(t["size"]) - 1)
+        rng = np.random.default_rng(10 + k)
+        x = o + (hi - o) * rng.random((200000, 3))
+        solid = x[_phi(t, x) <= 0.0]
+        assert len(solid) > 1000
+        W = rng.normal(size=(300, 3))
+        W /= np.linalg.norm(W, axis=1)[:, None]
+        sup = (P @ W.T).max(0)
+        assert np.all((solid @ W.T).max(0) <= sup + 1e-15)
+
+
+def test_support_over_refined_set_is_reached_on_its_boundary():
+    t = _template(3)  # capsule
+    m = sr.refined_solid_mask(t)
+    b = sr.boundary(m)
+    assert b.sum() < m.sum()
+    pa, pb = sr.lattice_points(t, m), sr.lattice_points(t, b)
+    W = np.random.default_rng(4).normal(size=(500, 3))
+    assert np.array_equal((pa @ W.T).max(0), (pb @ W.T).max(0))
