@@ -48,6 +48,7 @@ struct ShapeView {
   const double3* node_pos;    // node store, cluster order, unscaled
   const int* node_orig;       // original node index within the shape
   const double4* cl_sphere;   // cluster bounding sphere (xyz centre, w radius), unscaled
+  const float4* cl_sphere_f;  // the same rounded to FP32 (the precision forms' screen)
   const float4* sub_sphere;   // 4 per cluster (same shape offsets x 4): spheres of 8 nodes,
                               //   unscaled; radius < 0 for a sub-cluster past the last node
   const double* node_box;     // 8 per shape (unscaled): node bounding box lo xyz, hi xyz,

@@ -73,8 +73,8 @@ struct MlpTcSmem {
   uint4 a[MLP_TILE * 8];   // 128 rows x 128 B
   uint4 b[512];            // 64 rows x 128 B
   float4 w1[64];
-  float b2[64];
-  float w3[64];
+  alignas(16) float b2[64];
+  alignas(16) float w3[64];
   float b3;
   unsigned tmem;
   unsigned long long mbar;
@@ -194,7 +194,8 @@ __device__ __forceinline__ void mlp_tc_layer1(MlpTcSmem* S, float ux, float uy, 
 
 // Layer 2 of the tile: makes the A tile visible to the tensor core, thread 0 issues
 // the four K = 16 steps of the 128 x 64 x 64 MMA and commits them to the mbarrier,
-// and every thread waits for the completion (bounded). Returns false when the wait
+// the first warp waits for the completion (bounded) and the CTA meets it at a barrier,
+// after which every thread orders its tensor-memory reads. Returns false when the wait
 // gave up (the accumulators are then not valid; the caller sets its error flag).
 __device__ __forceinline__ bool mlp_tc_mma(MlpTcSmem* S) {
   asm volatile("fence.proxy.async.shared::cta;");
@@ -213,19 +214,23 @@ __device__ __forceinline__ bool mlp_tc_mma(MlpTcSmem* S) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
         smem_u32(&S->mbar)));
   }
+  // one warp waits for the completion (bounded); the others meet it at the barrier
   const unsigned mb = smem_u32(&S->mbar);
   const unsigned par = (unsigned)S->phase;
-  unsigned done = 0;
-  for (int it = 0; it < (1 << 22) && !done; ++it) {
-    asm volatile(
-        "{\n\t.reg .pred q;\n\tmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(done)
-        : "r"(mb), "r"(par));
+  unsigned done = 1;
+  if (threadIdx.x < 32) {
+    done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+      asm volatile(
+          "{\n\t.reg .pred q;\n\tmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+          : "=r"(done)
+          : "r"(mb), "r"(par));
+    }
   }
-  asm volatile("tcgen05.fence::after_thread_sync;");
   const bool all = __syncthreads_and(done) != 0;
   if (threadIdx.x == 0 && all) S->phase ^= 1;  // a wait that gave up keeps the parity it waits for
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
   return all;
 }
 
@@ -245,11 +250,17 @@ __device__ __forceinline__ float mlp_tc_output(MlpTcSmem* S) {
         : "r"(taddr + 16u * q));
     asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-    for (int j = 0; j < 16; j += 2) {
+    for (int j = 0; j < 16; j += 4) {
       const int n = 16 * q + j;
-      const unsigned s = silu_bf16x2(pack_bf16x2(__uint_as_float(v[j]) + S->b2[n], __uint_as_float(v[j + 1]) + S->b2[n + 1]));
-      const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&s);
-      y = fmaf(S->w3[n], __low2float(h), fmaf(S->w3[n + 1], __high2float(h), y));
+      // bias and output weights of four units in one 16-byte shared-memory load each
+      const float4 b = *reinterpret_cast<const float4*>(S->b2 + n);
+      const float4 w = *reinterpret_cast<const float4*>(S->w3 + n);
+      const unsigned s0 = silu_bf16x2(pack_bf16x2(__uint_as_float(v[j]) + b.x, __uint_as_float(v[j + 1]) + b.y));
+      const unsigned s1 = silu_bf16x2(pack_bf16x2(__uint_as_float(v[j + 2]) + b.z, __uint_as_float(v[j + 3]) + b.w));
+      const __nv_bfloat162 h0 = *reinterpret_cast<const __nv_bfloat162*>(&s0);
+      const __nv_bfloat162 h1 = *reinterpret_cast<const __nv_bfloat162*>(&s1);
+      y = fmaf(w.x, __low2float(h0), fmaf(w.y, __high2float(h0), y));
+      y = fmaf(w.z, __low2float(h1), fmaf(w.w, __high2float(h1), y));
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");

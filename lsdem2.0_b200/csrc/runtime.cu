@@ -345,6 +345,7 @@ struct lsdem_solver {
   DArr<int> s_node_off, s_node_cnt, s_cl_off, s_cl_cnt, s_node_orig;
   DArr<double3> s_node_pos;
   DArr<double4> s_cl;
+  DArr<float4> s_clf;   // cluster spheres in FP32 (each component rounded to nearest)
   DArr<float4> s_sub;   // sub-cluster spheres, 4 per cluster (FP32, radius rounded up)
   DArr<double> s_nbox;  // per shape: node bounding box (lo xyz, hi xyz), largest node distance, 0
   DArr<uint4> s_cell16;        // precision form: 16-bit corners of every grid cell
@@ -827,6 +828,12 @@ void initialize(lsdem_solver* s) {
   CK(s->s_node_orig.upload(node_orig.data(), node_orig.size(), st));
   CK(s->s_cl.upload(cl.data(), cl.size(), st));
   {
+    std::vector<float4> clf(cl.size());
+    for (size_t c = 0; c < cl.size(); ++c)
+      clf[c] = make_float4((float)cl[c].x, (float)cl[c].y, (float)cl[c].z, (float)cl[c].w);
+    CK(s->s_clf.upload(clf.data(), clf.size(), st));
+  }
+  {
     // support tables: per shape, points whose convex hull holds every point where the
     // trilinear phi is <= 0, template units. The grid is refined by two (points at half
     // spacings): phi restricted to one of the eight sub-cells of a cell is trilinear
@@ -1132,6 +1139,7 @@ StepArgs make_args(lsdem_solver* s, double dt) {
   a.S.node_off = s->s_node_off.p; a.S.node_cnt = s->s_node_cnt.p; a.S.cl_off = s->s_cl_off.p;
   a.S.cl_cnt = s->s_cl_cnt.p; a.S.node_pos = s->s_node_pos.p; a.S.node_orig = s->s_node_orig.p;
   a.S.cl_sphere = s->s_cl.p;
+  a.S.cl_sphere_f = s->s_clf.p;
   a.S.node_box = s->s_nbox.p;
   a.S.sub_sphere = s->s_sub.p;
   a.S.cell16 = s->s_cell16.p;

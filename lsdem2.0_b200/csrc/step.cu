@@ -1233,9 +1233,9 @@ LD bool node_may_hit_f(const StepArgs& a, double3 xA, const PairF& F, float4 nd,
 //    every node of the cluster.
 //  With up != nullptr (learned form), *up receives an estimate of the largest phi / h
 //  over the cluster's nodes (phi at q plus gmax times the reach; +inf when phi at q is
-//  not looked up): where it is below the network's rejection threshold the network
-//  cannot reject any of them (an efficiency choice only: every node the network does not
-//  see takes the grid test).
+//  not looked up): where it is below the network's rejection threshold the network would
+//  reject a node only by overestimating phi there, so the nodes are not sent to it (an
+//  efficiency choice only: every node the network does not see takes the grid test).
 template <int KIND, int SDFK>
 LD bool cluster_may_hit_f(const PairF& F, float4 cn, float scA, float* up = nullptr) {
   if (up) *up = INFINITY;
@@ -1299,11 +1299,7 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   for (int c0 = 0; c0 < ncl; c0 += 32) {
     const int c = c0 + lane;
     bool keep = false;
-    if (c < ncl) {
-      const double2* sp = reinterpret_cast<const double2*>(a.S.cl_sphere + cl0 + c);
-      const double2 s0 = __ldg(sp), s1 = __ldg(sp + 1);
-      keep = cluster_may_hit_f<KIND, SDFK>(F, make_float4((float)s0.x, (float)s0.y, (float)s1.x, (float)s1.y), scA);
-    }
+    if (c < ncl) keep = cluster_may_hit_f<KIND, SDFK>(F, __ldg(a.S.cl_sphere_f + cl0 + c), scA);
     const unsigned m = __ballot_sync(FULL, keep);
     if (keep) s_cl[nsurv + __popc(m & lanemask_lt())] = c;
     nsurv += __popc(m);
@@ -1311,8 +1307,8 @@ LD void screen_pair_f(const StepArgs& a, int A, int slot, int pid, int li, int* 
   __syncwarp();
   // second level: sub-clusters of 8 nodes of the surviving clusters, compacted in
   // ascending order; chunk k of the node loop is sub-clusters 4k .. 4k + 3. Learned
-  // form: bit 15 marks a sub-cluster whose nodes the network cannot reject (their phi / h
-  // estimate is below its threshold); they take the grid test here.
+  // form: bit 15 marks a sub-cluster whose phi / h estimate is below the network's
+  // threshold; its nodes take the grid test here instead of the network.
   int nsub = 0;
   for (int j0 = 0; j0 < 4 * nsurv; j0 += 32) {
     const int j = j0 + lane;
