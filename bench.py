@@ -110,9 +110,17 @@ B_PARTICLE_SCREEN = 72
 B_PAIR_SCREEN = 120
 # whole-step algorithmic bytes per particle (state, keys, sort, candidates)
 B_STEP_PARTICLE = 448
-# What bounds the screen, from an ncu capture of k_screen_f (particle pairs, FP32/BF16 form)
-# on the 200,000-particle settling box (the recipe and figures are in profiles/).
-SCREEN_LIMITER = None
+# What bounds the screen: an ncu full-set capture of k_screen_f<1, 2, 0> (particle pairs,
+# FP32/BF16 form) on the settling configuration at 200,000 particles (two launches alike).
+SCREEN_CAPTURE = {
+    "case": "settling configuration at 200,000 particles, FP32/BF16 form, particle-pair screen, steps 2-3",
+    "dram_bytes_per_launch": 38.35e6,
+    # 72 B x 200,000 owners + 120 B x ~51,500 particle pairs (of 55,400 pairs of all kinds)
+    "algorithmic_bytes_per_launch": 72 * 200_000 + 120 * 51_500,
+    "issue_active": 0.616, "warps_active": 0.447, "warps_active_limit": 0.50,
+    "leading_stall": "long_scoreboard (5.5 warps per issue): dependent L2 loads",
+    "dram_throughput": 0.039,
+}
 
 
 class Clocks:
@@ -767,7 +775,11 @@ def main():
         else:
             kernel = "k_screen_f"
             bytes_launch = (B_PARTICLE_SCREEN * n * launches_per_step + B_PAIR_SCREEN * pairs) / launches_per_step
-        traffic = None
+        # DRAM bytes per launch: the capture's measured traffic scaled by algorithmic bytes
+        # (its excess over them is the 16-bit template store read once per step after the
+        # L2 flush, so the scaling overstates it for larger cases: an upper estimate)
+        traffic = (SCREEN_CAPTURE["dram_bytes_per_launch"] / SCREEN_CAPTURE["algorithmic_bytes_per_launch"] *
+                   bytes_launch) if prec != 0 else None
         achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
         b_step = B_STEP_PARTICLE * n + B_CONTACT * stats["contacts"] + 16 * pairs
         ms_step = head["ms"] / args.steps
@@ -787,7 +799,10 @@ def main():
             "config": dict(cfg, form=args.form, parallelism=f"replicas x{world}",
                            l2=f"flushed: {L2_FLUSH_BYTES >> 20} MB written before every timed step, outside "
                               f"its events (per-step algorithmic traffic {b_step / 1e6:.0f} MB)",
-                           contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs),
+                           contacts_per_step=stats["contacts"], candidate_pairs_per_step=pairs,
+                           pairs_per_step={"particle": stats["pairs_particle"], "wall": stats["pairs_wall"],
+                                           "image": stats["pairs_ghost"]},
+                           contacts_per_particle=stats["contacts"] / n),
             "forms": forms,
             "headline_over_plain_grid": (value / plain) if plain else None,
             "contacts_per_s": stats["contacts"] * per_s,
@@ -798,7 +813,13 @@ def main():
             "roofline": {"bound": "latency/issue", "kernel": kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
-                         "hbm_is_limiter": False, "limiter": SCREEN_LIMITER if prec != 0 else None,
+                         "traffic_kind": "scaled from a 200,000-particle ncu capture" if prec != 0 else None,
+                         "hbm_is_limiter": False,
+                         "limiter": ({"bound": "L2 load latency / issue", "issue_active": SCREEN_CAPTURE["issue_active"],
+                                      "warps_active": SCREEN_CAPTURE["warps_active"],
+                                      "warps_active_limit": SCREEN_CAPTURE["warps_active_limit"],
+                                      "leading_stall": SCREEN_CAPTURE["leading_stall"],
+                                      "case": SCREEN_CAPTURE["case"]} if prec != 0 else None),
                          "node_tests_per_s_in_screen": (scr.get("node_tests", 0.0) * head["profile_steps"] /
                                                         ((np_ms + g_ms) * 1e-3)) if scr else None},
             "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (ms_step * 1e-3) / 1e9},
