@@ -261,6 +261,10 @@ int lsdem_step_stats(lsdem_solver* s, long long* out4);
  * Enabling resets them; off by default. */
 int lsdem_set_screen_stats(lsdem_solver* s, int on);
 int lsdem_get_screen_stats(lsdem_solver* s, long long* out8);
+/* Precision forms without the network: of the screen's queued nodes, those of particle,
+ * wall and image pairs (out3), summed like lsdem_get_screen_stats (no counterpart in the
+ * reference). */
+int lsdem_get_screen_queue(lsdem_solver* s, long long* out3);
 
 /* Learned per-shape SDF (no counterpart in the reference). After lsdem_initialize,
  * trains one 3-64-64-1 SiLU network per shape template on the GPU (own forward,
@@ -274,6 +278,13 @@ int lsdem_get_screen_stats(lsdem_solver* s, long long* out8);
  * measured bound (template units). Either may be NULL. */
 int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samples, double lr,
                             unsigned long long seed, double* loss_out, double* err_out);
+/* Training options of the learned SDF (no counterpart in the reference), before
+ * lsdem_train_learned_sdf: the target phi / R is clipped to [clip_lo, clip_hi]
+ * (defaults -0.25, 0.5; the one-sided error is measured against the clipped value,
+ * so clip_lo <= -0.05 and clip_hi >= 0.1 keep the trust band inside the range), and
+ * near_fraction (default 0.5) of the samples are drawn near the surface, the rest
+ * uniform in the grid box. LSDEM_ERR_ARG outside those ranges. */
+int lsdem_set_learned_training(lsdem_solver* s, double clip_lo, double clip_hi, double near_fraction);
 /* Precision forms: when on, the screen rejects a node by the network where
  * phi_net exceeds the trust band delta (2 % of the shape size) plus 1.25 x the
  * measured one-sided error max(phi_net - phi_grid) over the validation points with

@@ -100,10 +100,12 @@ _SIGS = {
     "lsdem_get_bond_params": (C.c_int, [P, DP, DP, DP]),
     "lsdem_train_learned_sdf": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, DP, DP]),
     "lsdem_set_learned_sdf": (C.c_int, [P, C.c_int]),
+    "lsdem_set_learned_training": (C.c_int, [P, C.c_double, C.c_double, C.c_double]),
     "lsdem_get_learned_sdf": (C.c_int, [P, C.c_int, FP, FP]),
     "lsdem_mlp_eval": (C.c_int, [P, C.c_int, C.c_int, DP, FP]),
     "lsdem_mlp_gradient": (C.c_int, [C.c_int, C.c_int, FP, FP, FP, FP, FP]),
     "lsdem_get_screen_stats": (C.c_int, [P, LP]),
+    "lsdem_get_screen_queue": (C.c_int, [P, LP]),
     "lsdem_pack_rsa": (C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_ulonglong, C.c_int, IP, DP]),
     "lsdem_cell_sort_static": (C.c_int, [P, C.c_int, DP, DP, DP, IP, P, P, P, P, P, P]),
     "lsdem_mesh_grid_box": (C.c_int, [DP, C.c_int, C.c_double, C.c_int, DP, IP]),
@@ -505,6 +507,11 @@ class Solver:
         return {"pairs_particle": int(o[0]), "pairs_wall": int(o[1]), "pairs_ghost": int(o[2]), "contacts": int(o[3])}
 
     # ---- learned per-shape SDF ---------------------------------------------------
+    def set_learned_training(self, clip_lo=-0.25, clip_hi=0.5, near_fraction=0.5):
+        """Training options of the learned SDF: target clip range (units of R) and the share
+        of samples drawn near the surface."""
+        self._chk(lib.lsdem_set_learned_training(self.h, float(clip_lo), float(clip_hi), float(near_fraction)))
+
     def train_learned_sdf(self, iterations=3000, batch=4096, samples=1 << 18, lr=3e-3, seed=12345):
         """Trains one network per shape template; returns (loss, err) per shape (err in template units)."""
         ns = self.num(4)
@@ -539,7 +546,11 @@ class Solver:
     def screen_stats(self):
         o = np.zeros(8, np.int64)
         self._chk(lib.lsdem_get_screen_stats(self.h, o.ctypes.data_as(LP)), "get_screen_stats")
-        return dict(zip(self.SCREEN_COUNTERS, (int(v) for v in o)))
+        q = np.zeros(3, np.int64)
+        self._chk(lib.lsdem_get_screen_queue(self.h, q.ctypes.data_as(LP)), "get_screen_queue")
+        out = dict(zip(self.SCREEN_COUNTERS, (int(v) for v in o)))
+        out.update(queued_particle=int(q[0]), queued_wall=int(q[1]), queued_image=int(q[2]))
+        return out
 
     def device_pointers(self):
         ptrs = [P() for _ in range(6)]

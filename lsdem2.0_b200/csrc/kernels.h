@@ -264,13 +264,14 @@ struct MlpShapeData {
   const int* node_cnt;
   const double3* node_pos;
 };
-void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long seed, float4* samples, cudaStream_t st);
+void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long seed, const MlpTrainOpts& opt,
+                 float4* samples, cudaStream_t st);
 cudaError_t mlp_train_step(float* params, const float4* samples, int nshapes, int S, int B, long long it,
                            float* partial, float* loss, float* m1, float* m2, float lr, int step, cudaStream_t st);
 void mlp_pack(const float* params, int nshapes, MlpInfer* out, cudaStream_t st);
 // fail (device int): set to 1 when a tensor-core wait gave up (results not valid)
 void mlp_validate(const MlpShapeData& D, int nshapes, const MlpInfer* inf, int S2, unsigned long long seed,
-                  const float* delta, unsigned* err_bits, int* fail, cudaStream_t st);
+                  const MlpTrainOpts& opt, const float* delta, unsigned* err_bits, int* fail, cudaStream_t st);
 cudaError_t mlp_grad_once(const float* params, const float4* pts, int n, float* partial, float* loss, cudaStream_t st);
 void mlp_forward(const float* params, const float4* pts, int n, float* y, cudaStream_t st);
 void mlp_infer(const MlpInfer* inf, const MlpNorm& nm, const double3* pts, int n, float* phi, int* fail,

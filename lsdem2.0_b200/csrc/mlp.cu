@@ -55,8 +55,8 @@ __device__ __forceinline__ float dsilu_f(float x) {
 }  // namespace
 
 // Samples of all shapes: samples[s * S + k] = (u.x, u.y, u.z, phi / R clipped to
-// [MLP_CLIP_LO, MLP_CLIP_HI]).
-__global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, float4* samples) {
+// [opt.clip_lo, opt.clip_hi]); a share opt.near of them near the surface.
+__global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, MlpTrainOpts opt, float4* samples) {
   const int s = blockIdx.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= S) return;
@@ -67,7 +67,7 @@ __global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, fl
   const double3 hi = make_double3(o.x + (gs.x - 1) * h, o.y + (gs.y - 1) * h, o.z + (gs.z - 1) * h);
   const uint64_t base = seed ^ ((uint64_t)s << 40) ^ ((uint64_t)k << 2);
   double3 p;
-  if ((k & 1) == 0 || D.node_cnt[s] == 0) {  // uniform in the grid box
+  if (unit01(base ^ 0x5851f42d4c957f2dull) >= (double)opt.near || D.node_cnt[s] == 0) {  // uniform in the box
     p = make_double3(o.x + (hi.x - o.x) * unit01(base), o.y + (hi.y - o.y) * unit01(base + 1),
                      o.z + (hi.z - o.z) * unit01(base + 2));
   } else {             // near the surface: a node plus N(0, (2h)^2) per axis (Box-Muller)
@@ -84,7 +84,7 @@ __global__ void k_mlp_samples(MlpShapeData D, int S, unsigned long long seed, fl
   const double phi = grid_phi(D.sdf + D.sdf_off[s], gs, o, h, p);
   samples[(size_t)s * S + k] = make_float4((float)((p.x - nm.cx) / nm.R), (float)((p.y - nm.cy) / nm.R),
                                            (float)((p.z - nm.cz) / nm.R),
-                                           (float)fmin(fmax(phi / nm.R, (double)MLP_CLIP_LO), (double)MLP_CLIP_HI));
+                                           (float)fmin(fmax(phi / nm.R, (double)opt.clip_lo), (double)opt.clip_hi));
 }
 
 // Block-partial gradients of the mean squared error over points of the batch:
@@ -232,8 +232,9 @@ __global__ void k_mlp_pack(const float* __restrict__ params, MlpInfer* out) {
 // units of R). Float bits of running maxima of non-negative values (which order as
 // integers).
 __global__ void __launch_bounds__(MLP_TILE) k_mlp_validate(MlpShapeData D, const MlpInfer* __restrict__ inf, int S2,
-                                                           unsigned long long seed, const float* __restrict__ delta,
-                                                           unsigned* err_bits, int* fail) {
+                                                           unsigned long long seed, MlpTrainOpts opt,
+                                                           const float* __restrict__ delta, unsigned* err_bits,
+                                                           int* fail) {
   extern __shared__ unsigned char dyn[];
   MlpTcSmem* T = mlp_tc_smem(dyn);
   mlp_tc_setup(T);
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_validate(MlpShapeData D, const
     ok = mlp_tc_mma(T);
     const float net = mlp_tc_output(T) * nm.R;
     if (act && ok) {
-      const float tgt = (float)fmin(fmax(phi, (double)(MLP_CLIP_LO * nm.R)), (double)(MLP_CLIP_HI * nm.R));
+      const float tgt = (float)fmin(fmax(phi, (double)(opt.clip_lo * nm.R)), (double)(opt.clip_hi * nm.R));
       emax = fmaxf(emax, fabsf(net - tgt));
       if (phi <= (double)dlt) ein = fmaxf(ein, net - tgt);
     }
@@ -333,8 +334,9 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_infer(const MlpInfer* __restri
 // ---------------------------------------------------------------------------
 // Host launchers
 
-void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long seed, float4* samples, cudaStream_t st) {
-  k_mlp_samples<<<dim3((S + 255) / 256, nshapes), 256, 0, st>>>(D, S, seed, samples);
+void mlp_samples(const MlpShapeData& D, int nshapes, int S, unsigned long long seed, const MlpTrainOpts& opt,
+                 float4* samples, cudaStream_t st) {
+  k_mlp_samples<<<dim3((S + 255) / 256, nshapes), 256, 0, st>>>(D, S, seed, opt, samples);
 }
 
 cudaError_t mlp_train_step(float* params, const float4* samples, int nshapes, int S, int B, long long it,
@@ -366,9 +368,9 @@ static void mlp_tc_attr() {
 }
 
 void mlp_validate(const MlpShapeData& D, int nshapes, const MlpInfer* inf, int S2, unsigned long long seed,
-                  const float* delta, unsigned* err_bits, int* fail, cudaStream_t st) {
+                  const MlpTrainOpts& opt, const float* delta, unsigned* err_bits, int* fail, cudaStream_t st) {
   mlp_tc_attr();
-  k_mlp_validate<<<dim3(148, nshapes), MLP_TILE, MLP_TC_SMEM, st>>>(D, inf, S2, seed, delta, err_bits, fail);
+  k_mlp_validate<<<dim3(148, nshapes), MLP_TILE, MLP_TC_SMEM, st>>>(D, inf, S2, seed, opt, delta, err_bits, fail);
 }
 
 cudaError_t mlp_grad_once(const float* params, const float4* pts, int n, float* partial, float* loss, cudaStream_t st) {

@@ -62,6 +62,13 @@ struct MlpNorm {
 // range.
 constexpr float MLP_CLIP_LO = -0.25f;
 constexpr float MLP_CLIP_HI = 0.5f;
+// Training options: target clip range (units of R) and the share of samples drawn near the
+// surface (a node moved by N(0, (2h)^2) per axis; the rest uniform in the grid box).
+struct MlpTrainOpts {
+  float clip_lo = MLP_CLIP_LO;
+  float clip_hi = MLP_CLIP_HI;
+  float near = 0.5f;
+};
 
 // Points per tensor-core tile (= threads of an inference CTA) and TMEM columns.
 constexpr int MLP_TILE = 128;

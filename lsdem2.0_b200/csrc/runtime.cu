@@ -366,6 +366,7 @@ struct lsdem_solver {
   DArr<unsigned> mlp_err;
   std::vector<MlpNorm> h_mlp_norm;
   std::vector<float> h_mlp_band;
+  MlpTrainOpts mlp_opt;
   bool mlp_trained = false, mlp_on = false;
   DArr<int4> mb_pair;
   long long mb_cap = 0, mb_pcap = 0;
@@ -2019,7 +2020,7 @@ int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samp
     CK(s->mlp_loss.alloc((size_t)ns * nblk));
     CK(s->mlp_samples.alloc((size_t)ns * samples));
     const MlpShapeData D = mlp_shape_data(s);
-    mlp_samples(D, ns, samples, seed, s->mlp_samples.p, st);
+    mlp_samples(D, ns, samples, seed, s->mlp_opt, s->mlp_samples.p, st);
     CK(cudaGetLastError());
     // Adam with a cosine learning-rate schedule down to 1 % of lr
     for (int it = 0; it < iterations; ++it) {
@@ -2047,7 +2048,7 @@ int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samp
     CK(s->mlp_err.alloc(2 * (size_t)ns)); CK(s->mlp_err.zero(st));
     DArr<int> dfail;
     CK(dfail.alloc(1)); CK(dfail.zero(st));
-    mlp_validate(D, ns, s->mlp_inf.p, samples, seed ^ 0x5eedf00dull, ddelta.p, s->mlp_err.p, dfail.p, st);
+    mlp_validate(D, ns, s->mlp_inf.p, samples, seed ^ 0x5eedf00dull, s->mlp_opt, ddelta.p, s->mlp_err.p, dfail.p, st);
     CK(cudaGetLastError());
     std::vector<unsigned> eb = dl(s->mlp_err, 2 * (size_t)ns, st);
     std::vector<int> hf = dl(dfail, 1, st);
@@ -2076,6 +2077,19 @@ int lsdem_train_learned_sdf(lsdem_solver* s, int iterations, int batch, int samp
     s->mlp_trained = true;
     return LSDEM_OK;
   });
+}
+
+int lsdem_set_learned_training(lsdem_solver* s, double clip_lo, double clip_hi, double near_fraction) {
+  if (!s) return LSDEM_ERR_ARG;
+  // the trust band (at most 4 % of R) must lie inside the clip range
+  if (!(clip_lo >= -1.0 && clip_lo <= -0.05 && clip_hi >= 0.1 && clip_hi <= 2.0 && near_fraction >= 0.0 &&
+        near_fraction <= 1.0))
+    return fail(s, LSDEM_ERR_ARG,
+                "lsdem_set_learned_training: clip_lo in [-1, -0.05], clip_hi in [0.1, 2], near_fraction in [0, 1]");
+  s->mlp_opt.clip_lo = (float)clip_lo;
+  s->mlp_opt.clip_hi = (float)clip_hi;
+  s->mlp_opt.near = (float)near_fraction;
+  return LSDEM_OK;
 }
 
 int lsdem_set_learned_sdf(lsdem_solver* s, int on) {
@@ -2642,7 +2656,7 @@ int lsdem_set_screen_stats(lsdem_solver* s, int on) {
   if (!s) return LSDEM_ERR_ARG;
   return guard(s, [&] {
     if (on) {
-      CK(s->scr_stats.alloc(8));
+      CK(s->scr_stats.alloc(11));
       CK(s->scr_stats.zero(s->stream));
     } else {
       CK(cudaStreamSynchronize(s->stream));
@@ -2660,6 +2674,18 @@ int lsdem_get_screen_stats(lsdem_solver* s, long long* out8) {
     auto c = dl(s->scr_stats, 8, s->stream);
     CK(cudaStreamSynchronize(s->stream));
     for (int k = 0; k < 8; ++k) out8[k] = (long long)c[k];
+    return LSDEM_OK;
+  });
+}
+
+int lsdem_get_screen_queue(lsdem_solver* s, long long* out3) {
+  if (!s || !out3) return LSDEM_ERR_ARG;
+  return guard(s, [&] {
+    for (int k = 0; k < 3; ++k) out3[k] = 0;
+    if (!s->scr_stats.p) return LSDEM_OK;
+    auto c = dl(s->scr_stats, 11, s->stream);
+    CK(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 3; ++k) out3[k] = (long long)c[8 + k];
     return LSDEM_OK;
   });
 }

@@ -1532,9 +1532,12 @@ __global__ void __launch_bounds__(NP_WARPS * 32, KINDS == 1 ? 8 : 5) k_screen_f(
                                            s_mask[warp], cnt);
     }
   }
-  if (a.screen_stats && (threadIdx.x & 31) == 0)
+  if (a.screen_stats && (threadIdx.x & 31) == 0) {
     for (int k = 0; k < 8; ++k)
       if (cnt[k]) atomicAdd(&a.screen_stats[k], (unsigned long long)cnt[k]);
+    // grid screen: nodes queued for the FP64 test by partner kind (one kind per launch)
+    if (!LRN && cnt[5]) atomicAdd(&a.screen_stats[8 + (KINDS == 1 ? 0 : (KINDS == 2 ? 1 : 2))], (unsigned long long)cnt[5]);
+  }
 }
 
 // Queued pairs of the screen, one warp each, in FP64: the reference's node test

@@ -84,6 +84,12 @@ def test_invalid_input_errors(lsdem):
     with pytest.raises(lsdem.LSDEMError) as e:
         sv.initialize([0, 0, 0], [1, 0, 1])
     assert e.value.code == 1 and "domain" in str(e.value)
+    # training options of the learned SDF: the trust band must lie inside the clip range
+    sv.set_learned_training(-0.1, 0.3, 0.8)
+    for bad in ((-0.01, 0.5, 0.5), (-0.25, 0.05, 0.5), (-0.25, 0.5, 1.5)):
+        with pytest.raises(lsdem.LSDEMError) as e:
+            sv.set_learned_training(*bad)
+        assert e.value.code == 1 and "clip_lo" in str(e.value)
 
 
 def test_bond_stiffness_from_beam_theory(lsdem):
