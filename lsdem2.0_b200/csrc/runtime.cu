@@ -103,7 +103,10 @@ inline V3 hcross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x 
 
 inline int lin3h(int x, int y, int z, int nx, int ny) { return z * ny * nx + y * nx + x; }
 
-// Mass properties by smoothed Heaviside integration (LSSolver.h:66-135).
+// Mass properties by smoothed Heaviside integration (LSSolver.h:66-135). The loops, their
+// x / y / z order and the smoothed Heaviside are the reference's on purpose: the sums are
+// then taken in the reference's order and the masses and inertias equal its values bit for
+// bit (the GPU routine in massprops.cu sums in parallel and agrees to rounding).
 void mass_props(const double* sdf, const int* sz, const double* o, double h, double density, double* out) {
   auto H = [](double phi, double eps) -> double {
     if (eps <= 0.0) return (phi > 0.0) ? 0.0 : 1.0;
