@@ -907,20 +907,32 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
     re-placement cannot resolve. The default is 0.25 with exclusion 0.85 (~14 % of bodies in
     deep overlap before re-placement, a few per thousand after it); the bodies re-placement
     cannot fit go to a reserve slab above the packing (`reserve` x n bounding spheres at 20 %
-    fraction, no overlaps), which raises the ceiling accordingly."""
+    fraction, no overlaps). The domain is a cube: the packing fills its lower part at the stated
+    fraction and the slab its top, so no body starts above the domain's y extent (the
+    reference's image keys test z against the y bound, which would image such a body in place
+    onto itself)."""
     rng = np.random.default_rng(seed_for(4) if seed is None else seed)
     T = templates or superquadric_templates(lsdem, rng, shapes, exponents, semi_axes, n_grid, n_nodes, device=device)
     tm = _unit_density_templates(lsdem, T, gpu=True)
     shape = rng.integers(0, len(tm), size=n).astype(np.int32)
     vol = np.array([t["mass"] for t in tm])[shape].sum()
-    L = (vol / solid_fraction) ** (1.0 / 3.0)
     scale = np.ones(n)
     bound = np.array([t["bound"] for t in tm])[shape]
     b = float(bound.max())
-    slab = reserve * n * (4.0 / 3.0) * math.pi * float(np.mean(bound ** 3)) / 0.2 / (L * L) + 2 * b
-    H = L + b + slab
-    rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - b]), "periodic": True,
-           "bound": bound, "reserve_lo": np.array([0.0, 0.0, L + b]), "reserve_hi": np.array([L, L, H])}
+    # A cube of side L holds the packing (height L - slab, at the stated solid fraction) and
+    # the reserve slab above it. The domain is kept no taller than it is wide: the images'
+    # cell keys test z against the y bound (the reference's rule, kept), so a body above
+    # the y extent would be imaged in place onto itself.
+    sph = (4.0 / 3.0) * math.pi * float(np.mean(bound ** 3))
+    L = (vol / solid_fraction) ** (1.0 / 3.0)
+    for _ in range(60):
+        slab = reserve * n * sph / 0.2 / (L * L) + 2 * b
+        L = math.sqrt(vol / solid_fraction / (L - slab))
+    slab = reserve * n * sph / 0.2 / (L * L) + 2 * b
+    H = L
+    rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - slab - b]),
+           "periodic": True, "bound": bound, "reserve_lo": np.array([0.0, 0.0, L - slab + b]),
+           "reserve_hi": np.array([L, L, H])}
     pos = _rsa(lsdem, rng, rsa)
     inv_mass, inv_inertia = _body_arrays(tm, shape, scale, density)
     walls = [plane_wall(L, [0.5 * L, 0.5 * L, 0.0], True, mu, e), plane_wall(L, [0.5 * L, 0.5 * L, H], False, mu, e)]
