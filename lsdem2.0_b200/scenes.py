@@ -891,6 +891,18 @@ def drum(lsdem, n=500_000, shapes=64, exponents=(2.0, 8.0), semi_axes=(1e-3, 3e-
             "periodic": 0, "walls": [w], "size_factor": s, "rsa": rsa}
 
 
+def settling_geometry(vol, solid_fraction, n, sphere_volume, b, reserve):
+    """Side L of the cubic domain of the large-scale workload and the height of its reserve slab:
+    the packing fills [0, L)^2 x [0, L - slab) at solid_fraction (L^2 (L - slab) = vol /
+    solid_fraction), the slab on top holds reserve x n bounding spheres (mean volume
+    sphere_volume) at 20 % fraction plus a gap of two largest bounding radii b."""
+    L = (vol / solid_fraction) ** (1.0 / 3.0)
+    for _ in range(60):  # a contraction (factor about 1/2): converged to rounding
+        slab = reserve * n * sphere_volume / 0.2 / (L * L) + 2 * b
+        L = math.sqrt(vol / solid_fraction / (L - slab))
+    return L, reserve * n * sphere_volume / 0.2 / (L * L) + 2 * b
+
+
 def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=(1e-3, 2.5e-3), n_grid=48,
                  n_nodes=1500, solid_fraction=0.25, kn=1e5, kt_ratio=0.8, mu=0.5, e=0.6, density=2500.0, dt=5e-7,
                  exclusion=0.85, reserve=0.02, seed=None, device=0, templates=None):
@@ -923,12 +935,8 @@ def settling_box(lsdem, n=2_000_000, shapes=16, exponents=(2.0, 6.0), semi_axes=
     # the reserve slab above it. The domain is kept no taller than it is wide: the images'
     # cell keys test z against the y bound (the reference's rule, kept), so a body above
     # the y extent would be imaged in place onto itself.
-    sph = (4.0 / 3.0) * math.pi * float(np.mean(bound ** 3))
-    L = (vol / solid_fraction) ** (1.0 / 3.0)
-    for _ in range(60):
-        slab = reserve * n * sph / 0.2 / (L * L) + 2 * b
-        L = math.sqrt(vol / solid_fraction / (L - slab))
-    slab = reserve * n * sph / 0.2 / (L * L) + 2 * b
+    L, slab = settling_geometry(vol, solid_fraction, n, (4.0 / 3.0) * math.pi * float(np.mean(bound ** 3)), b,
+                                reserve)
     H = L
     rsa = {"radius": exclusion * bound, "lo": np.array([0.0, 0.0, b]), "hi": np.array([L, L, L - slab - b]),
            "periodic": True, "bound": bound, "reserve_lo": np.array([0.0, 0.0, L - slab + b]),

@@ -146,3 +146,18 @@ def test_host_model_of_a_scene_equals_the_solvers(lsdem):
         assert np.array_equal(np.asarray(m[k]), pp[k]), k
     assert np.allclose(m["quat"], sv.state()["quat"], rtol=0, atol=1e-15)
     sv.close()
+
+
+def test_settling_domain_is_a_cube_with_the_packing_at_its_fraction(lsdem):
+    """The large-scale workload's domain: a cube whose lower part holds the packing at the
+    stated solid fraction and whose top holds the reserve slab, so that no body starts above
+    the domain's y extent (the image-key rule tests z against the y bound)."""
+    import math
+    from lsdem_b200 import scenes
+    for n, b, sph in ((2_000_000, 2.9e-3, 4.0e-8), (200_000, 2.9e-3, 4.0e-8), (4000, 2.5e-3, 3.0e-8)):
+        vol = n * sph / 1.9  # bounding spheres hold ~1.9 x the body volume
+        L, slab = scenes.settling_geometry(vol, 0.25, n, sph, b, 0.02)
+        assert abs(L * L * (L - slab) * 0.25 / vol - 1.0) < 1e-9
+        assert slab == pytest.approx(0.02 * n * sph / 0.2 / (L * L) + 2 * b, rel=1e-12)
+        assert 2 * b < slab < 0.5 * L
+        assert L > (vol / 0.25) ** (1.0 / 3.0)
