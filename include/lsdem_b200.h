@@ -288,7 +288,9 @@ int lsdem_set_learned_training(lsdem_solver* s, double clip_lo, double clip_hi, 
 /* Precision forms: when on, the screen rejects a node by the network where
  * phi_net exceeds the trust band delta (2 % of the shape size) plus 1.25 x the
  * measured one-sided error max(phi_net - phi_grid) over the validation points with
- * phi_grid <= delta; every other node goes on to the grid screen and the FP64 test. */
+ * phi_grid <= delta; every other node goes on to the grid screen and the FP64 test.
+ * Nodes of 8-node sub-clusters whose grid estimate of phi lies below that threshold
+ * skip the network and take the grid test directly. */
 int lsdem_set_learned_sdf(lsdem_solver* s, int on);
 /* FP32 weights of a shape's network (LSDEM_MLP_PARAMS floats: W1[64][3], b1[64],
  * W2[64][64], b2[64], w3[64], b3, padding) and norm[8] = centre xyz, R, measured
